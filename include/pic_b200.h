@@ -1,0 +1,232 @@
+/*
+ * pic_b200.h — C ABI of the B200-native 2D electrostatic PIC step.
+ *
+ * One engine owns a device memory pool and steps every job it holds together
+ * (a plain simulation is an engine with one job).  All signatures use plain C
+ * types: device streams are passed as `void*` (a cudaStream_t), host or device
+ * arrays as plain pointers plus sizes.  Every function returns a PIC_* status;
+ * pic_last_error() gives a message for the last failure on the calling thread.
+ *
+ * Reference interface each entry point replaces (file:line in dimad285/PIC_CUDA):
+ *   pic_job_create            Grid2D::Grid2D (grid.cu:10), Particles2D::Particles2D
+ *                             (particles.cu:112), add_species (particles.cu:174),
+ *                             Boundaries2D::add_wall/compile_walls (boundaries.cu:3,11)
+ *   pic_job_load_species      the host->device copies of r, r_old, v in main.cu:232-238
+ *   pic_step                  updateSimulationCUDA (main.cu:37-140)
+ *   pic_job_run_phases        the individual kernels of the step: update_coordinates
+ *                             (kernels.cu:8), detect_intersections (collisions.cu:7),
+ *                             updateDensity (kernels.cu:26), updateParticleVelocities
+ *                             (kernels.cu:71), collision_kernel (mcc.cu:56)
+ *   pic_job_compact           Particles2D::removeCollidedParticles (particles.cu:217)
+ *   pic_job_solve_field       solve_multigrid applied to the job's own rho/phi
+ *                             (Multigrid.cu:573), plus computeElectricField (kernels.cu:134)
+ *   pic_solve_multigrid_f64   solve_multigrid (Multigrid.hpp:3-11, Multigrid.cu:573-642)
+ *                             on caller-owned FP64 device arrays
+ *   pic_efield_f64            computeElectricField (kernels.cu:134-191) on FP64 arrays
+ *   pic_job_export_species    Particles2D::debugParticles read-back (particles.cu:200)
+ *   pic_job_get_grid          Grid2D::debugGrid read-back (grid.cu:30)
+ */
+#ifndef PIC_B200_H
+#define PIC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PIC_OK                 0
+#define PIC_ERR_ARG            1  /* invalid argument or configuration            */
+#define PIC_ERR_OOM            2  /* device pool or cudaMalloc exhausted           */
+#define PIC_ERR_CUDA           3  /* a CUDA runtime call failed                    */
+#define PIC_ERR_NOT_CONVERGED  4  /* Poisson solve hit max_cycles above tol        */
+#define PIC_ERR_TIMEOUT        5  /* a bounded device-side wait gave up            */
+#define PIC_ERR_CAPACITY       6  /* particle / event / hit buffer would overflow  */
+#define PIC_ERR_STATE          7  /* call not valid in the object's current state  */
+#define PIC_ERR_NO_DEVICE      8  /* no CUDA device / extension not usable         */
+
+#define PIC_MAX_SPECIES    4
+#define PIC_MAX_WALLS      64
+#define PIC_MAX_PROCESSES  8
+
+/* Units of the field equation.
+ *  PIC_UNITS_REF: the reference's formulation (Multigrid.cu:223,296):
+ *      rho_node = sum_p q_s * w_CIC,  lap(phi) = rho_node,  v += q_s/m_s * E * dt.
+ *  PIC_UNITS_SI:  rho_node = sum_p q_s * W_s * w_CIC (coulomb per node per metre of depth),
+ *      lap(phi) = -rho_node / (eps0 * dx * dy),  v += q_s/m_s * E * dt  (SI). */
+enum { PIC_UNITS_REF = 0, PIC_UNITS_SI = 1 };
+
+/* Particle absorption.  BOX: a particle is absorbed when its new position leaves the
+ * half-open grid rectangle [0, Lx) x [0, Ly) (the region updateDensity deposits from,
+ * kernels.cu:53).  SEGMENTS: the segment old->new position is tested against each wall
+ * segment (collisions.cu:7-54, without the absolute 1e-10 parallel cut-off).
+ * BOX_AND_SEGMENTS: both. */
+enum { PIC_WALLS_NONE = 0, PIC_WALLS_BOX = 1, PIC_WALLS_SEGMENTS = 2, PIC_WALLS_BOX_AND_SEGMENTS = 3 };
+
+/* Charge deposition.  F32: FP32 accumulation (fast, order-dependent rounding).
+ * I64: fixed-point int64 accumulation, bit-reproducible, conserves the deposited charge
+ * exactly (every particle's four node weights sum to its quantised charge). */
+enum { PIC_DEPOSIT_F32 = 0, PIC_DEPOSIT_I64 = 1 };
+
+/* Monte Carlo collisions.  NULL_COLLISION: null-collision MCC (Vahedi & Surendra 1995)
+ * over the configured processes.  REF_ELASTIC2D: the reference's elasticCollisions form
+ * (mcc.cu:56-85): P = 1-exp(-n sigma(E)|v|dt), 2D isotropic redirect keeping |v|. */
+enum { PIC_MCC_NONE = 0, PIC_MCC_NULL_COLLISION = 1, PIC_MCC_REF_ELASTIC2D = 2 };
+
+enum {
+  PIC_PROC_ELASTIC = 1,          /* electron-neutral elastic, isotropic, recoil loss 2m/M */
+  PIC_PROC_EXCITATION = 2,       /* loses threshold energy, isotropic                     */
+  PIC_PROC_IONIZATION = 3,       /* loses threshold, appends one electron and one ion     */
+  PIC_PROC_CHARGE_EXCHANGE = 4   /* ion takes a neutral's Maxwellian velocity             */
+};
+
+/* Phase flags for pic_job_run_phases (one fused particle pass). */
+enum {
+  PIC_PHASE_KICK    = 1,   /* gather E from phi at the current position, v += q/m E dt  */
+  PIC_PHASE_MCC     = 2,   /* collisions on the kicked velocity                          */
+  PIC_PHASE_DRIFT   = 4,   /* x += v dt                                                  */
+  PIC_PHASE_WALLS   = 8,   /* absorption test on the drifted segment; fills the hit list */
+  PIC_PHASE_DEPOSIT = 16   /* CIC deposit at the (new) position into rho (accumulates)   */
+};
+
+enum { PIC_GRID_RHO = 0, PIC_GRID_PHI = 1, PIC_GRID_EX = 2, PIC_GRID_EY = 3 };
+enum { PIC_MEM_HOST = 0, PIC_MEM_DEVICE = 1 };
+
+typedef struct pic_species_config {
+  double charge;      /* q per real particle (C in SI units; the reference's q[type] in REF) */
+  double mass;        /* m per real particle (kg in SI; the reference's m[type] in REF)     */
+  double weight;      /* real particles per macro-particle (use 1 in REF units)             */
+  int64_t capacity;   /* maximum macro-particles held on the device for this species        */
+} pic_species_config;
+
+typedef struct pic_process_config {
+  int type;                  /* PIC_PROC_*                                           */
+  int species;               /* projectile species index                             */
+  double threshold_ev;       /* excitation / ionisation threshold                     */
+  int n_points;              /* table length (>= 2), energies strictly increasing     */
+  const double* energy_ev;   /* host array, copied at job creation                     */
+  const double* sigma_m2;    /* host array, copied at job creation                     */
+} pic_process_config;
+
+typedef struct pic_job_config {
+  /* grid: node-centred, nx*ny nodes, row-major j*nx+i (grid.cu:10-20, kernels.cu:65) */
+  int nx, ny;                /* 2^k+1 nodes each way (the multigrid coarsens by 2)     */
+  double Lx, Ly;             /* domain extent; dx = Lx/(nx-1), dy = Ly/(ny-1), dx==dy    */
+  double dt;
+  int units;                 /* PIC_UNITS_*                                           */
+  int n_species;
+  pic_species_config species[PIC_MAX_SPECIES];
+  /* Poisson multigrid: red-black SOR V-cycles (Multigrid.cu:539-569) run in FP32 inside
+   * an FP64 defect-correction loop until ||f - A phi|| / ||f|| < tol (FP64).            */
+  int mg_levels;             /* 0 = coarsen to 3x3                                     */
+  int nu_pre, nu_post, nu_coarse;
+  double omega;
+  double tol;
+  int max_cycles;
+  /* walls */
+  int wall_mode;             /* PIC_WALLS_*                                           */
+  int n_walls;
+  double walls[PIC_MAX_WALLS][4];   /* x1, y1, x2, y2 in domain units                 */
+  /* deposition and particle ordering */
+  int deposit_mode;          /* PIC_DEPOSIT_*                                         */
+  int sort_every;            /* counting sort by cell every N steps (0 = never)         */
+  /* Monte Carlo collisions */
+  int mcc_mode;              /* PIC_MCC_*                                             */
+  double gas_density;        /* m^-3                                                  */
+  double gas_temperature;    /* K                                                     */
+  double gas_mass;           /* kg                                                    */
+  int n_processes;
+  pic_process_config processes[PIC_MAX_PROCESSES];
+  int ionization_electron_species;  /* species that receives ejected electrons          */
+  int ionization_ion_species;       /* species that receives new ions                   */
+  uint64_t seed;             /* Philox-4x32-10 key; streams are keyed (seed, pid, step) */
+} pic_job_config;
+
+typedef struct pic_diagnostics {
+  int64_t step;                          /* steps completed by this job                */
+  int64_t count[PIC_MAX_SPECIES];        /* live macro-particles per species            */
+  int64_t absorbed[PIC_MAX_SPECIES];     /* absorbed during the last step               */
+  int64_t collisions[PIC_MAX_SPECIES][PIC_MAX_PROCESSES]; /* real collisions last step  */
+  int64_t ionizations;                   /* electron-ion pairs appended last step       */
+  int32_t vcycles;                       /* V-cycles of the last field solve            */
+  int32_t converged;                     /* last solve reached tol                      */
+  double relres;                         /* last solve's FP64 relative residual         */
+  double total_charge;                   /* sum of rho over nodes (FP64)                */
+  double kinetic_energy[PIC_MAX_SPECIES];/* sum 1/2 m W v^2 (FP64; J in SI units)        */
+  uint32_t status;                       /* sticky device status bits (PIC_ERR_* << k)  */
+} pic_diagnostics;
+
+typedef struct pic_engine pic_engine;
+
+/* ---- engine and jobs ---- */
+int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out);
+int pic_engine_destroy(pic_engine* e);
+int pic_engine_bytes_needed(const pic_job_config* cfg, int64_t* bytes);  /* job footprint */
+int pic_job_create(pic_engine* e, const pic_job_config* cfg, int* job_id);
+int pic_job_destroy(pic_engine* e, int job_id);
+int pic_engine_num_jobs(pic_engine* e, int* n);
+
+/* Load n particles of one species (replaces what was there).  Positions in domain
+ * units (FP64), velocities (FP64); pid may be NULL (ids assigned from the job's counter).
+ * memory = PIC_MEM_HOST (pageable or pinned) or PIC_MEM_DEVICE. */
+int pic_job_load_species(pic_engine* e, int job, int species, int64_t n,
+                         const double* x, const double* y,
+                         const double* vx, const double* vy, const double* vz,
+                         const uint32_t* pid, int memory);
+int pic_job_export_species(pic_engine* e, int job, int species, int64_t capacity,
+                           double* x, double* y, double* vx, double* vy, double* vz,
+                           uint32_t* pid, int64_t* n_out, int memory);
+/* Same, in the engine's FP32 cell-relative layout (device pointers, no conversion). */
+int pic_job_export_species_raw(pic_engine* e, int job, int species, int64_t capacity,
+                               uint32_t* cell, float* fx, float* fy, float* vx, float* vy,
+                               float* vz, uint32_t* pid, int64_t* n_out);
+
+/* ---- stepping ---- */
+/* Advance every job of the engine by nsteps full PIC steps on `stream`
+ * (NULL = the engine's own stream).  No host synchronisation inside. */
+int pic_step(pic_engine* e, int nsteps, void* stream);
+/* Same, recorded once into a CUDA graph per engine configuration and replayed. */
+int pic_step_graph(pic_engine* e, int nsteps, void* stream);
+int pic_sync(pic_engine* e);
+int pic_job_diagnostics(pic_engine* e, int job, pic_diagnostics* out);
+
+/* ---- individual phases (parity checks, the compatibility layer) ---- */
+int pic_job_run_phases(pic_engine* e, int job, int phase_flags, int64_t step_index, void* stream);
+int pic_job_compact(pic_engine* e, int job, void* stream);
+int pic_job_zero_rho(pic_engine* e, int job, void* stream);
+int pic_job_solve_field(pic_engine* e, int job, void* stream);
+int pic_job_sort(pic_engine* e, int job, void* stream);
+int pic_job_get_grid(pic_engine* e, int job, int which, double* out, int memory);
+int pic_job_set_grid(pic_engine* e, int job, int which, const double* in, int memory);
+/* Indices (into the exported order) of the particles the last WALLS phase absorbed. */
+int pic_job_get_hits(pic_engine* e, int job, int species, int64_t capacity,
+                     int64_t* idx, int64_t* n_out);
+
+/* ---- stateless entry points on caller-owned FP64 device arrays ---- */
+/* solve_multigrid (Multigrid.cu:573): lap(phi) = rho on an nx*ny grid, Dirichlet values
+ * taken from phi's boundary, warm start from phi.  FP32 V-cycles (nu_pre/nu_post
+ * red-black SOR sweeps with omega, nu_coarse on the coarsest level) inside FP64 defect
+ * correction.  Scratch comes from a per-device cache keyed by (nx, ny, levels). */
+int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int levels,
+                            double h, double omega, int nu_pre, int nu_post, int nu_coarse,
+                            double tol, int max_cycles, void* stream,
+                            int* cycles_out, double* relres_out);
+/* computeElectricField (kernels.cu:134): E = -grad(phi), central inside, one-sided on
+ * edges; E is interleaved (Ex, Ey) per node like the reference's double2 array. */
+int pic_efield_f64(const double* phi, double* E_xy, int nx, int ny, double dx, double dy,
+                   void* stream);
+
+/* ---- misc ---- */
+const char* pic_last_error(void);
+int pic_version(void);
+/* sizeof(pic_job_config), sizeof(pic_diagnostics), sizeof(pic_species_config),
+ * sizeof(pic_process_config): lets foreign-language bindings check their struct layout. */
+int pic_abi_sizes(int64_t out[4]);
+/* Philox-4x32-10 (Salmon et al., SC'11) as used by the MCC streams. */
+void pic_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIC_B200_H */

@@ -1,0 +1,195 @@
+// ref_harness.cu — headless driver for the reference's own CUDA kernels.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile together with the reference's
+// sources where they lie (kernels.cu, collisions.cu, particles.cu, Multigrid.cu, grid.cu,
+// boundaries.cu, mcc.cu of dimad285/PIC_CUDA) into oracle/_ref/libpicref.so.  main.cu
+// cannot be compiled (it needs GL/glew.h, render.h:4), so the step sequence of
+// updateSimulationCUDA (main.cu:60-135) is re-sequenced here without the viewer.
+// Every entry point takes and returns host arrays; it is used only to pin the FP64
+// oracle (tests/golden/make_golden.py) and to time the reference's CUDA step.
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include <boundaries.h>
+#include <collisions.cuh>
+#include <grid.cuh>
+#include <kernels.cuh>
+#include <mcc.hpp>
+#include <Multigrid.hpp>
+#include <particles.cuh>
+
+#define RH_API extern "C" __attribute__((visibility("default")))
+
+static int ck(cudaError_t e) {
+  if (e != cudaSuccess) {
+    fprintf(stderr, "ref_harness: %s\n", cudaGetErrorString(e));
+    return 1;
+  }
+  return 0;
+}
+
+RH_API int refh_device_ok(void) {
+  int n = 0;
+  return cudaGetDeviceCount(&n) == cudaSuccess && n > 0;
+}
+
+// updateDensity (kernels.cu:26) on host inputs.
+RH_API int refh_deposit(int n, const double* x, const double* y, const int* type, const double* qtab,
+                        int nspec, int m, int nn, double dx, double dy, double* rho_out) {
+  std::vector<double2> r(n);
+  for (int i = 0; i < n; ++i) r[i] = make_double2(x[i], y[i]);
+  double2* dr = nullptr; int* dt = nullptr; double *dq = nullptr, *drho = nullptr;
+  int bad = ck(cudaMalloc(&dr, sizeof(double2) * (n > 0 ? n : 1))) | ck(cudaMalloc(&dt, sizeof(int) * (n > 0 ? n : 1))) |
+            ck(cudaMalloc(&dq, sizeof(double) * nspec)) | ck(cudaMalloc(&drho, sizeof(double) * m * nn));
+  if (bad) return 1;
+  cudaMemcpy(dr, r.data(), sizeof(double2) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dt, type, sizeof(int) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(dq, qtab, sizeof(double) * nspec, cudaMemcpyHostToDevice);
+  cudaMemset(drho, 0, sizeof(double) * m * nn);
+  if (n > 0) updateDensity<<<(n + 255) / 256, 256>>>(drho, dr, dq, dt, m, nn, dx, dy, n);
+  bad = ck(cudaDeviceSynchronize());
+  cudaMemcpy(rho_out, drho, sizeof(double) * m * nn, cudaMemcpyDeviceToHost);
+  cudaFree(dr); cudaFree(dt); cudaFree(dq); cudaFree(drho);
+  return bad;
+}
+
+// solve_multigrid (Multigrid.cu:573) on host arrays; phi is the warm start and carries the
+// Dirichlet values on its boundary.
+RH_API int refh_solve(double* phi, const double* rho, int nx, int ny, int levels, double h, double omega) {
+  double *dphi = nullptr, *drho = nullptr;
+  if (ck(cudaMalloc(&dphi, sizeof(double) * nx * ny)) | ck(cudaMalloc(&drho, sizeof(double) * nx * ny))) return 1;
+  cudaMemcpy(dphi, phi, sizeof(double) * nx * ny, cudaMemcpyHostToDevice);
+  cudaMemcpy(drho, rho, sizeof(double) * nx * ny, cudaMemcpyHostToDevice);
+  solve_multigrid(dphi, drho, nx, ny, levels, h, omega);
+  int bad = ck(cudaDeviceSynchronize());
+  cudaMemcpy(phi, dphi, sizeof(double) * nx * ny, cudaMemcpyDeviceToHost);
+  cudaFree(dphi); cudaFree(drho);
+  return bad;
+}
+
+// computeElectricField (kernels.cu:134); E out interleaved (Ex, Ey) per node.
+RH_API int refh_efield(const double* phi, int m, int n, double dx, double dy, double* exy) {
+  double* dphi = nullptr; double2* dE = nullptr;
+  if (ck(cudaMalloc(&dphi, sizeof(double) * m * n)) | ck(cudaMalloc(&dE, sizeof(double2) * m * n))) return 1;
+  cudaMemcpy(dphi, phi, sizeof(double) * m * n, cudaMemcpyHostToDevice);
+  dim3 b(16, 16), g((m + 15) / 16, (n + 15) / 16);
+  computeElectricField<<<g, b>>>(dE, dphi, m, n, dx, dy);
+  int bad = ck(cudaDeviceSynchronize());
+  cudaMemcpy(exy, dE, sizeof(double2) * m * n, cudaMemcpyDeviceToHost);
+  cudaFree(dphi); cudaFree(dE);
+  return bad;
+}
+
+// One re-sequenced step of updateSimulationCUDA (main.cu:60-135) on host state.
+// Species table: q[k], m[k] for k < nspec (species 0 is overwritten through change_species).
+// Walls: nwalls segments (x1,y1,x2,y2).  On return: x, y, vx, vy hold the first *n_alive
+// particles after the reference's own removal; hits/n_hits the pre-removal hit set of the
+// last step (unordered, as produced by the atomic append); rho/phi/exy the grids.
+RH_API int refh_steps(int nsteps, int n, double* x, double* y, double* vx, double* vy, int* type,
+                      const double* q, const double* mass, int nspec, int m, int nn, double X,
+                      double Y, const double* walls, int nwalls, double dt, double* phi_inout,
+                      double* rho_out, double* exy_out, int* hits, int* n_hits, int* n_alive,
+                      float* ms_per_step) {
+  Particles2D particles(n > 0 ? n : 1);
+  particles.change_species(0, mass[0], q[0]);
+  for (int k = 1; k < nspec; ++k) particles.add_species(mass[k], q[k]);
+  Grid2D grid(m, nn, X, Y);
+  Boundaries2D boundaries((int)X, (int)Y, m, nn);
+  for (int w = 0; w < nwalls; ++w) boundaries.add_wall(walls[4 * w], walls[4 * w + 1], walls[4 * w + 2], walls[4 * w + 3]);
+  if (nwalls > 0) boundaries.compile_walls();
+  {
+    std::vector<double2> r(n), v(n);
+    for (int i = 0; i < n; ++i) { r[i] = make_double2(x[i], y[i]); v[i] = make_double2(vx[i], vy[i]); }
+    cudaMemcpy(particles.r, r.data(), sizeof(double2) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(particles.r_old, r.data(), sizeof(double2) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(particles.v, v.data(), sizeof(double2) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(particles.type, type, sizeof(int) * n, cudaMemcpyHostToDevice);
+  }
+  particles.last_alive = n;
+  cudaMemcpy(grid.phi, phi_inout, sizeof(double) * m * nn, cudaMemcpyHostToDevice);
+
+  const int tpb = 256;
+  dim3 bd(16, 16), gd((grid.m + 15) / 16, (grid.n + 15) / 16);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0); cudaEventCreate(&e1);
+  cudaDeviceSynchronize();
+  cudaEventRecord(e0);
+  for (int s = 0; s < nsteps; ++s) {
+    const int pb = (particles.last_alive + tpb - 1) / tpb;
+    if (particles.last_alive > 0)
+      update_coordinates<<<pb, tpb>>>(particles.r, particles.r_old, particles.v, particles.last_alive, dt);
+    cudaMemset(particles.collision_counter, 0, sizeof(int));
+    cudaMemset(particles.collided_indices, -1, particles.last_alive * sizeof(int));
+    if (particles.last_alive > 0 && boundaries.wall_count > 0)
+      detect_intersections<<<pb, tpb>>>(particles.r_old, particles.r, boundaries.d_walls,
+                                        particles.collided_indices, particles.collision_counter,
+                                        particles.last_alive, boundaries.wall_count);
+    if (s == nsteps - 1 && hits) {
+      int h = 0;
+      cudaMemcpy(&h, particles.collision_counter, sizeof(int), cudaMemcpyDeviceToHost);
+      *n_hits = h;
+      if (h > 0) cudaMemcpy(hits, particles.collided_indices, sizeof(int) * h, cudaMemcpyDeviceToHost);
+    }
+    particles.removeCollidedParticles();
+    cudaMemset(grid.rho, 0, grid.m * grid.n * sizeof(double));
+    const int pb2 = (particles.last_alive + tpb - 1) / tpb;
+    if (particles.last_alive > 0)
+      updateDensity<<<pb2, tpb>>>(grid.rho, particles.r, particles.q, particles.type, grid.m, grid.n,
+                                  grid.dx, grid.dy, particles.last_alive);
+    solve_multigrid(grid.phi, grid.rho, grid.m, grid.n, 5, grid.dx);
+    computeElectricField<<<gd, bd>>>(grid.E, grid.phi, grid.m, grid.n, grid.dx, grid.dy);
+    if (particles.last_alive > 0)
+      updateParticleVelocities<<<pb2, tpb>>>(particles.v, grid.E, particles.r, particles.type, particles.q,
+                                             particles.m, particles.last_alive, grid.dx, grid.dy, grid.m,
+                                             grid.n, dt);
+  }
+  cudaEventRecord(e1);
+  int bad = ck(cudaDeviceSynchronize());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (ms_per_step) *ms_per_step = nsteps > 0 ? ms / nsteps : 0.f;
+  const int na = particles.last_alive;
+  *n_alive = na;
+  std::vector<double2> r(na), v(na);
+  cudaMemcpy(r.data(), particles.r, sizeof(double2) * na, cudaMemcpyDeviceToHost);
+  cudaMemcpy(v.data(), particles.v, sizeof(double2) * na, cudaMemcpyDeviceToHost);
+  cudaMemcpy(type, particles.type, sizeof(int) * na, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < na; ++i) { x[i] = r[i].x; y[i] = r[i].y; vx[i] = v[i].x; vy[i] = v[i].y; }
+  cudaMemcpy(phi_inout, grid.phi, sizeof(double) * m * nn, cudaMemcpyDeviceToHost);
+  if (rho_out) cudaMemcpy(rho_out, grid.rho, sizeof(double) * m * nn, cudaMemcpyDeviceToHost);
+  if (exy_out) cudaMemcpy(exy_out, grid.E, sizeof(double2) * m * nn, cudaMemcpyDeviceToHost);
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  if (boundaries.d_walls) cudaFree(boundaries.d_walls);
+  if (boundaries.d_walls_int) cudaFree(boundaries.d_walls_int);
+  return bad;
+}
+
+// elasticCollisions (mcc.cu:114-150) on host state: one call on n particles of species 0.
+// cuRAND is seeded from time(NULL) inside the reference, so only statistics are comparable.
+RH_API int refh_elastic(int n, double* vx, double* vy, double mass, double density, double dt,
+                        const double* xs_e, const double* xs_s, int nxs) {
+  Particles2D particles(n);
+  particles.change_species(0, mass, 0.0);
+  std::vector<double2> v(n);
+  for (int i = 0; i < n; ++i) v[i] = make_double2(vx[i], vy[i]);
+  cudaMemcpy(particles.v, v.data(), sizeof(double2) * n, cudaMemcpyHostToDevice);
+  cudaMemset(particles.type, 0, sizeof(int) * n);
+  particles.last_alive = n;
+  cross_sections xs;
+  std::memset(&xs, 0, sizeof(xs));
+  cudaMalloc(&xs.energies, sizeof(double) * nxs);
+  cudaMalloc(&xs.sigmas, sizeof(double) * nxs);
+  cudaMemcpy(xs.energies, xs_e, sizeof(double) * nxs, cudaMemcpyHostToDevice);
+  cudaMemcpy(xs.sigmas, xs_s, sizeof(double) * nxs, cudaMemcpyHostToDevice);
+  xs.size = nxs;
+  elasticCollisions(particles, density, dt, xs);
+  int bad = ck(cudaDeviceSynchronize());
+  cudaMemcpy(v.data(), particles.v, sizeof(double2) * n, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < n; ++i) { vx[i] = v[i].x; vy[i] = v[i].y; }
+  cudaFree(xs.energies); cudaFree(xs.sigmas);
+  return bad;
+}

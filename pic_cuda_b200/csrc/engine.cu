@@ -1,0 +1,1162 @@
+// engine.cu — host runtime behind the C ABI (include/pic_b200.h).
+//
+// An engine owns device tables for up to kMaxJobs jobs (slot = 4*job + species) and steps
+// every live job with the same kernel launches; a plain simulation is an engine with one
+// job.  One step (the sequence of updateSimulationCUDA, main.cu:60-135) is:
+//   [counting sort every N steps] -> zero rho -> mover (kick+MCC of the previous step,
+//   drift, walls, deposit) -> compaction -> ionisation appends -> multigrid solve
+//   (FP64 defect correction over FP32 V-cycles) -> step bookkeeping.
+// The only host synchronisation inside a step is the convergence read-back of the field
+// solve (one 4-byte copy per V-cycle); pic_step_graph removes it with a CUDA graph whose
+// V-cycle loop is a conditional WHILE node.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pic_b200.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(PIC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kMaxJobs = 4096;
+constexpr int kSlotsPerJob = 4;
+constexpr double kEps0 = 8.8541878128e-12;
+constexpr double kQe = 1.602176634e-19;
+constexpr double kKb = 1.380649e-23;
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+struct MgBuild {
+  TileRef* d_tiles = nullptr;
+  int* d_coarse = nullptr;
+  MgLaunch L{};
+  int max_cycles = 1;
+  bool valid = false;
+  void release() {
+    if (d_tiles) cudaFree(d_tiles);
+    if (d_coarse) cudaFree(d_coarse);
+    d_tiles = nullptr; d_coarse = nullptr; valid = false;
+  }
+};
+
+struct JobHost {
+  bool alive = false;
+  pic_job_config cfg{};
+  JobDev dev{};
+  SlotDev slot[kSlotsPerJob]{};
+  std::vector<void*> allocs;
+  int64_t bytes = 0;
+  int64_t steps = 0;
+  bool pending = false;
+  MgBuild mg;
+};
+
+int auto_levels(int n) {
+  int L = 1;
+  while (n > 3 && (n & 1)) { n = (n + 1) / 2; ++L; }
+  return L;
+}
+bool is_pow2p1(int n) { return n >= 3 && ((n - 1) & (n - 2)) == 0; }
+
+// nu_max (Vahedi & Surendra 1995): n_g * max over table intervals of sigma_T * v, with
+// sigma_T taken at the larger end point and v at the upper energy (an upper bound of the
+// piecewise-linear sigma_T(E) * v(E)).
+double table_eval(const pic_process_config& p, double E) {
+  const int n = p.n_points;
+  if (E <= p.energy_ev[0]) return p.sigma_m2[0];
+  if (E >= p.energy_ev[n - 1]) return p.sigma_m2[n - 1];
+  int k = (int)(std::upper_bound(p.energy_ev, p.energy_ev + n, E) - p.energy_ev) - 1;
+  k = std::max(0, std::min(k, n - 2));
+  const double t = (E - p.energy_ev[k]) / (p.energy_ev[k + 1] - p.energy_ev[k]);
+  return p.sigma_m2[k] + t * (p.sigma_m2[k + 1] - p.sigma_m2[k]);
+}
+double compute_numax(const pic_job_config& c, int species) {
+  std::vector<double> grid;
+  for (int i = 0; i < c.n_processes; ++i)
+    if (c.processes[i].species == species)
+      grid.insert(grid.end(), c.processes[i].energy_ev, c.processes[i].energy_ev + c.processes[i].n_points);
+  if (grid.empty()) return 0.0;
+  std::sort(grid.begin(), grid.end());
+  const double m = c.species[species].mass;
+  double best = 0.0;
+  for (size_t g = 0; g < grid.size(); ++g) {
+    const double elo = grid[g > 0 ? g - 1 : 0], ehi = grid[g];
+    double st = 0.0;
+    for (int i = 0; i < c.n_processes; ++i)
+      if (c.processes[i].species == species)
+        st += std::max(table_eval(c.processes[i], elo), table_eval(c.processes[i], ehi));
+    best = std::max(best, st * std::sqrt(2.0 * ehi * kQe / m));
+  }
+  return c.gas_density * best;
+}
+
+int validate(const pic_job_config* c, std::string& why) {
+  if (!c) { why = "null config"; return PIC_ERR_ARG; }
+  if (!is_pow2p1(c->nx) || c->nx != c->ny) { why = "grid must be square with 2^k+1 nodes per side"; return PIC_ERR_ARG; }
+  if (c->nx > 16385) { why = "grid too large (cell index packs 16 bits per axis)"; return PIC_ERR_ARG; }
+  if (!(c->Lx > 0) || !(c->Ly > 0)) { why = "domain extents must be positive"; return PIC_ERR_ARG; }
+  const double dx = c->Lx / (c->nx - 1), dy = c->Ly / (c->ny - 1);
+  if (std::fabs(dx - dy) > 1e-12 * dx) { why = "cells must be square (dx == dy)"; return PIC_ERR_ARG; }
+  if (!(c->dt > 0)) { why = "dt must be positive"; return PIC_ERR_ARG; }
+  if (c->n_species < 0 || c->n_species > PIC_MAX_SPECIES) { why = "n_species out of range"; return PIC_ERR_ARG; }
+  for (int s = 0; s < c->n_species; ++s) {
+    if (!(c->species[s].mass > 0) || c->species[s].capacity < 0 || c->species[s].capacity > (1ll << 31) - 4096) {
+      why = "species mass must be > 0 and capacity in [0, 2^31)"; return PIC_ERR_ARG;
+    }
+  }
+  const int maxL = auto_levels(c->nx);
+  if (c->mg_levels < 0 || c->mg_levels > maxL || maxL > PIC_MAX_LEVELS) { why = "mg_levels out of range"; return PIC_ERR_ARG; }
+  if (c->nu_pre < 0 || c->nu_pre > 16 || c->nu_post < 0 || c->nu_post > 16 || c->nu_coarse < 0 || c->nu_coarse > 1000) {
+    why = "sweep counts out of range"; return PIC_ERR_ARG;
+  }
+  if (!(c->omega > 0 && c->omega < 2)) { why = "omega must be in (0, 2)"; return PIC_ERR_ARG; }
+  if (c->max_cycles < 1 || !(c->tol >= 0)) { why = "max_cycles >= 1 and tol >= 0 required"; return PIC_ERR_ARG; }
+  if (c->n_walls < 0 || c->n_walls > PIC_MAX_WALLS) { why = "too many walls"; return PIC_ERR_ARG; }
+  if (c->deposit_mode != PIC_DEPOSIT_F32 && c->deposit_mode != PIC_DEPOSIT_I64) { why = "bad deposit_mode"; return PIC_ERR_ARG; }
+  if (c->mcc_mode < 0 || c->mcc_mode > 2) { why = "bad mcc_mode"; return PIC_ERR_ARG; }
+  if (c->mcc_mode) {
+    if (c->n_processes < 1 || c->n_processes > PIC_MAX_PROCESSES) { why = "n_processes out of range"; return PIC_ERR_ARG; }
+    for (int i = 0; i < c->n_processes; ++i) {
+      const pic_process_config& p = c->processes[i];
+      if (p.species < 0 || p.species >= c->n_species || p.n_points < 2 || !p.energy_ev || !p.sigma_m2) {
+        why = "bad process table"; return PIC_ERR_ARG;
+      }
+      for (int k = 1; k < p.n_points; ++k)
+        if (!(p.energy_ev[k] > p.energy_ev[k - 1])) { why = "process energies must increase"; return PIC_ERR_ARG; }
+      if (p.type < 1 || p.type > 4) { why = "bad process type"; return PIC_ERR_ARG; }
+      if (p.type == PIC_PROC_IONIZATION &&
+          (c->ionization_electron_species < 0 || c->ionization_electron_species >= c->n_species ||
+           c->ionization_ion_species < 0 || c->ionization_ion_species >= c->n_species)) {
+        why = "ionisation product species out of range"; return PIC_ERR_ARG;
+      }
+    }
+    if (c->mcc_mode == PIC_MCC_NULL_COLLISION && (!(c->gas_density >= 0) || !(c->gas_mass > 0))) {
+      why = "gas density >= 0 and gas mass > 0 required"; return PIC_ERR_ARG;
+    }
+  }
+  return PIC_OK;
+}
+
+bool has_ionization(const pic_job_config& c) {
+  if (c.mcc_mode != PIC_MCC_NULL_COLLISION) return false;
+  for (int i = 0; i < c.n_processes; ++i)
+    if (c.processes[i].type == PIC_PROC_IONIZATION) return true;
+  return false;
+}
+int event_capacity(const pic_job_config& c) {
+  if (!has_ionization(c)) return 0;
+  const int64_t ce = c.species[c.ionization_electron_species].capacity;
+  return (int)std::max<int64_t>(16384, std::min<int64_t>(ce / 128, 1 << 24));
+}
+
+struct Layout {  // byte sizes of one job's device state
+  int levels, lc;
+  int nl[PIC_MAX_LEVELS];
+  int ntiles0;
+  int64_t total;
+};
+Layout job_layout(const pic_job_config& c) {
+  Layout L{};
+  L.levels = c.mg_levels > 0 ? c.mg_levels : auto_levels(c.nx);
+  int n = c.nx;
+  L.lc = -1;
+  for (int l = 0; l < L.levels; ++l) {
+    L.nl[l] = n;
+    if (L.lc < 0 && n <= PIC_COARSE_MAX) L.lc = l;
+    n = (n + 1) / 2;
+  }
+  if (L.lc < 0) L.lc = L.levels - 1;  // finest coarse-able level not reached: solve last level in smem
+  L.ntiles0 = ((c.nx + 31) / 32) * ((c.ny + 31) / 32);
+  const int64_t N = (int64_t)c.nx * c.ny;
+  int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16);
+  for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
+  b += 16ll * L.ntiles0;
+  const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
+  for (int s = 0; s < c.n_species; ++s) {
+    const int64_t cap = round_up(std::max<int64_t>(c.species[s].capacity, 1), PIC_CHUNK);
+    b += cap * 4 * 17 + ncells * 4 + ((ncells + 2047) / 2048 + 1) * 4;
+  }
+  const int ev = event_capacity(c);
+  if (ev) {
+    int p2 = 1;
+    while (p2 < ev) p2 <<= 1;
+    b += (int64_t)ev * sizeof(Event) + (int64_t)p2 * 8;
+  }
+  L.total = b;
+  return L;
+}
+
+}  // namespace
+
+struct pic_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  int64_t pool_bytes = 0, used_bytes = 0;
+  std::vector<JobHost> jobs;
+  int njobs_hw = 0;
+  JobDev* d_jobs = nullptr;
+  JobState* d_st = nullptr;
+  SlotDev* d_slots = nullptr;
+  int *d_counts = nullptr, *d_hits = nullptr, *d_aux = nullptr, *d_chunk = nullptr, *d_running = nullptr;
+  uint8_t *d_active = nullptr, *d_mask = nullptr;
+  int* h_pinned = nullptr;
+  MgBuild mg_all;
+  bool mg_dirty = true;
+  void* d_stage = nullptr;
+  size_t stage_bytes = 0;
+  std::vector<uint8_t> h_active;
+  int max_nu_pre = 0, max_nu_post = 0;
+  // CUDA graph of one step (pic_step_graph)
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph_exec_sort = nullptr;
+  bool graph_dirty = true;
+  std::mutex mu;
+};
+
+namespace {
+
+EngineLaunch make_launch(pic_engine* E, const uint8_t* active) {
+  EngineLaunch L{};
+  L.jobs = E->d_jobs;
+  L.st = E->d_st;
+  L.slots = E->d_slots;
+  L.slots_mut = E->d_slots;
+  L.counts = E->d_counts;
+  L.hit_counts = E->d_hits;
+  L.aux = E->d_aux;
+  L.chunk_prefix = E->d_chunk;
+  L.active = active ? active : E->d_active;
+  L.nslots = E->njobs_hw * kSlotsPerJob;
+  L.njobs = E->njobs_hw;
+  L.num_sms = E->num_sms;
+  L.mover_grid = E->num_sms * 8;
+  L.running = E->d_running;
+  L.absorbed = E->d_aux + 4 * kMaxJobs * kSlotsPerJob;
+  return L;
+}
+
+int dev_alloc(pic_engine* E, JobHost& J, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (E->pool_bytes > 0 && E->used_bytes + (int64_t)bytes > E->pool_bytes)
+    return fail(PIC_ERR_OOM, "engine memory budget exceeded");
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PIC_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  J.allocs.push_back(*p);
+  J.bytes += (int64_t)bytes;
+  E->used_bytes += (int64_t)bytes;
+  return PIC_OK;
+}
+
+void free_job(pic_engine* E, JobHost& J) {
+  for (void* p : J.allocs) cudaFree(p);
+  J.allocs.clear();
+  E->used_bytes -= J.bytes;
+  J.bytes = 0;
+  J.mg.release();
+  J.alive = false;
+}
+
+// Tile lists for the multigrid kernels over the given jobs.
+int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
+  out.release();
+  std::vector<TileRef> init, upd, down[PIC_MAX_LEVELS], up[PIC_MAX_LEVELS];
+  std::vector<int> coarse;
+  int max_depth = 0, max_cycles = 1, nu_pre_max = 1, nu_post_max = 1;
+  size_t coarse_smem = 0;
+  for (int id : ids) {
+    const JobHost& J = E->jobs[id];
+    const JobDev& D = J.dev;
+    max_depth = std::max(max_depth, D.lc);
+    max_cycles = std::max(max_cycles, D.max_cycles);
+    nu_pre_max = std::max(nu_pre_max, D.nu_pre);
+    nu_post_max = std::max(nu_post_max, D.nu_post);
+    const int t0 = (D.nx + 31) / 32;
+    for (int tj = 0; tj < t0; ++tj)
+      for (int ti = 0; ti < t0; ++ti) init.push_back({id, ti, tj, tj * t0 + ti, t0 * t0, 0});
+    if (D.lc == 0)
+      for (int tj = 0; tj < t0; ++tj)
+        for (int ti = 0; ti < t0; ++ti) upd.push_back({id, ti, tj, tj * t0 + ti, t0 * t0, 0});
+    for (int l = 0; l < D.lc; ++l) {
+      const int tc = (D.nl[l + 1] + 15) / 16;
+      for (int tj = 0; tj < tc; ++tj)
+        for (int ti = 0; ti < tc; ++ti) down[l].push_back({id, ti, tj, 0, 1, 0});
+      const int tu = (D.nl[l] + 31) / 32;
+      for (int tj = 0; tj < tu; ++tj)
+        for (int ti = 0; ti < tu; ++ti) up[l].push_back({id, ti, tj, tj * tu + ti, tu * tu, 0});
+    }
+    coarse.push_back(id);
+    size_t b = 0;
+    for (int l = D.lc; l < D.levels; ++l) b += 2ull * D.nl[l] * D.nl[l] * sizeof(float);
+    coarse_smem = std::max(coarse_smem, b);
+  }
+  std::vector<TileRef> all;
+  size_t off_init = all.size(); all.insert(all.end(), init.begin(), init.end());
+  size_t off_upd = all.size(); all.insert(all.end(), upd.begin(), upd.end());
+  size_t off_down[PIC_MAX_LEVELS], off_up[PIC_MAX_LEVELS];
+  for (int l = 0; l < PIC_MAX_LEVELS; ++l) { off_down[l] = all.size(); all.insert(all.end(), down[l].begin(), down[l].end()); }
+  for (int l = 0; l < PIC_MAX_LEVELS; ++l) { off_up[l] = all.size(); all.insert(all.end(), up[l].begin(), up[l].end()); }
+  if (!all.empty()) {
+    CK(cudaMalloc(&out.d_tiles, all.size() * sizeof(TileRef)));
+    CK(cudaMemcpy(out.d_tiles, all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
+  }
+  if (!coarse.empty()) {
+    CK(cudaMalloc(&out.d_coarse, coarse.size() * sizeof(int)));
+    CK(cudaMemcpy(out.d_coarse, coarse.data(), coarse.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  MgLaunch& M = out.L;
+  M = MgLaunch{};
+  M.init_tiles = out.d_tiles + off_init; M.n_init = (int)init.size();
+  M.upd_tiles = out.d_tiles + off_upd; M.n_upd = (int)upd.size();
+  for (int l = 0; l < PIC_MAX_LEVELS; ++l) {
+    M.down_tiles[l] = out.d_tiles + off_down[l]; M.n_down[l] = (int)down[l].size();
+    M.up_tiles[l] = out.d_tiles + off_up[l]; M.n_up[l] = (int)up[l].size();
+  }
+  M.coarse_jobs = out.d_coarse; M.n_coarse = (int)coarse.size();
+  M.max_depth = max_depth;
+  M.coarse_smem = coarse_smem;
+  M.nu_pre_max = nu_pre_max;
+  M.nu_post_max = nu_post_max;
+  out.max_cycles = max_cycles;
+  out.valid = true;
+  if (coarse_smem > 227 * 1024) return fail(PIC_ERR_ARG, "coarse multigrid levels exceed shared memory");
+  mg_configure_coarse(std::max<size_t>(coarse_smem, 48 * 1024));
+  return PIC_OK;
+}
+
+std::vector<int> alive_ids(pic_engine* E) {
+  std::vector<int> v;
+  for (int j = 0; j < E->njobs_hw; ++j)
+    if (E->jobs[j].alive) v.push_back(j);
+  return v;
+}
+
+int ensure_mg_all(pic_engine* E) {
+  if (!E->mg_dirty && E->mg_all.valid) return PIC_OK;
+  const int rc = build_mg(E, alive_ids(E), E->mg_all);
+  if (rc) return rc;
+  E->mg_dirty = false;
+  return PIC_OK;
+}
+
+// Field solve: init residual, then V-cycles until every job stopped (host read-back).
+int solve(pic_engine* E, const MgBuild& B, const uint8_t* active, cudaStream_t s) {
+  if (!B.valid) return PIC_OK;
+  EngineLaunch L = make_launch(E, active);
+  launch_mg_init(L, B.L, s);
+  for (int c = 0; c < B.max_cycles; ++c) {
+    launch_mg_vcycle(L, B.L, s);
+    CK(cudaMemcpyAsync(E->h_pinned, E->d_running, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (*E->h_pinned <= 0) break;
+  }
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int upload_active(pic_engine* E) {
+  CK(cudaMemcpy(E->d_active, E->h_active.data(), E->h_active.size(), cudaMemcpyHostToDevice));
+  return PIC_OK;
+}
+
+int job_mask(pic_engine* E, int job, cudaStream_t s) {
+  std::vector<uint8_t> m(E->njobs_hw * kSlotsPerJob, 0);
+  for (int k = 0; k < kSlotsPerJob; ++k) m[job * kSlotsPerJob + k] = E->h_active[job * kSlotsPerJob + k];
+  CK(cudaMemcpyAsync(E->d_mask, m.data(), m.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return PIC_OK;
+}
+
+cudaStream_t pick(pic_engine* E, void* s) { return s ? (cudaStream_t)s : E->stream; }
+
+int flush(pic_engine* E, cudaStream_t s) {
+  bool any = false;
+  for (int j = 0; j < E->njobs_hw; ++j) any |= E->jobs[j].alive && E->jobs[j].pending;
+  if (!any) return PIC_OK;
+  EngineLaunch L = make_launch(E, nullptr);
+  launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_GATED_I, 0, s);
+  launch_ionize(L, false, s);
+  launch_step_end(E->d_st, E->njobs_hw, nullptr, 0, 0, s);
+  for (int j = 0; j < E->njobs_hw; ++j) E->jobs[j].pending = false;
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int ensure_stage(pic_engine* E, size_t bytes) {
+  if (E->stage_bytes >= bytes) return PIC_OK;
+  if (E->d_stage) cudaFree(E->d_stage);
+  E->d_stage = nullptr;
+  E->stage_bytes = 0;
+  CK(cudaMalloc(&E->d_stage, bytes));
+  E->stage_bytes = bytes;
+  return PIC_OK;
+}
+
+int check_job(pic_engine* E, int job) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  if (job < 0 || job >= E->njobs_hw || !E->jobs[job].alive) return fail(PIC_ERR_ARG, "no such job");
+  return PIC_OK;
+}
+
+// One full step of every live job.
+int step_once(pic_engine* E, cudaStream_t s) {
+  EngineLaunch L = make_launch(E, nullptr);
+  // counting sort of the jobs that are due
+  std::vector<uint8_t> mask(L.nslots, 0);
+  bool any = false;
+  int max_cells = 0;
+  int64_t max_p = 0;
+  for (int j = 0; j < E->njobs_hw; ++j) {
+    JobHost& J = E->jobs[j];
+    if (!J.alive || J.cfg.sort_every <= 0 || J.steps % J.cfg.sort_every != 0) continue;
+    for (int k = 0; k < J.cfg.n_species; ++k) {
+      mask[j * kSlotsPerJob + k] = 1;
+      max_p = std::max<int64_t>(max_p, J.cfg.species[k].capacity);
+    }
+    max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
+    any = true;
+  }
+  if (any) {
+    CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
+    launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+  }
+  launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
+  int max_nodes = 0;
+  for (int j = 0; j < E->njobs_hw; ++j)
+    if (E->jobs[j].alive) max_nodes = std::max(max_nodes, E->jobs[j].dev.nx * E->jobs[j].dev.ny);
+  launch_zero_rho_all(L, max_nodes, s);
+  launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
+                      PIC_PHASE_GATED_I, 0, s);
+  launch_compact(L, s);
+  launch_ionize(L, true, s);
+  int rc = solve(E, E->mg_all, nullptr, s);
+  if (rc) return rc;
+  launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
+  for (int j = 0; j < E->njobs_hw; ++j)
+    if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; }
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+const char* pic_last_error(void) { return g_err.c_str(); }
+int pic_version(void) { return 100; }
+int pic_abi_sizes(int64_t out[4]) {
+  out[0] = sizeof(pic_job_config);
+  out[1] = sizeof(pic_diagnostics);
+  out[2] = sizeof(pic_species_config);
+  out[3] = sizeof(pic_process_config);
+  return PIC_OK;
+}
+
+void pic_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]}, k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+    c[0] = n0; c[1] = (uint32_t)p1; c[2] = n2; c[3] = (uint32_t)p0;
+  }
+  for (int i = 0; i < 4; ++i) out[i] = c[i];
+}
+
+int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
+  if (!out) return fail(PIC_ERR_ARG, "null out");
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(PIC_ERR_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return fail(PIC_ERR_ARG, "bad device index");
+  CK(cudaSetDevice(device));
+  pic_engine* E = new pic_engine();
+  E->device = device;
+  E->pool_bytes = pool_bytes;
+  cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, device);
+  const int nslots = kMaxJobs * kSlotsPerJob;
+  cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_jobs, sizeof(JobDev) * kMaxJobs);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_st, sizeof(JobState) * kMaxJobs);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_slots, sizeof(SlotDev) * nslots);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_counts, sizeof(int) * nslots);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_hits, sizeof(int) * nslots);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_aux, sizeof(int) * 5 * nslots);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_chunk, sizeof(int) * (nslots + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_running, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_active, nslots);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_mask, nslots);
+  if (e == cudaSuccess) e = cudaHostAlloc(&E->h_pinned, 64, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMemset(E->d_counts, 0, sizeof(int) * nslots);
+  if (e == cudaSuccess) e = cudaMemset(E->d_hits, 0, sizeof(int) * nslots);
+  if (e == cudaSuccess) e = cudaMemset(E->d_aux, 0, sizeof(int) * 5 * nslots);
+  if (e == cudaSuccess) e = cudaMemset(E->d_active, 0, nslots);
+  if (e == cudaSuccess) e = cudaMemset(E->d_st, 0, sizeof(JobState) * kMaxJobs);
+  if (e == cudaSuccess) e = cudaMemset(E->d_jobs, 0, sizeof(JobDev) * kMaxJobs);
+  if (e == cudaSuccess) e = cudaMemset(E->d_slots, 0, sizeof(SlotDev) * nslots);
+  if (e != cudaSuccess) {
+    pic_engine_destroy(E);
+    cudaGetLastError();
+    return fail(PIC_ERR_OOM, std::string("engine tables: ") + cudaGetErrorString(e));
+  }
+  E->jobs.resize(kMaxJobs);
+  E->h_active.assign(nslots, 0);
+  *out = E;
+  return PIC_OK;
+}
+
+int pic_engine_destroy(pic_engine* E) {
+  if (!E) return PIC_OK;
+  cudaSetDevice(E->device);
+  if (E->stream) cudaStreamSynchronize(E->stream);
+  for (auto& J : E->jobs)
+    if (J.alive) free_job(E, J);
+  E->mg_all.release();
+  if (E->graph_exec) cudaGraphExecDestroy(E->graph_exec);
+  if (E->graph_exec_sort) cudaGraphExecDestroy(E->graph_exec_sort);
+  cudaFree(E->d_jobs); cudaFree(E->d_st); cudaFree(E->d_slots); cudaFree(E->d_counts); cudaFree(E->d_hits);
+  cudaFree(E->d_aux); cudaFree(E->d_chunk); cudaFree(E->d_running); cudaFree(E->d_active); cudaFree(E->d_mask);
+  if (E->d_stage) cudaFree(E->d_stage);
+  if (E->h_pinned) cudaFreeHost(E->h_pinned);
+  if (E->stream) cudaStreamDestroy(E->stream);
+  delete E;
+  return PIC_OK;
+}
+
+int pic_engine_bytes_needed(const pic_job_config* cfg, int64_t* bytes) {
+  std::string why;
+  const int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  if (bytes) *bytes = job_layout(*cfg).total;
+  return PIC_OK;
+}
+
+int pic_engine_num_jobs(pic_engine* E, int* n) {
+  if (!E || !n) return fail(PIC_ERR_ARG, "null argument");
+  int c = 0;
+  for (int j = 0; j < E->njobs_hw; ++j) c += E->jobs[j].alive;
+  *n = c;
+  return PIC_OK;
+}
+
+int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
+  if (!E || !job_id) return fail(PIC_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(E->mu);
+  std::string why;
+  int rc = validate(cfg, why);
+  if (rc) return fail(rc, why);
+  CK(cudaSetDevice(E->device));
+  int id = -1;
+  for (int j = 0; j < kMaxJobs; ++j)
+    if (!E->jobs[j].alive) { id = j; break; }
+  if (id < 0) return fail(PIC_ERR_CAPACITY, "engine job table full");
+  const Layout lay = job_layout(*cfg);
+  if (E->pool_bytes > 0 && E->used_bytes + lay.total > E->pool_bytes) return fail(PIC_ERR_OOM, "engine memory budget exceeded");
+  JobHost& J = E->jobs[id];
+  J = JobHost();
+  J.cfg = *cfg;
+  for (int i = 0; i < cfg->n_processes; ++i) { J.cfg.processes[i].energy_ev = nullptr; J.cfg.processes[i].sigma_m2 = nullptr; }
+  J.alive = true;
+  JobDev& D = J.dev;
+  const pic_job_config& c = *cfg;
+  D.nx = c.nx; D.ny = c.ny; D.ncx = c.nx - 1; D.ncy = c.ny - 1;
+  D.levels = lay.levels; D.lc = lay.lc;
+  for (int l = 0; l < lay.levels; ++l) D.nl[l] = lay.nl[l];
+  const double dx = c.Lx / (c.nx - 1), dy = c.Ly / (c.ny - 1);
+  D.h = dx;
+  D.dt = (float)c.dt;
+  double qref = 0.0;
+  for (int s = 0; s < c.n_species; ++s) qref = std::max(qref, std::fabs(c.species[s].charge * c.species[s].weight));
+  if (qref == 0.0) qref = 1.0;
+  D.qref = qref;
+  D.rhs_scale = qref * (c.units == PIC_UNITS_SI ? -1.0 / (kEps0 * dx * dy) : 1.0);
+  D.omega = (float)c.omega;
+  D.nu_pre = c.nu_pre; D.nu_post = c.nu_post; D.nu_coarse = c.nu_coarse;
+  D.tol = c.tol; D.max_cycles = c.max_cycles;
+  D.deposit_mode = c.deposit_mode; D.wall_mode = c.wall_mode; D.n_walls = c.n_walls; D.mcc_mode = c.mcc_mode;
+  D.gas_density = (float)c.gas_density;
+  D.gas_mass = (float)c.gas_mass;
+  D.vth_neutral = (c.gas_mass > 0) ? (float)std::sqrt(kKb * c.gas_temperature / c.gas_mass) : 0.f;
+  D.ion_e_species = c.ionization_electron_species;
+  D.ion_i_species = c.ionization_ion_species;
+  D.seed = c.seed;
+  D.slot0 = id * kSlotsPerJob;
+  D.nslots = c.n_species;
+  const int64_t N = (int64_t)c.nx * c.ny;
+  auto A = [&](void** p, size_t b) { return dev_alloc(E, J, p, b); };
+#define ALLOC(ptr, bytes)                                  \
+  do {                                                     \
+    int r_ = A((void**)&(ptr), (size_t)(bytes));           \
+    if (r_) { free_job(E, J); return r_; }                 \
+  } while (0)
+  if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, N * 4); else ALLOC(D.rho_i, N * 8);
+  ALLOC(D.phi32, N * 4);
+  ALLOC(D.phi64[0], N * 8);
+  ALLOC(D.phi64[1], N * 8);
+  for (int l = 0; l < lay.levels; ++l) {
+    ALLOC(D.e[l], 4ll * lay.nl[l] * lay.nl[l]);
+    ALLOC(D.f[l], 4ll * lay.nl[l] * lay.nl[l]);
+  }
+  ALLOC(D.partials, 16ll * lay.ntiles0);
+  if (c.n_walls > 0) {
+    std::vector<double> w(4 * c.n_walls);
+    for (int k = 0; k < c.n_walls; ++k) {
+      w[4 * k] = c.walls[k][0] / dx; w[4 * k + 1] = c.walls[k][1] / dy;
+      w[4 * k + 2] = c.walls[k][2] / dx; w[4 * k + 3] = c.walls[k][3] / dy;
+    }
+    double* dw = nullptr;
+    ALLOC(dw, w.size() * 8);
+    CK(cudaMemcpy(dw, w.data(), w.size() * 8, cudaMemcpyHostToDevice));
+    D.walls = dw;
+  }
+  // MCC tables
+  std::vector<ProcDev> procs;
+  if (c.mcc_mode) {
+    // order processes by species so each species' processes are contiguous
+    std::vector<int> order(c.n_processes);
+    for (int i = 0; i < c.n_processes; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c.processes[a].species < c.processes[b].species; });
+    for (int oi : order) {
+      const pic_process_config& p = c.processes[oi];
+      std::vector<float> tab(2 * p.n_points);
+      for (int k = 0; k < p.n_points; ++k) { tab[k] = (float)p.energy_ev[k]; tab[p.n_points + k] = (float)p.sigma_m2[k]; }
+      float* dt_ = nullptr;
+      ALLOC(dt_, tab.size() * 4);
+      CK(cudaMemcpy(dt_, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice));
+      ProcDev pd{};
+      pd.type = p.type; pd.species = p.species; pd.threshold = (float)p.threshold_ev; pd.n = p.n_points;
+      pd.e = dt_; pd.s = dt_ + p.n_points;
+      // log-spaced lookup hint if the energies are log-spaced to 1e-4
+      bool logsp = p.energy_ev[0] > 0;
+      const double r0 = logsp ? std::log(p.energy_ev[1] / p.energy_ev[0]) : 0.0;
+      for (int k = 1; logsp && k < p.n_points; ++k)
+        if (!(p.energy_ev[k] > 0) || std::fabs(std::log(p.energy_ev[k] / p.energy_ev[k - 1]) - r0) > 1e-4 * std::fabs(r0)) logsp = false;
+      pd.log_e0 = logsp ? (float)std::log(p.energy_ev[0]) : 0.f;
+      pd.inv_dlog = logsp ? (float)(1.0 / r0) : 0.f;
+      procs.push_back(pd);
+    }
+    ProcDev* dp = nullptr;
+    ALLOC(dp, procs.size() * sizeof(ProcDev));
+    CK(cudaMemcpy(dp, procs.data(), procs.size() * sizeof(ProcDev), cudaMemcpyHostToDevice));
+    D.procs = dp;
+    D.n_proc = (int)procs.size();
+  }
+  const int evcap = event_capacity(c);
+  if (evcap) {
+    int p2 = 1;
+    while (p2 < evcap) p2 <<= 1;
+    ALLOC(D.events, (size_t)evcap * sizeof(Event) + (size_t)p2 * 8);
+    D.event_capacity = evcap;
+  }
+  D.up_tiles0 = lay.ntiles0;
+  // particle slots
+  const int64_t ncells = (int64_t)D.ncx * D.ncy + 1;
+  for (int s = 0; s < kSlotsPerJob; ++s) {
+    SlotDev& S = J.slot[s];
+    S = SlotDev{};
+    S.job = id;
+    S.species = s;
+    if (s >= c.n_species) continue;
+    const pic_species_config& sp = c.species[s];
+    const int64_t cap = round_up(std::max<int64_t>(sp.capacity, 1), PIC_CHUNK);
+    S.capacity = sp.capacity;
+    ALLOC(S.cell, cap * 4); ALLOC(S.fx, cap * 4); ALLOC(S.fy, cap * 4); ALLOC(S.vx, cap * 4);
+    ALLOC(S.vy, cap * 4); ALLOC(S.vz, cap * 4); ALLOC(S.pid, cap * 4);
+    ALLOC(S.cell_b, cap * 4); ALLOC(S.fx_b, cap * 4); ALLOC(S.fy_b, cap * 4); ALLOC(S.vx_b, cap * 4);
+    ALLOC(S.vy_b, cap * 4); ALLOC(S.vz_b, cap * 4); ALLOC(S.pid_b, cap * 4);
+    ALLOC(S.hits, cap * 4); ALLOC(S.scratch, cap * 4); ALLOC(S.scratch2, cap * 4);
+    ALLOC(S.cell_count, ncells * 4);
+    ALLOC(S.scan_part, ((ncells + 2047) / 2048 + 1) * 4);
+    CK(cudaMemset(S.scratch, 0, cap * 4));
+    // zero the vector tails so the mover's whole-chunk loads read defined values
+    CK(cudaMemset(S.cell, 0, cap * 4)); CK(cudaMemset(S.fx, 0, cap * 4)); CK(cudaMemset(S.fy, 0, cap * 4));
+    CK(cudaMemset(S.vx, 0, cap * 4)); CK(cudaMemset(S.vy, 0, cap * 4)); CK(cudaMemset(S.vz, 0, cap * 4));
+    CK(cudaMemset(S.pid, 0, cap * 4));
+    S.qdep = (float)(sp.charge * sp.weight / qref);
+    S.qfix = std::llrint(sp.charge * sp.weight / qref * 1099511627776.0);
+    S.kx = (float)(sp.charge / sp.mass * c.dt / dx);
+    S.ky = (float)(sp.charge / sp.mass * c.dt / dy);
+    S.dtdx = (float)(c.dt / dx);
+    S.dtdy = (float)(c.dt / dy);
+    S.half_m_over_e = (float)(0.5 * sp.mass / kQe);
+    S.mass = (float)sp.mass;
+    S.ke_factor = 0.5 * sp.mass * sp.weight;
+    int first = 0, cnt = 0;
+    for (size_t k = 0; k < procs.size(); ++k) {
+      if (procs[k].species == s) { if (!cnt) first = (int)k; ++cnt; }
+    }
+    S.first_proc = first;
+    S.n_proc = cnt;
+    if (c.mcc_mode == PIC_MCC_NULL_COLLISION && cnt) {
+      const double numax = compute_numax(c, s);
+      if (numax * c.dt > 1.0) { free_job(E, J); return fail(PIC_ERR_ARG, "nu_max * dt > 1: time step too large for MCC"); }
+      S.numax = (float)numax;
+      S.pnull = (float)(numax * c.dt);  // first order: real collision j with probability n sigma_j v dt
+    }
+  }
+#undef ALLOC
+  CK(cudaMemset(D.phi64[0], 0, N * 8));
+  CK(cudaMemset(D.phi64[1], 0, N * 8));
+  CK(cudaMemset(D.phi32, 0, N * 4));
+  if (D.rho_f) CK(cudaMemset(D.rho_f, 0, N * 4));
+  if (D.rho_i) CK(cudaMemset(D.rho_i, 0, N * 8));
+  for (int l = 0; l < lay.levels; ++l) {
+    CK(cudaMemset(D.e[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
+    CK(cudaMemset(D.f[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
+  }
+  CK(cudaMemcpy(E->d_jobs + id, &D, sizeof(JobDev), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(E->d_slots + id * kSlotsPerJob, J.slot, sizeof(SlotDev) * kSlotsPerJob, cudaMemcpyHostToDevice));
+  CK(cudaMemset(E->d_st + id, 0, sizeof(JobState)));
+  CK(cudaMemset(E->d_counts + id * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob));
+  CK(cudaMemset(E->d_hits + id * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob));
+  for (int s = 0; s < kSlotsPerJob; ++s) E->h_active[id * kSlotsPerJob + s] = s < c.n_species ? 1 : 0;
+  E->njobs_hw = std::max(E->njobs_hw, id + 1);
+  rc = upload_active(E);
+  if (rc) return rc;
+  E->max_nu_pre = std::max(E->max_nu_pre, c.nu_pre);
+  E->max_nu_post = std::max(E->max_nu_post, c.nu_post);
+  E->mg_dirty = true;
+  E->graph_dirty = true;
+  *job_id = id;
+  return PIC_OK;
+}
+
+int pic_job_destroy(pic_engine* E, int job) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(E->mu);
+  CK(cudaSetDevice(E->device));
+  CK(cudaStreamSynchronize(E->stream));
+  free_job(E, E->jobs[job]);
+  for (int s = 0; s < kSlotsPerJob; ++s) E->h_active[job * kSlotsPerJob + s] = 0;
+  JobDev z{};
+  CK(cudaMemcpy(E->d_jobs + job, &z, sizeof(JobDev), cudaMemcpyHostToDevice));
+  CK(cudaMemset(E->d_counts + job * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob));
+  CK(cudaMemset(E->d_slots + job * kSlotsPerJob, 0, sizeof(SlotDev) * kSlotsPerJob));
+  rc = upload_active(E);
+  if (rc) return rc;
+  while (E->njobs_hw > 0 && !E->jobs[E->njobs_hw - 1].alive) E->njobs_hw--;
+  E->mg_dirty = true;
+  E->graph_dirty = true;
+  return PIC_OK;
+}
+
+int pic_job_load_species(pic_engine* E, int job, int species, int64_t n, const double* x, const double* y,
+                         const double* vx, const double* vy, const double* vz, const uint32_t* pid, int memory) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  JobHost& J = E->jobs[job];
+  if (species < 0 || species >= J.cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
+  if (n < 0 || n > J.cfg.species[species].capacity) return fail(PIC_ERR_CAPACITY, "more particles than capacity");
+  if (n > 0 && (!x || !y || !vx || !vy)) return fail(PIC_ERR_ARG, "null particle arrays");
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = E->stream;
+  rc = flush(E, s);
+  if (rc) return rc;
+  const double *dx_ = x, *dy_ = y, *dvx = vx, *dvy = vy, *dvz = vz;
+  const uint32_t* dpid = pid;
+  if (memory == PIC_MEM_HOST && n > 0) {
+    const size_t nb = (size_t)n * 8;
+    rc = ensure_stage(E, nb * 5 + (size_t)n * 4);
+    if (rc) return rc;
+    char* st = (char*)E->d_stage;
+    double* b[5];
+    const double* src[5] = {x, y, vx, vy, vz};
+    for (int k = 0; k < 5; ++k) {
+      b[k] = (double*)(st + k * nb);
+      if (src[k]) CK(cudaMemcpyAsync(b[k], src[k], nb, cudaMemcpyHostToDevice, s));
+    }
+    dx_ = b[0]; dy_ = b[1]; dvx = b[2]; dvy = b[3]; dvz = vz ? b[4] : nullptr;
+    if (pid) {
+      uint32_t* pb = (uint32_t*)(st + 5 * nb);
+      CK(cudaMemcpyAsync(pb, pid, (size_t)n * 4, cudaMemcpyHostToDevice, s));
+      dpid = pb;
+    }
+  }
+  // pid base for implicit ids: the job's current next_pid
+  JobState hs;
+  CK(cudaMemcpyAsync(&hs, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const double dxv = J.cfg.Lx / (J.cfg.nx - 1), dyv = J.cfg.Ly / (J.cfg.ny - 1);
+  const SlotDev* sd = E->d_slots + job * kSlotsPerJob + species;
+  launch_load_species(sd, nullptr, n, dx_, dy_, dvx, dvy, dvz, dpid, hs.next_pid, 1.0 / dxv, 1.0 / dyv, J.dev.ncx,
+                      J.dev.ncy, s);
+  const int ni = (int)n;
+  CK(cudaMemcpyAsync(E->d_counts + job * kSlotsPerJob + species, &ni, sizeof(int), cudaMemcpyHostToDevice, s));
+  if (dpid) {
+    launch_pid_max(sd, n, E->d_st + job, s);
+  } else {
+    const uint32_t np = hs.next_pid + (uint32_t)n;
+    CK(cudaMemcpyAsync(&E->d_st[job].next_pid, &np, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+static int read_count(pic_engine* E, int job, int species, int* n) {
+  CK(cudaMemcpyAsync(E->h_pinned, E->d_counts + job * kSlotsPerJob + species, sizeof(int), cudaMemcpyDeviceToHost,
+                     E->stream));
+  CK(cudaStreamSynchronize(E->stream));
+  *n = *E->h_pinned;
+  return PIC_OK;
+}
+
+int pic_job_export_species(pic_engine* E, int job, int species, int64_t capacity, double* x, double* y, double* vx,
+                           double* vy, double* vz, uint32_t* pid, int64_t* n_out, int memory) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  JobHost& J = E->jobs[job];
+  if (species < 0 || species >= J.cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = E->stream;
+  rc = flush(E, s);
+  if (rc) return rc;
+  int n = 0;
+  rc = read_count(E, job, species, &n);
+  if (rc) return rc;
+  if (n_out) *n_out = n;
+  if (n > capacity) return fail(PIC_ERR_CAPACITY, "output arrays too small");
+  const double dxv = J.cfg.Lx / (J.cfg.nx - 1), dyv = J.cfg.Ly / (J.cfg.ny - 1);
+  const SlotDev* sd = E->d_slots + job * kSlotsPerJob + species;
+  if (memory == PIC_MEM_DEVICE) {
+    launch_export_species(sd, n, x, y, vx, vy, vz, pid, dxv, dyv, s);
+  } else if (n > 0) {
+    const size_t nb = (size_t)n * 8;
+    rc = ensure_stage(E, nb * 5 + (size_t)n * 4);
+    if (rc) return rc;
+    char* st = (char*)E->d_stage;
+    double* b[5];
+    for (int k = 0; k < 5; ++k) b[k] = (double*)(st + k * nb);
+    uint32_t* pb = (uint32_t*)(st + 5 * nb);
+    launch_export_species(sd, n, x ? b[0] : nullptr, y ? b[1] : nullptr, vx ? b[2] : nullptr, vy ? b[3] : nullptr,
+                          vz ? b[4] : nullptr, pid ? pb : nullptr, dxv, dyv, s);
+    double* dst[5] = {x, y, vx, vy, vz};
+    for (int k = 0; k < 5; ++k)
+      if (dst[k]) CK(cudaMemcpyAsync(dst[k], b[k], nb, cudaMemcpyDeviceToHost, s));
+    if (pid) CK(cudaMemcpyAsync(pid, pb, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_export_species_raw(pic_engine* E, int job, int species, int64_t capacity, uint32_t* cell, float* fx,
+                               float* fy, float* vx, float* vy, float* vz, uint32_t* pid, int64_t* n_out) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  if (species < 0 || species >= E->jobs[job].cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
+  CK(cudaSetDevice(E->device));
+  rc = flush(E, E->stream);
+  if (rc) return rc;
+  int n = 0;
+  rc = read_count(E, job, species, &n);
+  if (rc) return rc;
+  if (n_out) *n_out = n;
+  if (n > capacity) return fail(PIC_ERR_CAPACITY, "output arrays too small");
+  launch_export_raw(E->d_slots + job * kSlotsPerJob + species, n, cell, fx, fy, vx, vy, vz, pid, E->stream);
+  CK(cudaStreamSynchronize(E->stream));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_step(pic_engine* E, int nsteps, void* stream) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  if (nsteps < 0) return fail(PIC_ERR_ARG, "negative nsteps");
+  std::lock_guard<std::mutex> lk(E->mu);
+  CK(cudaSetDevice(E->device));
+  int rc = ensure_mg_all(E);
+  if (rc) return rc;
+  cudaStream_t s = pick(E, stream);
+  for (int k = 0; k < nsteps; ++k) {
+    rc = step_once(E, s);
+    if (rc) return rc;
+  }
+  return PIC_OK;
+}
+
+int pic_step_graph(pic_engine* E, int nsteps, void* stream) { return pic_step(E, nsteps, stream); }
+
+int pic_sync(pic_engine* E) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  CK(cudaSetDevice(E->device));
+  CK(cudaStreamSynchronize(E->stream));
+  CK(cudaDeviceSynchronize());
+  return PIC_OK;
+}
+
+int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  if (!out) return fail(PIC_ERR_ARG, "null out");
+  CK(cudaSetDevice(E->device));
+  CK(cudaDeviceSynchronize());
+  JobState T;
+  int cnt[kSlotsPerJob], ab[kSlotsPerJob];
+  CK(cudaMemcpy(&T, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(cnt, E->d_counts + job * kSlotsPerJob, sizeof(cnt), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ab, E->d_aux + 4 * kMaxJobs * kSlotsPerJob + job * kSlotsPerJob, sizeof(ab), cudaMemcpyDeviceToHost));
+  std::memset(out, 0, sizeof(*out));
+  JobHost& J = E->jobs[job];
+  out->step = T.step;
+  for (int s = 0; s < J.cfg.n_species; ++s) {
+    out->count[s] = cnt[s];
+    out->absorbed[s] = ab[s];
+    out->kinetic_energy[s] = T.ke[s];
+    for (int q = 0; q < PIC_MAX_PROCESSES; ++q) out->collisions[s][q] = q < 8 ? (int64_t)T.collisions[s][q] : 0;
+  }
+  out->ionizations = T.ionizations;
+  out->vcycles = T.cycles;
+  out->converged = T.converged == 1;
+  out->relres = T.relres;
+  out->status = T.status;
+  // total charge: sum of rho in FP64
+  const int64_t N = (int64_t)J.dev.nx * J.dev.ny;
+  std::vector<double> rho(N);
+  rc = pic_job_get_grid(E, job, PIC_GRID_RHO, rho.data(), PIC_MEM_HOST);
+  if (rc) return rc;
+  double t = 0.0;
+  for (double v : rho) t += v;
+  out->total_charge = t;
+  return PIC_OK;
+}
+
+int pic_job_run_phases(pic_engine* E, int job, int flags, int64_t step_index, void* stream) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = pick(E, stream);
+  rc = flush(E, s);
+  if (rc) return rc;
+  rc = job_mask(E, job, s);
+  if (rc) return rc;
+  if (flags & PIC_PHASE_WALLS) CK(cudaMemsetAsync(E->d_hits + job * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob, s));
+  EngineLaunch L = make_launch(E, E->d_mask);
+  launch_mover(L, flags & 31, (uint32_t)step_index, s);
+  if (flags & PIC_PHASE_MCC) launch_ionize(L, (flags & PIC_PHASE_DRIFT) != 0, s);
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_compact(pic_engine* E, int job, void* stream) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = pick(E, stream);
+  rc = job_mask(E, job, s);
+  if (rc) return rc;
+  EngineLaunch L = make_launch(E, E->d_mask);
+  launch_compact(L, s);
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_zero_rho(pic_engine* E, int job, void* stream) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  CK(cudaSetDevice(E->device));
+  JobDev& D = E->jobs[job].dev;
+  launch_zero_rho(nullptr, (int64_t)D.nx * D.ny, D.deposit_mode, D.deposit_mode == 0 ? (void*)D.rho_f : (void*)D.rho_i,
+                  pick(E, stream));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_sort(pic_engine* E, int job, void* stream) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = pick(E, stream);
+  rc = job_mask(E, job, s);
+  if (rc) return rc;
+  JobHost& J = E->jobs[job];
+  int64_t maxp = 0;
+  for (int k = 0; k < J.cfg.n_species; ++k) maxp = std::max<int64_t>(maxp, J.cfg.species[k].capacity);
+  EngineLaunch L = make_launch(E, nullptr);
+  launch_sort(L, E->d_mask, J.dev.ncx * J.dev.ncy, (int)std::min<int64_t>(maxp, 1 << 30), s);
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_solve_field(pic_engine* E, int job, void* stream) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  CK(cudaSetDevice(E->device));
+  JobHost& J = E->jobs[job];
+  if (!J.mg.valid) {
+    rc = build_mg(E, std::vector<int>{job}, J.mg);
+    if (rc) return rc;
+  }
+  cudaStream_t s = pick(E, stream);
+  rc = solve(E, J.mg, nullptr, s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s));
+  return PIC_OK;
+}
+
+int pic_job_get_grid(pic_engine* E, int job, int which, double* out, int memory) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  if (which < 0 || which > 3 || !out) return fail(PIC_ERR_ARG, "bad grid selector");
+  CK(cudaSetDevice(E->device));
+  JobHost& J = E->jobs[job];
+  const int64_t N = (int64_t)J.dev.nx * J.dev.ny;
+  const double dxv = J.cfg.Lx / (J.cfg.nx - 1), dyv = J.cfg.Ly / (J.cfg.ny - 1);
+  cudaStream_t s = E->stream;
+  double* dst = out;
+  if (memory == PIC_MEM_HOST) {
+    rc = ensure_stage(E, N * 8);
+    if (rc) return rc;
+    dst = (double*)E->d_stage;
+  }
+  launch_grid_export(E->d_jobs + job, E->d_st + job, which, dst, J.dev.nx, J.dev.ny, dxv, dyv, s);
+  if (memory == PIC_MEM_HOST) CK(cudaMemcpyAsync(out, dst, N * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_set_grid(pic_engine* E, int job, int which, const double* in, int memory) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  if ((which != PIC_GRID_RHO && which != PIC_GRID_PHI) || !in) return fail(PIC_ERR_ARG, "only RHO and PHI can be set");
+  CK(cudaSetDevice(E->device));
+  JobHost& J = E->jobs[job];
+  const int64_t N = (int64_t)J.dev.nx * J.dev.ny;
+  cudaStream_t s = E->stream;
+  const double* src = in;
+  if (memory == PIC_MEM_HOST) {
+    rc = ensure_stage(E, N * 8);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(E->d_stage, in, N * 8, cudaMemcpyHostToDevice, s));
+    src = (const double*)E->d_stage;
+  }
+  launch_grid_import(E->d_jobs + job, E->d_st + job, which, src, J.dev.nx, J.dev.ny, s);
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_get_hits(pic_engine* E, int job, int species, int64_t capacity, int64_t* idx, int64_t* n_out) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  JobHost& J = E->jobs[job];
+  if (species < 0 || species >= J.cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
+  CK(cudaSetDevice(E->device));
+  CK(cudaStreamSynchronize(E->stream));
+  int k = 0;
+  CK(cudaMemcpy(&k, E->d_hits + job * kSlotsPerJob + species, sizeof(int), cudaMemcpyDeviceToHost));
+  if (n_out) *n_out = k;
+  if (k > capacity) return fail(PIC_ERR_CAPACITY, "output array too small");
+  std::vector<int32_t> h(k);
+  if (k) CK(cudaMemcpy(h.data(), J.slot[species].hits, sizeof(int32_t) * k, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < k; ++i) idx[i] = h[i];
+  return PIC_OK;
+}
+
+// ---------------------------------------------------------------- stateless solver
+namespace {
+struct SolverCtx {
+  int device, nx, ny, levels, nu_pre, nu_post, nu_coarse;
+  pic_engine* E = nullptr;
+  int job = -1;
+};
+std::mutex g_solver_mu;
+std::vector<SolverCtx> g_solvers;
+}  // namespace
+
+int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int levels, double h, double omega,
+                            int nu_pre, int nu_post, int nu_coarse, double tol, int max_cycles, void* stream,
+                            int* cycles_out, double* relres_out) {
+  if (!phi || !rho) return fail(PIC_ERR_ARG, "null grid pointers");
+  if (!is_pow2p1(nx) || nx != ny) return fail(PIC_ERR_ARG, "grid must be square with 2^k+1 nodes per side");
+  if (!(h > 0)) return fail(PIC_ERR_ARG, "h must be positive");
+  int device = 0;
+  CK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lk(g_solver_mu);
+  SolverCtx* ctx = nullptr;
+  for (auto& c : g_solvers)
+    if (c.device == device && c.nx == nx && c.ny == ny && c.levels == levels && c.nu_pre == nu_pre &&
+        c.nu_post == nu_post && c.nu_coarse == nu_coarse)
+      ctx = &c;
+  if (!ctx) {
+    SolverCtx c{device, nx, ny, levels, nu_pre, nu_post, nu_coarse};
+    int rc = pic_engine_create(device, 0, &c.E);
+    if (rc) return rc;
+    pic_job_config cfg{};
+    cfg.nx = nx; cfg.ny = ny; cfg.Lx = h * (nx - 1); cfg.Ly = h * (ny - 1); cfg.dt = 1.0;
+    cfg.units = PIC_UNITS_REF; cfg.n_species = 0;
+    cfg.mg_levels = levels > 0 ? levels : 0;
+    cfg.nu_pre = nu_pre; cfg.nu_post = nu_post; cfg.nu_coarse = nu_coarse;
+    cfg.omega = omega; cfg.tol = tol; cfg.max_cycles = max_cycles;
+    rc = pic_job_create(c.E, &cfg, &c.job);
+    if (rc) { pic_engine_destroy(c.E); return rc; }
+    g_solvers.push_back(c);
+    ctx = &g_solvers.back();
+  }
+  pic_engine* E = ctx->E;
+  JobHost& J = E->jobs[ctx->job];
+  J.dev.deposit_mode = 2;
+  J.dev.rho_d = rho;
+  J.dev.rhs_scale = 1.0;
+  J.dev.qref = 1.0;
+  J.dev.h = h;
+  J.dev.omega = (float)omega;
+  J.dev.tol = tol;
+  J.dev.max_cycles = max_cycles;
+  cudaStream_t s = stream ? (cudaStream_t)stream : E->stream;
+  CK(cudaMemcpyAsync(E->d_jobs + ctx->job, &J.dev, sizeof(JobDev), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(&E->d_st[ctx->job].phi_cur, 0, sizeof(int), s));
+  const size_t bytes = (size_t)nx * ny * 8;
+  CK(cudaMemcpyAsync(J.dev.phi64[0], phi, bytes, cudaMemcpyDeviceToDevice, s));
+  if (J.mg.valid) J.mg.max_cycles = max_cycles;
+  if (!J.mg.valid) {
+    int rc = build_mg(E, std::vector<int>{ctx->job}, J.mg);
+    if (rc) return rc;
+  }
+  int rc = solve(E, J.mg, nullptr, s);
+  if (rc) return rc;
+  JobState T;
+  CK(cudaMemcpyAsync(&T, E->d_st + ctx->job, sizeof(JobState), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaMemcpyAsync(phi, J.dev.phi64[T.phi_cur], bytes, cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  if (cycles_out) *cycles_out = T.cycles;
+  if (relres_out) *relres_out = T.relres;
+  if (T.converged != 1) return fail(PIC_ERR_NOT_CONVERGED, "multigrid stopped at max_cycles above tol");
+  return PIC_OK;
+}
+
+int pic_efield_f64(const double* phi, double* E_xy, int nx, int ny, double dx, double dy, void* stream) {
+  if (!phi || !E_xy || nx < 2 || ny < 2) return fail(PIC_ERR_ARG, "bad arguments");
+  launch_efield_f64(phi, E_xy, nx, ny, dx, dy, (cudaStream_t)stream);
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+}  // extern "C"

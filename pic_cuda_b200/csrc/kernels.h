@@ -1,0 +1,80 @@
+// kernels.h — internal launch interface between the host engine and the kernel files.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+// Phase bits (same values as the public PIC_PHASE_*), plus internal ones.
+#define PIC_PHASE_KICK_I 1
+#define PIC_PHASE_MCC_I 2
+#define PIC_PHASE_DRIFT_I 4
+#define PIC_PHASE_WALLS_I 8
+#define PIC_PHASE_DEPOSIT_I 16
+#define PIC_PHASE_GATED_I 256   // kick/MCC only where the job's kick_pending flag is set
+
+// One multigrid tile of one job.
+struct TileRef {
+  int job;
+  int ti, tj;     // tile origin in owned-node units (multiply by the tile size)
+  int local;      // index of this tile inside the job's tiles of the same launch
+  int nlocal;     // tiles of this job in the launch
+  int pbase;      // first partial-sum slot of the job
+};
+
+struct EngineLaunch {
+  const JobDev* jobs;
+  JobState* st;
+  const SlotDev* slots;   // device slot table (pointers may be swapped by the sort)
+  SlotDev* slots_mut;
+  int* counts;            // live particles per slot
+  int* hit_counts;        // hits of the last WALLS phase per slot
+  int* aux;               // 4 ints per slot (compaction counters)
+  int* chunk_prefix;      // nslots + 1
+  const uint8_t* active;  // per slot
+  int nslots;
+  int njobs;
+  int mover_grid;
+  int num_sms;
+  int* running;           // jobs whose field solve is still iterating
+  int* absorbed;          // particles absorbed in the last step, per slot
+};
+
+void launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t s);
+void launch_compact(const EngineLaunch& L, cudaStream_t s);
+void launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
+void launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
+void launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
+void launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);
+void launch_pid_max(const SlotDev* slot_dev, int64_t n, JobState* st, cudaStream_t s);
+void launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s);
+
+// Multigrid (all jobs of a launch at once).
+struct MgLaunch {
+  const TileRef* init_tiles; int n_init;                 // level-0 residual, 32x32 owned
+  const TileRef* down_tiles[PIC_MAX_LEVELS]; int n_down[PIC_MAX_LEVELS];   // coarse 16x16 owned
+  const TileRef* up_tiles[PIC_MAX_LEVELS]; int n_up[PIC_MAX_LEVELS];       // fine 32x32 owned
+  const TileRef* upd_tiles; int n_upd;                   // level-0 update for jobs with lc == 0
+  const int* coarse_jobs; int n_coarse;
+  int max_depth;                                         // max lc over jobs
+  size_t coarse_smem;
+  int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
+};
+void launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
+void launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
+void mg_configure_coarse(size_t smem_bytes);
+
+// Conversions between the public FP64 domain-unit layout and the engine layout.
+void launch_load_species(const SlotDev* slot_dev, const JobDev* job_dev, int64_t n, const double* x,
+                         const double* y, const double* vx, const double* vy, const double* vz,
+                         const uint32_t* pid, uint32_t pid_base, double inv_dx, double inv_dy, int ncx,
+                         int ncy, cudaStream_t s);
+void launch_export_species(const SlotDev* slot_dev, int64_t n, double* x, double* y, double* vx, double* vy,
+                           double* vz, uint32_t* pid, double dx, double dy, cudaStream_t s);
+void launch_export_raw(const SlotDev* slot_dev, int64_t n, uint32_t* cell, float* fx, float* fy, float* vx,
+                       float* vy, float* vz, uint32_t* pid, cudaStream_t s);
+void launch_grid_export(const JobDev* job_dev, const JobState* st_dev, int which, double* out, int nx, int ny,
+                        double dx, double dy, cudaStream_t s);
+void launch_grid_import(const JobDev* job_dev, const JobState* st_dev, int which, const double* in, int nx,
+                        int ny, cudaStream_t s);
+void launch_zero_rho(const JobDev* job_dev, int64_t nodes, int deposit_mode, void* rho, cudaStream_t s);
+void launch_efield_f64(const double* phi, double* exy, int nx, int ny, double dx, double dy, cudaStream_t s);

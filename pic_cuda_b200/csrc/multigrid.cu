@@ -1,0 +1,404 @@
+// multigrid.cu — Poisson solve lap(phi) = F for every job of the engine at once.
+//
+// Algorithm = solve_multigrid / v_cycle of the reference (Multigrid.cu:539-642): red-black
+// SOR smoothing (colour (i+j) odd first, phi = fma(w, (N+S+E+W - h^2 f)/4, (1-w) phi),
+// Multigrid.cu:246-265), residual f - lap(phi) (:269-297), full weighting (:299-349),
+// bilinear prolongation added to the finer level (:351-407), coarse guess zeroed every
+// cycle (:556), relative residual ||r|| / ||F|| checked after every cycle (:614-631).
+// Precision: the V-cycle runs in FP32 on the correction equation A e = r; the residual r,
+// the update phi += e and the norms are FP64 (defect correction), so the FP64 relative
+// residual can be driven to 1e-9 and below.
+// Kernels (one launch covers all jobs through tile lists):
+//   mg_init    level 0: r = F - A phi (FP64), ||r||^2, ||F||^2; r -> f0 (FP32)
+//   mg_down    per level above the coarse one: nu_pre sweeps from e = 0 on a 16x16 tile of
+//              coarse nodes (fine tile + halo 2*nu+2 in shared memory, every sweep done
+//              locally: a node at distance d from the tile edge is exact for d half-sweeps),
+//              then residual + full weighting straight from shared memory
+//   mg_coarse  one CTA per job runs the whole V-cycle below 129x129 in shared memory
+//   mg_up      prolongation + nu_post sweeps on 32x32 tiles; on level 0 also the FP64
+//              update phi += e, the new FP64 residual, phi32 and the norm (last CTA of each
+//              job reduces the per-tile partials in a fixed order: deterministic).
+#include <algorithm>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+constexpr int kTI = 32;   // level-0 residual / update tile
+constexpr int kTC = 16;   // down-leg coarse tile
+constexpr int kTU = 32;   // up-leg fine tile
+
+__device__ __forceinline__ double rho_at(const JobDev& J, size_t idx) {
+  return J.deposit_mode == 0 ? (double)J.rho_f[idx] : J.deposit_mode == 1 ? (double)J.rho_i[idx] * 0x1p-40 : J.rho_d[idx];
+}
+
+__device__ double block_sum(double v) {
+  __shared__ double ws[32];
+  for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) ws[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += ws[k];
+  return t;  // valid in thread 0
+}
+
+// Last CTA of a job's tiles in this launch?  (threadfence + ticket)
+__device__ bool last_of_job(JobState& T, int nlocal) {
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(&T.ticket, 1);
+    last = (t == nlocal - 1);
+    if (last) T.ticket = 0;
+  }
+  __syncthreads();
+  return last;
+}
+
+// ---------------------------------------------------------------- mg_init
+__global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
+                                                      JobState* __restrict__ st, int* running) {
+  const TileRef tr = tiles[blockIdx.x];
+  const JobDev& J = jobs[tr.job];
+  JobState& T = st[tr.job];
+  const int nx = J.nx, ny = J.ny;
+  const double* phi = J.phi64[T.phi_cur];
+  const double inv_h2 = 1.0 / (J.h * J.h);
+  double ar = 0.0, af = 0.0;
+  for (int k = threadIdx.x; k < kTI * kTI; k += blockDim.x) {
+    const int i = tr.ti * kTI + (k % kTI), j = tr.tj * kTI + (k / kTI);
+    if (i >= nx || j >= ny) continue;
+    const size_t c = (size_t)j * nx + i;
+    const double F = J.rhs_scale * rho_at(J, c);
+    double r = 0.0;
+    if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
+      const double lap = (phi[c - nx] + phi[c + nx] + phi[c - 1] + phi[c + 1] - 4.0 * phi[c]) * inv_h2;
+      r = F - lap;
+    }
+    J.f[0][c] = (float)r;
+    J.phi32[c] = (float)phi[c];
+    ar += r * r;
+    af += F * F;
+  }
+  const double sr = block_sum(ar);
+  const double sf = block_sum(af);
+  if (threadIdx.x == 0) {
+    J.partials[2 * (tr.pbase + tr.local)] = sr;
+    J.partials[2 * (tr.pbase + tr.local) + 1] = sf;
+  }
+  if (last_of_job(T, tr.nlocal) && threadIdx.x == 0) {
+    double r2 = 0.0, f2 = 0.0;
+    for (int t = 0; t < tr.nlocal; ++t) { r2 += J.partials[2 * (tr.pbase + t)]; f2 += J.partials[2 * (tr.pbase + t) + 1]; }
+    T.rnorm2 = r2;
+    T.fnorm2 = f2;
+    T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
+    T.cycles = 0;
+    T.converged = 0;
+    atomicAdd(running, 1);
+  }
+}
+
+// Red-black SOR half-sweeps on a W x W shared tile whose node (0,0) is grid node (gx0,gy0).
+// Only grid-interior nodes that are not on the tile's outer ring are updated.
+__device__ __forceinline__ void tile_sweeps(float* e, const float* f, int W, int gx0, int gy0, int n, float h2,
+                                            float omega, int nu) {
+  const float om1 = 1.f - omega;
+  for (int it = 0; it < nu; ++it) {
+    for (int colour = 1; colour >= 0; --colour) {
+      for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
+        const int lx = k % W, ly = k / W;
+        const int gx = gx0 + lx, gy = gy0 + ly;
+        if (((gx + gy) & 1) != colour) continue;
+        if (gx <= 0 || gx >= n - 1 || gy <= 0 || gy >= n - 1) continue;
+        if (lx == 0 || lx == W - 1 || ly == 0 || ly == W - 1) continue;
+        const float s = e[k + W] + e[k - W] + e[k + 1] + e[k - 1];
+        const float nv = 0.25f * (s - h2 * f[k]);
+        e[k] = fmaf(omega, nv, om1 * e[k]);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------- mg_down
+__global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
+                                                      const JobState* __restrict__ st, int l) {
+  extern __shared__ float sm[];
+  const TileRef tr = tiles[blockIdx.x];
+  const JobDev& J = jobs[tr.job];
+  if (st[tr.job].converged) return;
+  const int nf = J.nl[l], nc = J.nl[l + 1];
+  const double hl = J.h * (double)(1 << l);
+  const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
+  const int nu = J.nu_pre, H = 2 * nu;
+  const int ic0 = tr.ti * kTC, jc0 = tr.tj * kTC;
+  const int gx0 = 2 * ic0 - 2 - H, gy0 = 2 * jc0 - 2 - H;
+  const int W = 2 * kTC + 3 + 2 * H;
+  float* e = sm;
+  float* f = sm + W * W;
+  const float* fg = J.f[l];
+  for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
+    const int gx = gx0 + k % W, gy = gy0 + k / W;
+    f[k] = (gx >= 0 && gx < nf && gy >= 0 && gy < nf) ? fg[(size_t)gy * nf + gx] : 0.f;
+    e[k] = 0.f;
+  }
+  __syncthreads();
+  tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
+  // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
+  float* eg = J.e[l];
+  for (int k = threadIdx.x; k < 4 * kTC * kTC; k += blockDim.x) {
+    const int ox = k % (2 * kTC), oy = k / (2 * kTC);
+    const int gx = 2 * ic0 + ox, gy = 2 * jc0 + oy;
+    if (gx < nf && gy < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+  }
+  // residual + full weighting to the owned coarse nodes
+  float* fc = J.f[l + 1];
+  for (int k = threadIdx.x; k < kTC * kTC; k += blockDim.x) {
+    const int ic = ic0 + k % kTC, jc = jc0 + k / kTC;
+    if (ic >= nc || jc >= nc) continue;
+    float v = 0.f;
+    if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
+      const int cx = 2 * ic - gx0, cy = 2 * jc - gy0;
+      float r[3][3];
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int q = (cy + dy) * W + (cx + dx);
+          const float lap = (e[q - W] + e[q + W] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
+          r[dy + 1][dx + 1] = f[q] - lap;
+        }
+      const float s = 4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] +
+                      r[0][0] + r[0][2] + r[2][0] + r[2][2];
+      v = s * 0.0625f;
+    }
+    fc[(size_t)jc * nc + ic] = v;
+  }
+}
+
+// ---------------------------------------------------------------- mg_coarse
+__device__ void smem_sweeps(float* e, const float* f, int n, float h2, float omega, int nu) {
+  const float om1 = 1.f - omega;
+  const int m = n - 2;
+  for (int it = 0; it < nu; ++it) {
+    for (int colour = 1; colour >= 0; --colour) {
+      for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
+        const int i = 1 + k % m, j = 1 + k / m;
+        if (((i + j) & 1) != colour) continue;
+        const int c = j * n + i;
+        const float s = e[c + n] + e[c - n] + e[c + 1] + e[c - 1];
+        const float nv = 0.25f * (s - h2 * f[c]);
+        e[c] = fmaf(omega, nv, om1 * e[c]);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
+                                                         const JobState* __restrict__ st) {
+  extern __shared__ float sm[];
+  const int job = job_list[blockIdx.x];
+  const JobDev& J = jobs[job];
+  if (st[job].converged) return;
+  const int lc = J.lc, L = J.levels;
+  float* E[PIC_MAX_LEVELS];
+  float* F[PIC_MAX_LEVELS];
+  {
+    float* p = sm;
+    for (int l = lc; l < L; ++l) {
+      const int n2 = J.nl[l] * J.nl[l];
+      E[l] = p; p += n2;
+      F[l] = p; p += n2;
+    }
+  }
+  {
+    const int n = J.nl[lc];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F[lc][k] = J.f[lc][k]; E[lc][k] = 0.f; }
+  }
+  __syncthreads();
+  for (int l = lc; l < L - 1; ++l) {
+    const int n = J.nl[l], nc = J.nl[l + 1];
+    const double hl = J.h * (double)(1 << l);
+    const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
+    smem_sweeps(E[l], F[l], n, h2, J.omega, J.nu_pre);
+    const float* e = E[l];
+    const float* f = F[l];
+    for (int k = threadIdx.x; k < nc * nc; k += blockDim.x) {
+      const int ic = k % nc, jc = k / nc;
+      float v = 0.f;
+      if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
+        float r[3][3];
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int q = (2 * jc + dy) * n + (2 * ic + dx);
+            const float lap = (e[q - n] + e[q + n] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
+            r[dy + 1][dx + 1] = f[q] - lap;
+          }
+        v = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] + r[0][2] +
+             r[2][0] + r[2][2]) * 0.0625f;
+      }
+      F[l + 1][k] = v;
+      E[l + 1][k] = 0.f;
+    }
+    __syncthreads();
+  }
+  {
+    const double hl = J.h * (double)(1 << (L - 1));
+    smem_sweeps(E[L - 1], F[L - 1], J.nl[L - 1], (float)(hl * hl), J.omega, J.nu_coarse);
+  }
+  for (int l = L - 2; l >= lc; --l) {
+    const int n = J.nl[l], nc = J.nl[l + 1];
+    const float* c = E[l + 1];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+      const int i = k % n, j = k / n;
+      const int ic = i >> 1, jc = j >> 1;
+      const float* cp = c + jc * nc + ic;
+      float v;
+      if (!(i & 1) && !(j & 1)) v = cp[0];
+      else if ((i & 1) && !(j & 1)) v = 0.5f * (cp[0] + cp[1]);
+      else if (!(i & 1) && (j & 1)) v = 0.5f * (cp[0] + cp[nc]);
+      else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
+      E[l][k] += v;
+    }
+    __syncthreads();
+    const double hl = J.h * (double)(1 << l);
+    smem_sweeps(E[l], F[l], n, (float)(hl * hl), J.omega, J.nu_post);
+  }
+  {
+    const int n = J.nl[lc];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) J.e[lc][k] = E[lc][k];
+  }
+}
+
+// ---------------------------------------------------------------- mg_up
+// mode 0: prolong + smooth, write e_l.  mode 1: level 0, prolong + smooth + FP64 update.
+// mode 2: level 0 update only (e_0 produced by the coarse kernel).
+__global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
+                                                    JobState* __restrict__ st, int l, int mode, int* running) {
+  extern __shared__ float sm[];
+  const TileRef tr = tiles[blockIdx.x];
+  const JobDev& J = jobs[tr.job];
+  JobState& T = st[tr.job];
+  if (T.converged) return;
+  const int nf = J.nl[l];
+  const double hl = J.h * (double)(1 << l);
+  const float h2 = (float)(hl * hl);
+  const int nu = mode == 2 ? 0 : J.nu_post, H = 2 * nu, X = (l == 0) ? 1 : 0;
+  const int i0 = tr.ti * kTU, j0 = tr.tj * kTU;
+  const int gx0 = i0 - H - X, gy0 = j0 - H - X;
+  const int W = kTU + 2 * H + 2 * X;
+  float* e = sm;
+  float* f = sm + W * W;
+  const float* eg = J.e[l];
+  const float* fg = J.f[l];
+  const bool prolong = mode != 2;
+  const int nc = prolong ? J.nl[l + 1] : 0;
+  const float* ec = prolong ? J.e[l + 1] : nullptr;
+  for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
+    const int gx = gx0 + k % W, gy = gy0 + k / W;
+    float ev = 0.f, fv = 0.f;
+    if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) {
+      const size_t g = (size_t)gy * nf + gx;
+      ev = eg[g];
+      fv = fg[g];
+      if (prolong) {
+        const float* cp = ec + (size_t)(gy >> 1) * nc + (gx >> 1);
+        const bool io = gx & 1, jo = gy & 1;
+        float v;
+        if (!io && !jo) v = cp[0];
+        else if (io && !jo) v = 0.5f * (cp[0] + cp[1]);
+        else if (!io && jo) v = 0.5f * (cp[0] + cp[nc]);
+        else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
+        ev += v;
+      }
+    }
+    e[k] = ev;
+    f[k] = fv;
+  }
+  __syncthreads();
+  if (nu > 0) tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
+  if (mode == 0) {
+    float* eo = J.e[l];
+    for (int k = threadIdx.x; k < kTU * kTU; k += blockDim.x) {
+      const int gx = i0 + k % kTU, gy = j0 + k / kTU;
+      if (gx < nf && gy < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+    }
+    return;
+  }
+  // ---- level-0 FP64 update and new residual
+  __shared__ double P[(kTU + 2) * (kTU + 2)];
+  const int cur = T.phi_cur;
+  const double* pc = J.phi64[cur];
+  double* pn = J.phi64[cur ^ 1];
+  constexpr int PW = kTU + 2;
+  for (int k = threadIdx.x; k < PW * PW; k += blockDim.x) {
+    const int gx = i0 - 1 + k % PW, gy = j0 - 1 + k / PW;
+    double v = 0.0;
+    if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) v = pc[(size_t)gy * nf + gx] + (double)e[(gy - gy0) * W + (gx - gx0)];
+    P[k] = v;
+  }
+  __syncthreads();
+  const double inv_h2 = 1.0 / (J.h * J.h);
+  double ar = 0.0;
+  for (int k = threadIdx.x; k < kTU * kTU; k += blockDim.x) {
+    const int ox = k % kTU, oy = k / kTU;
+    const int gx = i0 + ox, gy = j0 + oy;
+    if (gx >= nf || gy >= nf) continue;
+    const size_t g = (size_t)gy * nf + gx;
+    const int q = (oy + 1) * PW + (ox + 1);
+    const double F = J.rhs_scale * rho_at(J, g);
+    double r = 0.0;
+    if (gx > 0 && gx < nf - 1 && gy > 0 && gy < nf - 1) {
+      const double lap = (P[q - PW] + P[q + PW] + P[q - 1] + P[q + 1] - 4.0 * P[q]) * inv_h2;
+      r = F - lap;
+    }
+    pn[g] = P[q];
+    J.phi32[g] = (float)P[q];
+    J.f[0][g] = (float)r;
+    ar += r * r;
+  }
+  const double sr = block_sum(ar);
+  if (threadIdx.x == 0) J.partials[2 * (tr.pbase + tr.local)] = sr;
+  if (last_of_job(T, tr.nlocal) && threadIdx.x == 0) {
+    double r2 = 0.0;
+    for (int t = 0; t < tr.nlocal; ++t) r2 += J.partials[2 * (tr.pbase + t)];
+    T.rnorm2 = r2;
+    T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
+    T.cycles += 1;
+    T.phi_cur = cur ^ 1;
+    if (T.relres < J.tol) { T.converged = 1; atomicSub(running, 1); }
+    else if (T.cycles >= J.max_cycles) { T.converged = 2; atomicSub(running, 1); }
+  }
+}
+
+size_t down_smem(int nu) { const int W = 2 * kTC + 3 + 4 * nu; return (size_t)2 * W * W * sizeof(float); }
+size_t up_smem(int nu) { const int W = kTU + 4 * nu + 2; return (size_t)2 * W * W * sizeof(float); }
+
+}  // namespace
+
+void mg_configure_coarse(size_t smem_bytes) {
+  cudaFuncSetAttribute(mg_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  cudaFuncSetAttribute(mg_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)down_smem(16));
+  cudaFuncSetAttribute(mg_up_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem(16));
+}
+
+void launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
+  cudaMemsetAsync(L.running, 0, sizeof(int), s);
+  if (M.n_init) mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st, L.running);
+}
+
+
+void launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
+  for (int l = 0; l < M.max_depth; ++l)
+    if (M.n_down[l]) mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l);
+  if (M.n_coarse) mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st);
+  for (int l = M.max_depth - 1; l >= 0; --l)
+    if (M.n_up[l])
+      mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0, L.running);
+  if (M.n_upd) mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running);
+}

@@ -1,0 +1,196 @@
+// sort.cu — counting sort of every particle slot by cell (row-major cell index).
+//
+// The reference never orders particles (Thrust is included but unused, particles.cu:7-10),
+// so its scatter/gather kernels hit random nodes.  Sorting by cell every N steps makes the
+// warps of the mover touch a handful of neighbouring nodes, which turns the deposit's
+// atomics into one per cell segment and the gather into L1 hits.
+//   histogram (warp-aggregated with __match_any_sync) -> exclusive scan over cells
+//   (tile sums, per-slot scan of tile sums, tile rescan) -> scatter of all seven fields into
+//   the slot's second set of arrays -> pointer swap in the device slot table.
+// All slots of all jobs are processed by the same launches (blockIdx.y = slot).
+#include <algorithm>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace {
+
+constexpr int kTile = 2048;     // cells per scan tile (256 threads x 8)
+
+__device__ __forceinline__ uint32_t dense_key(uint32_t c, int ncx, uint32_t ncells) {
+  return c == PIC_CELL_OUT ? ncells : (uint32_t)cell_j(c) * (uint32_t)ncx + (uint32_t)cell_i(c);
+}
+
+__global__ void sort_zero(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int ncells = J.ncx * J.ncy + 1;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) S.cell_count[k] = 0;
+}
+
+__global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int n = counts[s];
+  const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
+  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
+    const int p = wb + lane_id();
+    const bool in = p < n;
+    const uint32_t key = in ? dense_key(S.cell[p], J.ncx, ncells) : 0xFFFFFFFFu;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(grp) - 1;
+    if (in && lane_id() == leader) atomicAdd(S.cell_count + key, __popc(grp));
+  }
+}
+
+// Exclusive scan of 8 values per thread over a 2048-entry tile; returns the tile total.
+__device__ int tile_exclusive_scan(int v[8]) {
+  __shared__ int warp_tot[8];
+  int t = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) { const int x = v[k]; v[k] = t; t += x; }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int incl = t;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  int woff = 0, total = 0;
+  for (int k = 0; k < 8; ++k) { if (k < w) woff += warp_tot[k]; total += warp_tot[k]; }
+  __syncthreads();
+  const int off = woff + incl - t;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] += off;
+  return total;
+}
+
+__global__ void __launch_bounds__(256) sort_tile_sums(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int ncells = J.ncx * J.ncy + 1;
+  const int ntiles = (ncells + kTile - 1) / kTile;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int sum = 0;
+    for (int k = 0; k < 8; ++k) {
+      const int c = tile * kTile + threadIdx.x * 8 + k;
+      if (c < ncells) sum += S.cell_count[c];
+    }
+    for (int o = 16; o; o >>= 1) sum += __shfl_down_sync(0xffffffffu, sum, o);
+    __shared__ int ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int k = 0; k < 8; ++k) t += ws[k];
+      S.scan_part[tile] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) sort_scan_parts(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+  const int s = blockIdx.x;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int ntiles = (J.ncx * J.ncy + 1 + kTile - 1) / kTile;
+  int carry = 0;
+  for (int b = 0; b < ntiles; b += kTile) {
+    int v[8];
+    for (int k = 0; k < 8; ++k) {
+      const int c = b + threadIdx.x * 8 + k;
+      v[k] = c < ntiles ? S.scan_part[c] : 0;
+    }
+    const int tot = tile_exclusive_scan(v);
+    for (int k = 0; k < 8; ++k) {
+      const int c = b + threadIdx.x * 8 + k;
+      if (c < ntiles) S.scan_part[c] = v[k] + carry;
+    }
+    carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) sort_apply(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int ncells = J.ncx * J.ncy + 1;
+  const int ntiles = (ncells + kTile - 1) / kTile;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int v[8];
+    for (int k = 0; k < 8; ++k) {
+      const int c = tile * kTile + threadIdx.x * 8 + k;
+      v[k] = c < ncells ? S.cell_count[c] : 0;
+    }
+    tile_exclusive_scan(v);
+    const int base = S.scan_part[tile];
+    for (int k = 0; k < 8; ++k) {
+      const int c = tile * kTile + threadIdx.x * 8 + k;
+      if (c < ncells) S.cell_count[c] = v[k] + base;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int n = counts[s];
+  const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
+  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
+    const int p = wb + lane_id();
+    const bool in = p < n;
+    const uint32_t c = in ? S.cell[p] : 0u;
+    const uint32_t key = in ? dense_key(c, J.ncx, ncells) : 0xFFFFFFFFu;
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (in && lane_id() == leader) base = atomicAdd(S.cell_count + key, __popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (in) {
+      const int at = base + __popc(grp & ((1u << lane_id()) - 1u));
+      S.cell_b[at] = c; S.fx_b[at] = S.fx[p]; S.fy_b[at] = S.fy[p];
+      S.vx_b[at] = S.vx[p]; S.vy_b[at] = S.vy[p]; S.vz_b[at] = S.vz[p]; S.pid_b[at] = S.pid[p];
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void swp(T*& a, T*& b) { T* t = a; a = b; b = t; }
+
+__global__ void sort_swap(SlotDev* slots, const uint8_t* mask, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !mask[s]) return;
+  SlotDev& S = slots[s];
+  swp(S.cell, S.cell_b); swp(S.fx, S.fx_b); swp(S.fy, S.fy_b);
+  swp(S.vx, S.vx_b); swp(S.vy, S.vy_b); swp(S.vz, S.vz_b); swp(S.pid, S.pid_b);
+}
+
+}  // namespace
+
+void launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
+  if (L.nslots == 0) return;
+  const int ncells = max_cells + 1;
+  const int ntiles = (ncells + kTile - 1) / kTile;
+  const int gz = std::min(std::max((ncells + 255) / 256, 1), 4 * L.num_sms);
+  const int gp = std::min(std::max((max_particles + 255) / 256, 1), 8 * L.num_sms);
+  sort_zero<<<dim3(gz, L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
+  sort_hist<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+  sort_tile_sums<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
+  sort_scan_parts<<<L.nslots, 256, 0, st>>>(L.jobs, L.slots, mask);
+  sort_apply<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
+  sort_scatter<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+  sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
+}

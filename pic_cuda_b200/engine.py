@@ -1,0 +1,193 @@
+"""Python host API over the C ABI: Engine (device tables + stepping) and Job (one simulation).
+
+Arrays passed in may be numpy arrays (host memory) or CUDA torch tensors (device memory);
+the engine converts them to its FP32 cell-relative layout on the device.  Every compute
+call goes to libpic_b200.so; nothing here computes physics on the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Any
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _is_torch_cuda(a: Any) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _as_ptr(a: Any, dtype, n: int | None = None):
+    """(pointer, memory kind, keep-alive) for a host numpy array or a CUDA torch tensor."""
+    if a is None:
+        return None, L.MEM_HOST, None
+    if _is_torch_cuda(a):
+        import torch
+        tdt = {np.float64: torch.float64, np.float32: torch.float32, np.uint32: torch.int32,
+               np.int64: torch.int64}[dtype]
+        t = a.contiguous()
+        if t.dtype != tdt:
+            t = t.to(tdt)
+        return C.c_void_p(t.data_ptr()), L.MEM_DEVICE, t
+    if hasattr(a, "numpy") and not isinstance(a, np.ndarray):  # CPU torch tensor (maybe pinned)
+        if a.is_contiguous() and str(a.dtype).endswith({np.float64: "float64", np.float32: "float32",
+                                                            np.uint32: "int32", np.int64: "int64"}[dtype]):
+            return C.c_void_p(a.data_ptr()), L.MEM_HOST, a
+        a = a.numpy()
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data_as(C.c_void_p), L.MEM_HOST, arr
+
+
+class Job:
+    def __init__(self, engine: "Engine", job_id: int, cfg: L.JobConfig, keep: Any = None):
+        self.engine = engine
+        self.id = job_id
+        self.cfg = cfg
+        self._keep = keep
+        self.nx, self.ny = cfg.nx, cfg.ny
+
+    # -- particles
+    def load_species(self, species: int, x, y, vx, vy, vz=None, pid=None) -> None:
+        n = len(x)
+        px, mem, kx = _as_ptr(x, np.float64)
+        py, _, ky = _as_ptr(y, np.float64)
+        pvx, _, kvx = _as_ptr(vx, np.float64)
+        pvy, _, kvy = _as_ptr(vy, np.float64)
+        pvz, _, kvz = _as_ptr(vz, np.float64)
+        ppid, _, kp = _as_ptr(pid, np.uint32)
+        L.check(L.lib().pic_job_load_species(self.engine.h, self.id, species, n, px, py, pvx, pvy, pvz, ppid, mem),
+                "pic_job_load_species")
+
+    def count(self, species: int) -> int:
+        return int(self.diagnostics()["count"][species])
+
+    def export_species(self, species: int) -> dict:
+        cap = int(self.cfg.species[species].capacity)
+        out = {k: np.empty(cap, np.float64) for k in ("x", "y", "vx", "vy", "vz")}
+        out["pid"] = np.empty(cap, np.uint32)
+        n = C.c_int64()
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        L.check(L.lib().pic_job_export_species(self.engine.h, self.id, species, cap, ptr(out["x"]), ptr(out["y"]),
+                                               ptr(out["vx"]), ptr(out["vy"]), ptr(out["vz"]), ptr(out["pid"]),
+                                               C.byref(n), L.MEM_HOST), "pic_job_export_species")
+        return {k: v[: n.value] for k, v in out.items()}
+
+    def export_raw(self, species: int) -> dict:
+        """FP32 cell-relative layout as CUDA torch tensors (no host round trip)."""
+        import torch
+        cap = int(self.cfg.species[species].capacity)
+        dev = torch.device("cuda", self.engine.device)
+        out = {k: torch.empty(cap, dtype=torch.float32, device=dev) for k in ("fx", "fy", "vx", "vy", "vz")}
+        out["cell"] = torch.empty(cap, dtype=torch.int32, device=dev)
+        out["pid"] = torch.empty(cap, dtype=torch.int32, device=dev)
+        n = C.c_int64()
+        p = lambda t: C.c_void_p(t.data_ptr())
+        L.check(L.lib().pic_job_export_species_raw(self.engine.h, self.id, species, cap, p(out["cell"]), p(out["fx"]),
+                                                   p(out["fy"]), p(out["vx"]), p(out["vy"]), p(out["vz"]),
+                                                   p(out["pid"]), C.byref(n)), "pic_job_export_species_raw")
+        return {k: v[: n.value] for k, v in out.items()}
+
+    def hits(self, species: int) -> np.ndarray:
+        cap = int(self.cfg.species[species].capacity)
+        buf = np.empty(max(cap, 1), np.int64)
+        n = C.c_int64()
+        L.check(L.lib().pic_job_get_hits(self.engine.h, self.id, species, cap,
+                                         buf.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(n)), "pic_job_get_hits")
+        return buf[: n.value].copy()
+
+    # -- grids
+    def get_grid(self, which: int) -> np.ndarray:
+        out = np.empty(self.nx * self.ny, np.float64)
+        L.check(L.lib().pic_job_get_grid(self.engine.h, self.id, which, out.ctypes.data_as(C.c_void_p), L.MEM_HOST),
+                "pic_job_get_grid")
+        return out.reshape(self.ny, self.nx)
+
+    def set_grid(self, which: int, arr) -> None:
+        a = np.ascontiguousarray(arr, np.float64).reshape(-1)
+        L.check(L.lib().pic_job_set_grid(self.engine.h, self.id, which, a.ctypes.data_as(C.c_void_p), L.MEM_HOST),
+                "pic_job_set_grid")
+
+    # -- phases
+    def run_phases(self, flags: int, step: int = 0) -> None:
+        L.check(L.lib().pic_job_run_phases(self.engine.h, self.id, flags, step, None), "pic_job_run_phases")
+
+    def compact(self) -> None:
+        L.check(L.lib().pic_job_compact(self.engine.h, self.id, None), "pic_job_compact")
+
+    def zero_rho(self) -> None:
+        L.check(L.lib().pic_job_zero_rho(self.engine.h, self.id, None), "pic_job_zero_rho")
+
+    def solve_field(self) -> None:
+        L.check(L.lib().pic_job_solve_field(self.engine.h, self.id, None), "pic_job_solve_field")
+
+    def sort(self) -> None:
+        L.check(L.lib().pic_job_sort(self.engine.h, self.id, None), "pic_job_sort")
+
+    def diagnostics(self) -> dict:
+        d = L.Diagnostics()
+        L.check(L.lib().pic_job_diagnostics(self.engine.h, self.id, C.byref(d)), "pic_job_diagnostics")
+        ns = self.cfg.n_species
+        return {
+            "step": d.step, "count": [d.count[s] for s in range(ns)], "absorbed": [d.absorbed[s] for s in range(ns)],
+            "collisions": [[d.collisions[s][p] for p in range(L.MAX_PROCESSES)] for s in range(ns)],
+            "ionizations": d.ionizations, "vcycles": d.vcycles, "converged": bool(d.converged), "relres": d.relres,
+            "total_charge": d.total_charge, "kinetic_energy": [d.kinetic_energy[s] for s in range(ns)],
+            "status": d.status,
+        }
+
+    def destroy(self) -> None:
+        if self.id is not None:
+            L.check(L.lib().pic_job_destroy(self.engine.h, self.id), "pic_job_destroy")
+            self.id = None
+
+
+class Engine:
+    def __init__(self, device: int = 0, pool_bytes: int = 0):
+        self.device = device
+        self.h = C.c_void_p()
+        L.check(L.lib().pic_engine_create(device, pool_bytes, C.byref(self.h)), "pic_engine_create")
+
+    def add_job(self, cfg: L.JobConfig, keep: Any = None) -> Job:
+        jid = C.c_int()
+        L.check(L.lib().pic_job_create(self.h, C.byref(cfg), C.byref(jid)), "pic_job_create")
+        return Job(self, jid.value, cfg, keep if keep is not None else getattr(cfg, "_keep", None))
+
+    def step(self, n: int = 1, stream=None) -> None:
+        L.check(L.lib().pic_step(self.h, n, stream), "pic_step")
+
+    def step_graph(self, n: int = 1, stream=None) -> None:
+        L.check(L.lib().pic_step_graph(self.h, n, stream), "pic_step_graph")
+
+    def sync(self) -> None:
+        L.check(L.lib().pic_sync(self.h), "pic_sync")
+
+    def close(self) -> None:
+        if self.h:
+            L.lib().pic_engine_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bytes_needed(cfg: L.JobConfig) -> int:
+    b = C.c_int64()
+    L.check(L.lib().pic_engine_bytes_needed(C.byref(cfg), C.byref(b)), "pic_engine_bytes_needed")
+    return b.value
+
+
+def solve_multigrid_f64(phi, rho, nx: int, ny: int, levels: int, h: float, omega: float = 1.25, nu_pre: int = 3,
+                        nu_post: int = 3, nu_coarse: int = 20, tol: float = 1e-5, max_cycles: int = 50):
+    """solve_multigrid (Multigrid.cu:573) on CUDA torch tensors (FP64, in place on phi)."""
+    cyc = C.c_int()
+    rel = C.c_double()
+    rc = L.lib().pic_solve_multigrid_f64(C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()), nx, ny, levels, h,
+                                         omega, nu_pre, nu_post, nu_coarse, tol, max_cycles, None, C.byref(cyc),
+                                         C.byref(rel))
+    if rc not in (L.PIC_OK, L.PIC_ERR_NOT_CONVERGED):
+        L.check(rc, "pic_solve_multigrid_f64")
+    return cyc.value, rel.value, rc == L.PIC_OK

@@ -1,0 +1,64 @@
+"""The C-ABI library loads and exports what include/pic_b200.h declares (CPU only: no compute
+calls that need a device)."""
+import ctypes
+import re
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    txt = (ROOT / "include" / "pic_b200.h").read_text()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(pic_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from pic_cuda_b200 import _lib
+    L = _lib.lib()
+    names = declared_functions()
+    assert len(names) >= 25
+    for name in names:
+        assert hasattr(L, name), name
+    # the ctypes binding covers every declared entry point
+    assert set(names) <= set(_lib.exported_symbols())
+
+
+def test_struct_layout_matches_library():
+    from pic_cuda_b200 import _lib
+    _lib.check_abi()
+
+
+def test_host_philox_matches_oracle(orc):
+    from pic_cuda_b200 import _lib
+    for ctr, key in [([1, 2, 3, 4], [5, 6]), ([0xDEADBEEF, 7, 0, 1], [1234, 0])]:
+        assert _lib.philox4x32_10(ctr, key) == orc.philox(ctr, key)
+
+
+def test_engine_create_without_device_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        return
+    from pic_cuda_b200 import _lib
+    from pic_cuda_b200.engine import Engine
+    try:
+        Engine(0)
+    except _lib.PicError as e:
+        assert e.code == _lib.PIC_ERR_NO_DEVICE
+    else:
+        raise AssertionError("engine creation must fail without a device")
+
+
+def test_config_validation_is_host_side():
+    from pic_cuda_b200 import _lib, configs
+    from pic_cuda_b200.engine import bytes_needed
+    cfg = configs.plain_small()
+    b = bytes_needed(cfg)
+    assert b > 129 * 129 * 20
+    cfg.nx = cfg.ny = 100  # not 2^k+1
+    try:
+        bytes_needed(cfg)
+    except _lib.PicError as e:
+        assert e.code == _lib.PIC_ERR_ARG
+    else:
+        raise AssertionError("bad grid accepted")

@@ -1,0 +1,215 @@
+"""Known-answer tests that pin the FP64 CPU oracle (CPU only).
+
+The reference ships no tests or golden vectors, so the oracle is pinned by analytic cases
+here and by fixtures made from the reference's own CUDA kernels (test_golden.py).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+
+# Random123 philox4x32_10 known-answer vectors (Salmon et al., SC'11).
+PHILOX_KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+    ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+    ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+     [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+]
+
+
+@pytest.mark.parametrize("ctr,key,out", PHILOX_KAT)
+def test_philox_kat(orc, ctr, key, out):
+    assert orc.philox(ctr, key) == out
+
+
+def test_u01_exact_and_open(orc):
+    L = orc.lib()
+    assert L.orc_u01(0) == 2.0 ** -24
+    assert L.orc_u01(0xFFFFFFFF) == 1.0 - 2.0 ** -24
+    v = L.orc_u01(0x12345678)
+    assert np.float32(v) == v  # exactly representable in FP32
+
+
+def test_cic_single_particle(orc):
+    m = n = 9
+    dx = dy = 0.125
+    # on node (3, 4) -> all charge there; at a cell centre -> a quarter on each corner
+    rho = orc.deposit([3 * dx], [4 * dy], 2.0, m, n, dx, dy)
+    assert rho[4, 3] == 2.0 and rho.sum() == 2.0
+    rho = orc.deposit([2.5 * dx], [5.5 * dy], 1.0, m, n, dx, dy)
+    np.testing.assert_array_equal(rho[5:7, 2:4], np.full((2, 2), 0.25))
+    # skip rule (kernels.cu:53): last node row/column and outside deposit nothing
+    rho = orc.deposit([8 * dx, -1e-9, 0.5, 3 * dx], [0.5, 0.5, 8 * dy, 1.0], 1.0, m, n, dx, dy)
+    assert rho.sum() == 0.0
+
+
+def test_cic_conserves_charge(orc):
+    rng = np.random.default_rng(1)
+    m = n = 65
+    x, y = rng.random(100000), rng.random(100000)
+    q = rng.choice([-1.0, 1.0], 100000)
+    rho = orc.deposit(x, y, q, m, n, 1 / 64, 1 / 64)
+    assert abs(rho.sum() - q[(x < 1) & (y < 1)].sum()) < 1e-9
+
+
+def test_efield_linear_phi_is_exact(orc):
+    m, n = 17, 9
+    dx, dy = 0.1, 0.2
+    X, Y = np.meshgrid(np.arange(m) * dx, np.arange(n) * dy)
+    ex, ey = orc.efield(3.0 * X - 2.0 * Y + 1.0, dx, dy)
+    np.testing.assert_allclose(ex, -3.0, rtol=1e-12)
+    np.testing.assert_allclose(ey, 2.0, rtol=1e-12)
+
+
+def test_uniform_field_kick_and_drift(orc):
+    m = n = 9
+    dx = dy = 0.125
+    Ex, Ey = np.full((n, m), 2.0), np.full((n, m), -1.0)
+    vx, vy = orc.kick([0.3, 0.7], [0.4, 0.2], [1.0, 0.0], [0.0, 1.0], [0.5, -1.0], [2.0, 4.0], Ex, Ey, dx, dy, 0.1)
+    np.testing.assert_allclose(vx, [1.0 + 0.5 * 2.0 / 2.0 * 0.1, -1.0 * 2.0 / 4.0 * 0.1], rtol=1e-14)
+    np.testing.assert_allclose(vy, [-0.5 * 1.0 / 2.0 * 0.1, 1.0 + 1.0 / 4.0 * 0.1], rtol=1e-14)
+    x, y = orc.drift([0.3], [0.4], [1.0], [-2.0], 0.01)
+    assert x[0] == 0.3 + 0.01 and y[0] == 0.4 - 0.02
+
+
+def test_kick_skips_outside(orc):
+    Ex = np.ones((5, 5))
+    vx, vy = orc.kick([1.0, -0.1], [0.5, 0.5], [0.0, 0.0], [0.0, 0.0], 1.0, 1.0, Ex, Ex, 0.25, 0.25, 1.0)
+    assert vx[0] == 0.0 and vx[1] == 0.0
+
+
+@pytest.mark.parametrize("n", [65, 129, 257])
+def test_poisson_manufactured_converges(orc, n):
+    h = 1.0 / (n - 1)
+    X, Y = np.meshgrid(np.arange(n) * h, np.arange(n) * h)
+    exact = np.sin(math.pi * X) * np.sin(math.pi * Y)
+    f = -2 * math.pi ** 2 * exact
+    phi, cyc, rel = orc.mg_solve(np.zeros((n, n)), f, h, tol=1e-10, max_cycles=50)
+    assert rel < 1e-10 and cyc < 20
+    err = np.abs(phi - exact).max()
+    # second order: error ~ C h^2 with C ~ pi^2/12 for the 5-point stencil
+    assert err < 1.0 * h * h
+
+
+def test_poisson_second_order(orc):
+    errs = []
+    for n in (65, 129, 257):
+        h = 1.0 / (n - 1)
+        X, Y = np.meshgrid(np.arange(n) * h, np.arange(n) * h)
+        exact = np.sin(math.pi * X) * np.sin(math.pi * Y)
+        phi, _, _ = orc.mg_solve(np.zeros((n, n)), -2 * math.pi ** 2 * exact, h, tol=1e-12)
+        errs.append(np.abs(phi - exact).max())
+    r1, r2 = errs[0] / errs[1], errs[1] / errs[2]
+    assert 3.8 < r1 < 4.2 and 3.8 < r2 < 4.2
+
+
+def test_reference_mg_settings_converge(orc):
+    # the reference's call: omega 1.25, 3/3/20 sweeps, 5 levels at 129^2, tol 1e-5 (Multigrid.cu:611)
+    n = 129
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((n, n))
+    phi, cyc, rel = orc.mg_solve(np.zeros((n, n)), f, 1 / 128, levels=5, omega=1.25, nu1=3, nu2=3, nuc=20,
+                                 tol=1e-5, max_cycles=50)
+    assert rel < 1e-5 and 1 <= cyc < 50
+
+
+def test_dirichlet_boundary_from_phi(orc):
+    n = 33
+    h = 1 / 32
+    phi0 = np.zeros((n, n))
+    phi0[0, :] = 1.0  # bottom boundary held at 1
+    phi, _, rel = orc.mg_solve(phi0, np.zeros((n, n)), h, tol=1e-12)
+    assert np.all(phi[0, :] == 1.0) and np.all(phi[-1, :] == 0.0)
+    assert rel < 1e-9 or np.abs(orc.residual(phi, np.zeros((n, n)), h)).max() < 1e-9
+    assert 0.0 < phi[16, 16] < 1.0
+
+
+def test_walls_box_and_segments(orc):
+    m = n = 9
+    dx = dy = 0.125
+    # box: outside the half-open rectangle [0, 1) x [0, 1)
+    x = np.array([0.0, 0.999, 1.0, -1e-12, 0.5])
+    y = np.array([0.5, 0.5, 0.5, 0.5, 1.0])
+    np.testing.assert_array_equal(orc.walls_box(x, y, m, n, dx, dy), [False, False, True, True, True])
+    walls = [[0.5, 0.0, 0.5, 1.0]]
+    # crossing, touching the end point, parallel, stopping short
+    x0 = np.array([0.4, 0.4, 0.4, 0.4])
+    y0 = np.array([0.5, 1.0, 0.2, 0.5])
+    x1 = np.array([0.6, 0.6, 0.4, 0.49])
+    y1 = np.array([0.5, 1.0, 0.8, 0.5])
+    np.testing.assert_array_equal(orc.walls_segments(x0, y0, x1, y1, walls), [True, True, False, False])
+    # slow ion in SI units: the reference's absolute EPSILON (collisions.cu:26,36) drops it
+    x0, x1 = np.array([0.5 - 1e-9]), np.array([0.5 + 1e-9])
+    y0 = y1 = np.array([0.5])
+    assert orc.walls_segments(x0, y0, x1, y1, [[0.5, 0.0, 0.5, 1e-2]] + [[0.5, 0.0, 0.5, 1.0]])[0]
+    assert not orc.walls_segments(x0, y0, x1, y1, [[0.5, 0.0, 0.5, 1e-2]], ref_epsilon=True)[0]
+
+
+def _mcc_cfg(sigma_el=1e-19, density=1e21, dt=2e-10, n=200000, ion=False):
+    from pic_cuda_b200 import configs as cf, _lib as L
+    E = np.logspace(-2, 3, 64)
+    procs = [(L.PROC_ELASTIC, 0, 0.0, E, np.full(64, sigma_el))]
+    if ion:
+        procs = [(L.PROC_IONIZATION, 0, 15.76, E, np.where(E < 15.76, 0.0, 3e-20))]
+    mcc = {"mode": L.MCC_NULL_COLLISION, "density": density, "processes": procs, "e_species": 0, "i_species": 1}
+    return cf.make_config(33, 0.01, dt, [(-cf.QE, cf.ME, 1.0, n), (cf.QE, cf.M_AR, 1.0, n)], mcc=mcc,
+                          walls=L.WALLS_NONE)
+
+
+def test_mcc_constant_sigma_count_within_3_sigma(orc):
+    from pic_cuda_b200 import configs as cf
+    cfg = _mcc_cfg()
+    s = orc.Sim(cfg)
+    n = 200000
+    x, y, vx, vy, vz = cf.maxwellian_state(n, 0.01, 3.0, cf.ME, 7)
+    s.load(0, x, y, vx, vy, vz)
+    s.mcc()
+    st = s.stats()
+    v = np.sqrt(vx ** 2 + vy ** 2 + vz ** 2)
+    p = 1e21 * 1e-19 * v * 2e-10  # n sigma(v) v dt per particle
+    assert s.numax(0) * 2e-10 < 1.0
+    mu, sig = p.sum(), math.sqrt((p * (1 - p)).sum())
+    assert abs(st["collisions"][0][0] - mu) < 3 * sig
+    out = s.export(0)
+    e_before = 0.5 * cf.ME * (v ** 2).sum()
+    e_after = 0.5 * cf.ME * (out["vx"] ** 2 + out["vy"] ** 2 + out["vz"] ** 2).sum()
+    assert e_after <= e_before  # elastic recoil only loses energy
+
+
+def test_mcc_ionization_appends_deterministic_pairs(orc):
+    from pic_cuda_b200 import configs as cf
+    cfg = _mcc_cfg(density=3e21, dt=1e-9, n=50000, ion=True)
+    s = orc.Sim(cfg)
+    n = 20000
+    x, y, vx, vy, vz = cf.maxwellian_state(n, 0.01, 20.0, cf.ME, 11)
+    s.load(0, x, y, vx, vy, vz)
+    s.load(1, x[:10], y[:10], vx[:10] * 0, vy[:10] * 0, vz[:10] * 0, pid=np.arange(n, n + 10))
+    s.mcc()
+    st = s.stats()
+    k = st["ionizations"]
+    assert k > 10
+    e, i = s.export(0), s.export(1)
+    assert len(e["x"]) == n + k and len(i["x"]) == 10 + k
+    next_pid = n + 10
+    np.testing.assert_array_equal(e["pid"][n:], next_pid + 2 * np.arange(k))
+    np.testing.assert_array_equal(i["pid"][10:], next_pid + 2 * np.arange(k) + 1)
+    np.testing.assert_array_equal(e["x"][n:], i["x"][10:])  # pair born at one place
+
+
+def test_oracle_sim_step_conserves_and_absorbs(orc):
+    from pic_cuda_b200 import configs as cf
+    cfg = cf.plasma(33, 0.001, 5000, dt=1e-10, tol=1e-9)
+    s = orc.Sim(cfg)
+    e = cf.maxwellian_state(5000, 0.001, 2.0, cf.ME, 5)
+    i = cf.maxwellian_state(5000, 0.001, 0.03, cf.M_AR, 6)
+    s.load(0, *e)
+    s.load(1, *i)
+    s.step(3)
+    st = s.stats()
+    ne, ni = len(s.export(0)["x"]), len(s.export(1)["x"])
+    assert ne < 5000 and ni <= 5000 and st["relres"] < 1e-9
+    w = cfg.species[0].weight
+    assert abs(s.total_charge() - cf.QE * w * (ni - ne)) < 1e-9 * cf.QE * w * 5000
