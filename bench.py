@@ -1,0 +1,319 @@
+#!/usr/bin/env python
+"""Benchmark of the full 2D electrostatic PIC step (particle-steps/s).
+
+Workload (default, `--workload mcc_mixed`): 1025^2 nodes over 5 cm^2, 1e7 electrons + 1e7
+Ar+ (FP32 state), Te 3 eV, argon 3.2e21 m^-3 null-collision MCC with 512-point synthetic
+tables, FP32 V-cycles inside FP64 defect correction to 1e-9 relative residual, absorbing
+walls, sort every 10 steps.  Synthetic seeded data; the particle state (~0.6 GB) is larger
+than L2, so no explicit flush is needed between steps.
+
+  value     device-timed throughput (CUDA events on the launching stream, inputs resident)
+  e2e       one complete job through the public C ABI with host buffers: load from pinned
+            host memory, the workload's own step count with a diagnostics read-back after
+            every step, export to pinned host memory
+  roofline  the fused particle pass (dominant kernel): algorithmic bytes / event time
+  cpu_baseline  the FP64 CPU oracle (OpenMP) on a bounded sample of the same workload
+
+`--impl reference` times the reference path's CPU implementation: the reference has none
+(its only implementation is CUDA), so the FP64 oracle port of its step runs on all host
+threads.  Multi-GPU (torchrun): one independent replica per rank ("replicas only"), no
+collective on the data path; the timed region is bracketed by barriers, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s full PIC step at 1 B200; batched/served vs plain; p50/p99"
+UNIT = "particle-steps/s"
+BYTES_PER_PARTICLE = {"collisionless": 32, "mcc": 44}  # algorithmic bytes per particle-step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="mcc_mixed", choices=["plain_small", "mcc_mixed", "large"])
+    ap.add_argument("--n-per-species", type=int, default=None)
+    ap.add_argument("--deposit", choices=["f32", "i64"], default="f32")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload(args):
+    from pic_cuda_b200 import _lib as L
+    from pic_cuda_b200 import configs as cf
+    w = cf.WORKLOADS[args.workload]
+    n = args.n_per_species or w["n"]
+    dep = L.DEPOSIT_I64 if args.deposit == "i64" else L.DEPOSIT_F32
+    cfg = w["builder"](n_per_species=n, deposit=dep) if args.workload != "plain_small" else cf.plasma(
+        129, 0.01, n, tol=1e-6, deposit=dep)
+    steps_job = {"plain_small": 100, "mcc_mixed": 500, "large": 200}[args.workload]
+    return cfg, n, w["Te"], w["Ti"], cfg.Lx, steps_job
+
+
+def cpu_baseline(args, cfg, n, Te, Ti, Ld, state=None):
+    """FP64 oracle step on the host cores, bounded sample: args.cpu_steps full steps."""
+    from oracle import oracle as orc
+    from pic_cuda_b200 import configs as cf
+    sim = orc.Sim(cfg)
+    if state is None:
+        state = (cf.maxwellian_state(n, Ld, Te, cf.ME, 1234), cf.maxwellian_state(n, Ld, Ti, cf.M_AR, 1235))
+    sim.load(0, *state[0])
+    sim.load(1, *state[1])
+    sim.step(1)  # warm-up (first-touch allocation of the multigrid hierarchy)
+    t0 = time.perf_counter()
+    sim.step(args.cpu_steps)
+    dt = time.perf_counter() - t0
+    np_ = len(sim.export(0)["x"]) + len(sim.export(1)["x"])
+    return {"value": np_ * args.cpu_steps / dt, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
+            "sample": f"{args.cpu_steps} full FP64 oracle steps of {args.workload} ({2 * n} particles, "
+                      f"{cfg.nx}x{cfg.ny}) after 1 warm-up step", "seconds": dt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, n, Te, Ti, Ld, _ = workload(args)
+    steps = max(1, min(args.steps, args.cpu_steps))
+    cb = cpu_baseline(argparse.Namespace(**{**vars(args), "cpu_steps": steps}), cfg, n, Te, Ti, Ld)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1000.0 * cb["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.workload, "grid": f"{cfg.nx}x{cfg.ny}", "particles": 2 * n,
+                       "note": "the reference has no CPU implementation; its step is restated in FP64 "
+                               "(oracle/pic_oracle.cpp) and run with OpenMP on every host thread"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    from pic_cuda_b200 import _lib as L
+    from pic_cuda_b200 import configs as cf
+    from pic_cuda_b200.engine import Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    cfg, n, Te, Ti, Ld, steps_job = workload(args)
+    eng = Engine(local)
+    job = eng.add_job(cfg)
+    cf.load_plasma(job, n, Ld, Te, Ti, seed=1234 + 17 * rank, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    eng.step(args.warmup, stream=sptr)
+    torch.cuda.synchronize(dev)
+    d0 = job.diagnostics()
+    n0 = sum(d0["count"])
+    eng.profile(True)
+    eng.stats(reset=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        eng.step(args.steps, stream=sptr)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    st = eng.stats(reset=True)
+    eng.profile(False)
+    d1 = job.diagnostics()
+    n1 = sum(d1["count"])
+    particles = 0.5 * (n0 + n1)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = torch.tensor([particles], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        ms_max, particles_all = float(t.item()), float(tot.item())
+    else:
+        ms_max, particles_all = ms, particles
+    value = particles_all * args.steps / (ms_max / 1000.0)
+
+    # roofline of the fused particle pass
+    peak, peak_kind = peaks()
+    mcc_on = cfg.mcc_mode != 0
+    bpp = BYTES_PER_PARTICLE["mcc" if mcc_on else "collisionless"]
+    mover_ms = st["mover_ms"] / max(st["mover_launches"], 1)
+    achieved = particles * bpp / (mover_ms / 1000.0) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "mover_traffic.json"
+    if tf.exists():
+        t = json.loads(tf.read_text())
+        traffic = t["bytes_per_particle"] * particles
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "mover_kernel (fused kick/MCC/drift/walls/deposit)",
+                "bytes_per_particle": bpp, "mover_ms": mover_ms, "peak_source": f"{peak_kind} hbm_gbs",
+                "mover_share_of_step": (st["mover_ms"] / ms) if ms > 0 else None}
+
+    # end to end through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, cfg, n, Te, Ti, Ld, steps_job, local, rank)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": f"{cfg.nx}x{cfg.ny}", "particles": 2 * n,
+                   "mcc": mcc_on, "deposit": args.deposit, "tol": cfg.tol, "sort_every": cfg.sort_every,
+                   "precision": "FP32 particles and V-cycles, FP64 defect correction and diagnostics",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "state larger than L2 (no flush needed)",
+                   "vcycles_per_step": st["vcycles"] / max(st["steps"], 1)},
+        "roofline": roofline,
+        "gpu_launches": st["kernel_launches"],
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args, cfg, n, Te, Ti, Ld)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    job.destroy()
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, cfg, n, Te, Ti, Ld, steps_job, local, rank):
+    import torch
+    from pic_cuda_b200 import configs as cf
+    from pic_cuda_b200.engine import Engine
+    steps = args.e2e_steps or steps_job
+    host = []
+    for s, (T, m, seed) in enumerate([(Te, cf.ME, 2000 + rank), (Ti, cf.M_AR, 3000 + rank)]):
+        arrs = cf.maxwellian_state(n, Ld, T, m, seed)
+        host.append([torch.from_numpy(a).pin_memory() for a in arrs])
+    out = [[torch.empty(cfg.species[s].capacity, dtype=torch.float64).pin_memory() for _ in range(5)] for s in (0, 1)]
+    eng = Engine(local)
+    job = eng.add_job(cfg)
+    torch.cuda.synchronize()
+    import ctypes as C
+    from pic_cuda_b200 import _lib as L
+    t0 = time.perf_counter()
+    for s in (0, 1):
+        job.load_species(s, *host[s])
+    for _ in range(steps):
+        eng.step(1)
+        job.diagnostics()
+    counts = []
+    for s in (0, 1):
+        nn = C.c_int64()
+        p = [C.c_void_p(t.data_ptr()) for t in out[s]]
+        L.check(L.lib().pic_job_export_species(eng.h, job.id, s, cfg.species[s].capacity, *p, None, C.byref(nn),
+                                               L.MEM_HOST), "export")
+        counts.append(nn.value)
+    dt = time.perf_counter() - t0
+    h2d = 2 * n * 5 * 8
+    d2h = sum(counts) * 5 * 8 + steps * L.C.sizeof(L.Diagnostics)
+    job.destroy()
+    eng.close()
+    return {"value": 2 * n * steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": d2h / steps, "steps": steps, "seconds": dt,
+            "path": "pic_job_load_species (pinned host) -> pic_step + pic_job_diagnostics per step -> "
+                    "pic_job_export_species (pinned host)"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

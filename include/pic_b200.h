@@ -157,6 +157,14 @@ typedef struct pic_diagnostics {
   uint32_t status;                       /* sticky device status bits (PIC_ERR_* << k)  */
 } pic_diagnostics;
 
+typedef struct pic_engine_stats {
+  int64_t kernel_launches;   /* kernels this engine launched since the last reset          */
+  int64_t steps;             /* full steps taken since the last reset                      */
+  int64_t vcycles;           /* V-cycle launches since the last reset                      */
+  int64_t mover_launches;    /* fused particle passes timed (profiling on)                 */
+  double mover_ms;           /* their summed CUDA-event time on the launching stream       */
+} pic_engine_stats;
+
 typedef struct pic_engine pic_engine;
 
 /* ---- engine and jobs ---- */
@@ -189,6 +197,9 @@ int pic_step(pic_engine* e, int nsteps, void* stream);
 /* Same, recorded once into a CUDA graph per engine configuration and replayed. */
 int pic_step_graph(pic_engine* e, int nsteps, void* stream);
 int pic_sync(pic_engine* e);
+/* Record CUDA events around every fused particle pass (on the stream it runs on). */
+int pic_engine_profile(pic_engine* e, int enable);
+int pic_engine_get_stats(pic_engine* e, pic_engine_stats* out, int reset);
 int pic_job_diagnostics(pic_engine* e, int job, pic_diagnostics* out);
 
 /* ---- individual phases (parity checks, the compatibility layer) ---- */

@@ -49,6 +49,7 @@ def lib():
             "orc_mg_vcycles": (None, [_D, _D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                       C.c_int, C.c_int]),
             "orc_relres": (C.c_double, [_D, _D, C.c_int, C.c_int, C.c_double]),
+            "orc_set_reference_convergence": (None, [C.c_int]),
             "orc_residual": (None, [_D, _D, _D, C.c_int, C.c_int, C.c_double]),
             "orc_auto_levels": (C.c_int, [C.c_int, C.c_int]),
             "orc_sim_create": (C.c_void_p, [C.c_void_p]),
@@ -144,13 +145,23 @@ def walls_box(x, y, m, n, dx, dy):
     return hit.astype(bool)
 
 
-def mg_solve(phi, f, h, levels=0, omega=1.0, nu1=2, nu2=2, nuc=2, tol=1e-9, max_cycles=50):
+def mg_solve(phi, f, h, levels=0, omega=1.0, nu1=2, nu2=2, nuc=2, tol=1e-9, max_cycles=50, ref_convergence=False):
+    """ref_convergence: stop like the reference (||r|| < tol * ||f||^2, Multigrid.cu:466-467)."""
     phi = f64(phi).copy()
     f = f64(f)
     ny, nx = phi.shape
     rel = C.c_double()
-    cyc = lib().orc_mg_solve(_d(phi), _d(f), nx, ny, levels, h, omega, nu1, nu2, nuc, tol, max_cycles, C.byref(rel))
+    set_reference_convergence(ref_convergence)
+    try:
+        cyc = lib().orc_mg_solve(_d(phi), _d(f), nx, ny, levels, h, omega, nu1, nu2, nuc, tol, max_cycles,
+                                 C.byref(rel))
+    finally:
+        set_reference_convergence(False)
     return phi, cyc, rel.value
+
+
+def set_reference_convergence(on: bool) -> None:
+    lib().orc_set_reference_convergence(1 if on else 0)
 
 
 def mg_vcycles(phi, f, h, cycles, levels=0, omega=1.0, nu1=2, nu2=2, nuc=2):

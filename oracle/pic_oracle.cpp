@@ -348,6 +348,11 @@ static int auto_levels(int nx, int ny) {
 ORC_API int orc_auto_levels(int nx, int ny) { return auto_levels(nx, ny); }
 
 static MgWork g_mg;
+static int g_ref_convergence = 0;
+// conv_mode 1 reproduces the reference's own stopping test: check_convergence_kernel divides
+// ||r|| by the value l2_norm_device left in rhs_norm, which is the SQUARED norm ||rho||^2
+// (Multigrid.cu:413-453, 466-467, 602), so the reference stops at ||r|| < tol ||rho||^2.
+ORC_API void orc_set_reference_convergence(int on) { g_ref_convergence = on; }
 // solve_multigrid (Multigrid.cu:573-642): V-cycles until ||f - A phi|| / ||f|| < tol or
 // max_cycles; the check follows every cycle, so at least one cycle runs.  Returns the
 // number of cycles; relres_out gets the final relative residual.
@@ -357,7 +362,8 @@ ORC_API int orc_mg_solve(double* phi, const double* f, int nx, int ny, int level
   if (levels <= 0) levels = auto_levels(nx, ny);
   g_mg.ensure(nx, ny, levels);
   const int64_t N = (int64_t)nx * ny;
-  const double fn = std::sqrt(norm2sq(f, N));
+  const double fn2 = norm2sq(f, N);
+  const double fn = g_ref_convergence ? fn2 : std::sqrt(fn2);
   std::vector<double> r(N);
   int cyc = 0;
   double rel = 0.0;

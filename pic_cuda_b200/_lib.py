@@ -56,6 +56,11 @@ class Diagnostics(C.Structure):
     ]
 
 
+class EngineStats(C.Structure):
+    _fields_ = [("kernel_launches", C.c_int64), ("steps", C.c_int64), ("vcycles", C.c_int64),
+                ("mover_launches", C.c_int64), ("mover_ms", C.c_double)]
+
+
 class PicError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where} failed with status {code}: {msg}")
@@ -79,6 +84,8 @@ _SIGS = {
     "pic_step": (_I, [_VP, _I, _VP]),
     "pic_step_graph": (_I, [_VP, _I, _VP]),
     "pic_sync": (_I, [_VP]),
+    "pic_engine_profile": (_I, [_VP, _I]),
+    "pic_engine_get_stats": (_I, [_VP, C.POINTER(EngineStats), _I]),
     "pic_job_diagnostics": (_I, [_VP, _I, C.POINTER(Diagnostics)]),
     "pic_job_run_phases": (_I, [_VP, _I, _I, _I64, _VP]),
     "pic_job_compact": (_I, [_VP, _I, _VP]),

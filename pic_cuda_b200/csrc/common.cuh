@@ -117,6 +117,7 @@ struct JobState {
   int pad;
   unsigned long long collisions[PIC_MAX_SPECIES][8];
   double ke[PIC_MAX_SPECIES];
+  double total_charge;     // filled on request (diagnostics)
 };
 
 // ---------------------------------------------------------------- Philox-4x32-10

@@ -83,11 +83,12 @@ __global__ void compact_finish(int* __restrict__ counts, int* __restrict__ hit_c
 
 }  // namespace
 
-void launch_compact(const EngineLaunch& L, cudaStream_t st) {
-  if (L.nslots == 0) return;
+int launch_compact(const EngineLaunch& L, cudaStream_t st) {
+  if (L.nslots == 0) return 0;
   dim3 grid(8, L.nslots);
   compact_mark<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
   compact_lists<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
   compact_move<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
   compact_finish<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.counts, L.hit_counts, L.nslots, L.active, L.absorbed);
+  return 4;
 }

@@ -151,6 +151,22 @@ __global__ void step_end_kernel(JobState* st, int njobs, const uint8_t* job_mask
   st[j].kick_pending = set_pending;
 }
 
+// Sum of rho (charge units) in FP64 with a fixed reduction order (one CTA).
+__global__ void __launch_bounds__(1024) rho_sum_kernel(const JobDev* __restrict__ jd, JobState* st) {
+  const JobDev& J = *jd;
+  const int64_t N = (int64_t)J.nx * J.ny;
+  double s = 0.0;
+  for (int64_t k = threadIdx.x; k < N; k += blockDim.x) s += rho_at(J, k);
+  __shared__ double sh[1024];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 512; o; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st->total_charge = sh[0] * J.qref;
+}
+
 __global__ void zero_rho_all_kernel(const JobDev* __restrict__ jobs, int njobs) {
   const JobDev& J = jobs[blockIdx.y];
   if (J.nslots == 0 && J.nx == 0) return;
@@ -205,14 +221,20 @@ void launch_zero_rho(const JobDev*, int64_t nodes, int deposit_mode, void* rho, 
 void launch_efield_f64(const double* phi, double* exy, int nx, int ny, double dx, double dy, cudaStream_t s) {
   efield_f64_kernel<<<grid_for((int64_t)nx * ny), 256, 0, s>>>(phi, exy, nx, ny, dx, dy);
 }
-void launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s) {
-  if (njobs) step_begin_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(st, jobs, njobs, job_mask);
+int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s) {
+  if (!njobs) return 0;
+  step_begin_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(st, jobs, njobs, job_mask);
+  return 1;
 }
-void launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s) {
-  if (njobs) step_end_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(st, njobs, job_mask, set_pending, advance);
+int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s) {
+  if (!njobs) return 0;
+  step_end_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(st, njobs, job_mask, set_pending, advance);
+  return 1;
 }
-void launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s) {
-  if (!L.njobs) return;
+int launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s) {
+  if (!L.njobs) return 0;
   const int gx = (int)std::min<int64_t>(std::max<int64_t>(((int64_t)max_nodes + 1023) / 1024, 1), 1024);
   zero_rho_all_kernel<<<dim3(gx, L.njobs), 256, 0, s>>>(L.jobs, L.njobs);
+  return 1;
 }
+void launch_rho_sum(const JobDev* jd, JobState* st, cudaStream_t s) { rho_sum_kernel<<<1, 1024, 0, s>>>(jd, st); }

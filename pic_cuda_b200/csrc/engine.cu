@@ -227,6 +227,11 @@ struct pic_engine {
   cudaGraphExec_t graph_exec_sort = nullptr;
   bool graph_dirty = true;
   std::mutex mu;
+  // statistics and optional timing of the particle pass
+  int64_t launches = 0, steps_taken = 0, vcycles = 0;
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> mover_events;
+  size_t mover_events_used = 0;
 };
 
 namespace {
@@ -361,9 +366,10 @@ int ensure_mg_all(pic_engine* E) {
 int solve(pic_engine* E, const MgBuild& B, const uint8_t* active, cudaStream_t s) {
   if (!B.valid) return PIC_OK;
   EngineLaunch L = make_launch(E, active);
-  launch_mg_init(L, B.L, s);
+  E->launches += launch_mg_init(L, B.L, s);
   for (int c = 0; c < B.max_cycles; ++c) {
-    launch_mg_vcycle(L, B.L, s);
+    E->launches += launch_mg_vcycle(L, B.L, s);
+    E->vcycles++;
     CK(cudaMemcpyAsync(E->h_pinned, E->d_running, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*E->h_pinned <= 0) break;
@@ -392,9 +398,9 @@ int flush(pic_engine* E, cudaStream_t s) {
   for (int j = 0; j < E->njobs_hw; ++j) any |= E->jobs[j].alive && E->jobs[j].pending;
   if (!any) return PIC_OK;
   EngineLaunch L = make_launch(E, nullptr);
-  launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_GATED_I, 0, s);
-  launch_ionize(L, false, s);
-  launch_step_end(E->d_st, E->njobs_hw, nullptr, 0, 0, s);
+  E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_GATED_I, 0, s);
+  E->launches += launch_ionize(L, false, s);
+  E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 0, 0, s);
   for (int j = 0; j < E->njobs_hw; ++j) E->jobs[j].pending = false;
   CK(cudaGetLastError());
   return PIC_OK;
@@ -436,20 +442,33 @@ int step_once(pic_engine* E, cudaStream_t s) {
   }
   if (any) {
     CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
-    launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+    E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
   }
-  launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
+  E->launches += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
   int max_nodes = 0;
   for (int j = 0; j < E->njobs_hw; ++j)
     if (E->jobs[j].alive) max_nodes = std::max(max_nodes, E->jobs[j].dev.nx * E->jobs[j].dev.ny);
-  launch_zero_rho_all(L, max_nodes, s);
-  launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
-                      PIC_PHASE_GATED_I, 0, s);
-  launch_compact(L, s);
-  launch_ionize(L, true, s);
+  E->launches += launch_zero_rho_all(L, max_nodes, s);
+  if (E->profile) {
+    if (E->mover_events_used == E->mover_events.size()) {
+      std::pair<cudaEvent_t, cudaEvent_t> ev;
+      CK(cudaEventCreate(&ev.first));
+      CK(cudaEventCreate(&ev.second));
+      E->mover_events.push_back(ev);
+    }
+    L.ev_mover_begin = E->mover_events[E->mover_events_used].first;
+    L.ev_mover_end = E->mover_events[E->mover_events_used].second;
+    E->mover_events_used++;
+  }
+  E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I |
+                                     PIC_PHASE_DEPOSIT_I | PIC_PHASE_GATED_I, 0, s);
+  L.ev_mover_begin = L.ev_mover_end = nullptr;
+  E->launches += launch_compact(L, s);
+  E->launches += launch_ionize(L, true, s);
   int rc = solve(E, E->mg_all, nullptr, s);
   if (rc) return rc;
-  launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
+  E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
+  E->steps_taken++;
   for (int j = 0; j < E->njobs_hw; ++j)
     if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; }
   CK(cudaGetLastError());
@@ -539,6 +558,7 @@ int pic_engine_destroy(pic_engine* E) {
   cudaFree(E->d_jobs); cudaFree(E->d_st); cudaFree(E->d_slots); cudaFree(E->d_counts); cudaFree(E->d_hits);
   cudaFree(E->d_aux); cudaFree(E->d_chunk); cudaFree(E->d_running); cudaFree(E->d_active); cudaFree(E->d_mask);
   if (E->d_stage) cudaFree(E->d_stage);
+  for (auto& ev : E->mover_events) { cudaEventDestroy(ev.first); cudaEventDestroy(ev.second); }
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (E->stream) cudaStreamDestroy(E->stream);
   delete E;
@@ -899,6 +919,35 @@ int pic_step(pic_engine* E, int nsteps, void* stream) {
 
 int pic_step_graph(pic_engine* E, int nsteps, void* stream) { return pic_step(E, nsteps, stream); }
 
+int pic_engine_profile(pic_engine* E, int enable) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  E->profile = enable != 0;
+  return PIC_OK;
+}
+
+int pic_engine_get_stats(pic_engine* E, pic_engine_stats* out, int reset) {
+  if (!E || !out) return fail(PIC_ERR_ARG, "null argument");
+  CK(cudaSetDevice(E->device));
+  std::memset(out, 0, sizeof(*out));
+  out->kernel_launches = E->launches;
+  out->steps = E->steps_taken;
+  out->vcycles = E->vcycles;
+  double ms = 0.0;
+  for (size_t k = 0; k < E->mover_events_used; ++k) {
+    CK(cudaEventSynchronize(E->mover_events[k].second));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, E->mover_events[k].first, E->mover_events[k].second));
+    ms += t;
+  }
+  out->mover_launches = (int64_t)E->mover_events_used;
+  out->mover_ms = ms;
+  if (reset) {
+    E->launches = E->steps_taken = E->vcycles = 0;
+    E->mover_events_used = 0;
+  }
+  return PIC_OK;
+}
+
 int pic_sync(pic_engine* E) {
   if (!E) return fail(PIC_ERR_ARG, "null engine");
   CK(cudaSetDevice(E->device));
@@ -912,34 +961,31 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
   if (rc) return rc;
   if (!out) return fail(PIC_ERR_ARG, "null out");
   CK(cudaSetDevice(E->device));
+  cudaStream_t s = E->stream;
   CK(cudaDeviceSynchronize());
+  launch_rho_sum(E->d_jobs + job, E->d_st + job, s);
   JobState T;
   int cnt[kSlotsPerJob], ab[kSlotsPerJob];
-  CK(cudaMemcpy(&T, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(cnt, E->d_counts + job * kSlotsPerJob, sizeof(cnt), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(ab, E->d_aux + 4 * kMaxJobs * kSlotsPerJob + job * kSlotsPerJob, sizeof(ab), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(&T, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cnt, E->d_counts + job * kSlotsPerJob, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ab, E->d_aux + 4 * kMaxJobs * kSlotsPerJob + job * kSlotsPerJob, sizeof(ab),
+                     cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
   std::memset(out, 0, sizeof(*out));
   JobHost& J = E->jobs[job];
   out->step = T.step;
-  for (int s = 0; s < J.cfg.n_species; ++s) {
-    out->count[s] = cnt[s];
-    out->absorbed[s] = ab[s];
-    out->kinetic_energy[s] = T.ke[s];
-    for (int q = 0; q < PIC_MAX_PROCESSES; ++q) out->collisions[s][q] = q < 8 ? (int64_t)T.collisions[s][q] : 0;
+  for (int k = 0; k < J.cfg.n_species; ++k) {
+    out->count[k] = cnt[k];
+    out->absorbed[k] = ab[k];
+    out->kinetic_energy[k] = T.ke[k];
+    for (int q = 0; q < PIC_MAX_PROCESSES; ++q) out->collisions[k][q] = q < 8 ? (int64_t)T.collisions[k][q] : 0;
   }
   out->ionizations = T.ionizations;
   out->vcycles = T.cycles;
   out->converged = T.converged == 1;
   out->relres = T.relres;
+  out->total_charge = T.total_charge;
   out->status = T.status;
-  // total charge: sum of rho in FP64
-  const int64_t N = (int64_t)J.dev.nx * J.dev.ny;
-  std::vector<double> rho(N);
-  rc = pic_job_get_grid(E, job, PIC_GRID_RHO, rho.data(), PIC_MEM_HOST);
-  if (rc) return rc;
-  double t = 0.0;
-  for (double v : rho) t += v;
-  out->total_charge = t;
   return PIC_OK;
 }
 

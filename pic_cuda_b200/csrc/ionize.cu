@@ -140,8 +140,9 @@ ionize_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const 
 
 }  // namespace
 
-void launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s) {
-  if (L.njobs == 0) return;
+int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s) {
+  if (L.njobs == 0) return 0;
   ionize_kernel<<<L.njobs, 256, 0, s>>>(L.jobs, L.st, L.slots, L.counts, L.absorbed,
                                          drift_and_deposit ? 1 : 0);
+  return 1;
 }

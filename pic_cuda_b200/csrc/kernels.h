@@ -37,16 +37,18 @@ struct EngineLaunch {
   int num_sms;
   int* running;           // jobs whose field solve is still iterating
   int* absorbed;          // particles absorbed in the last step, per slot
+  cudaEvent_t ev_mover_begin, ev_mover_end;  // optional timing of the particle pass
 };
 
-void launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t s);
-void launch_compact(const EngineLaunch& L, cudaStream_t s);
-void launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
-void launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
-void launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
-void launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);
+int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t s);
+int launch_compact(const EngineLaunch& L, cudaStream_t s);
+int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
+int launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
+int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
+int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);
 void launch_pid_max(const SlotDev* slot_dev, int64_t n, JobState* st, cudaStream_t s);
-void launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s);
+int launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s);
+void launch_rho_sum(const JobDev* jd, JobState* st, cudaStream_t s);
 
 // Multigrid (all jobs of a launch at once).
 struct MgLaunch {
@@ -59,8 +61,8 @@ struct MgLaunch {
   size_t coarse_smem;
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
 };
-void launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
-void launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
+int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
+int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 void mg_configure_coarse(size_t smem_bytes);
 
 // Conversions between the public FP64 domain-unit layout and the engine layout.

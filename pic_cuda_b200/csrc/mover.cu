@@ -357,8 +357,11 @@ __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t
   }
 }
 
-void launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t stream) {
+int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t stream) {
   chunk_table_kernel<<<1, 32, 0, stream>>>(L.counts, L.active, L.chunk_prefix, L.nslots);
+  if (L.ev_mover_begin) cudaEventRecord(L.ev_mover_begin, stream);
   mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, 0, stream>>>(L.jobs, L.st, L.slots, L.counts, L.hit_counts,
                                                               L.chunk_prefix, L.nslots, flags, explicit_step);
+  if (L.ev_mover_end) cudaEventRecord(L.ev_mover_end, stream);
+  return 2;
 }

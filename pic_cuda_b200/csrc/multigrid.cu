@@ -382,23 +382,34 @@ size_t up_smem(int nu) { const int W = kTU + 4 * nu + 2; return (size_t)2 * W * 
 }  // namespace
 
 void mg_configure_coarse(size_t smem_bytes) {
-  cudaFuncSetAttribute(mg_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+  // the attribute only grows, so every launch list built so far stays launchable
+  static size_t configured = 0;
+  if (smem_bytes > configured) {
+    cudaFuncSetAttribute(mg_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    configured = smem_bytes;
+  }
   cudaFuncSetAttribute(mg_down_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)down_smem(16));
   cudaFuncSetAttribute(mg_up_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)up_smem(16));
 }
 
-void launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
+int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   cudaMemsetAsync(L.running, 0, sizeof(int), s);
-  if (M.n_init) mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st, L.running);
+  if (!M.n_init) return 0;
+  mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st, L.running);
+  return 1;
 }
 
 
-void launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
+int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
+  int k = 0;
   for (int l = 0; l < M.max_depth; ++l)
-    if (M.n_down[l]) mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l);
-  if (M.n_coarse) mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st);
+    if (M.n_down[l]) { mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l); ++k; }
+  if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
   for (int l = M.max_depth - 1; l >= 0; --l)
-    if (M.n_up[l])
+    if (M.n_up[l]) {
       mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0, L.running);
-  if (M.n_upd) mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running);
+      ++k;
+    }
+  if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
+  return k;
 }

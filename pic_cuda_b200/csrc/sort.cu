@@ -180,8 +180,8 @@ __global__ void sort_swap(SlotDev* slots, const uint8_t* mask, int nslots) {
 
 }  // namespace
 
-void launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
-  if (L.nslots == 0) return;
+int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
+  if (L.nslots == 0) return 0;
   const int ncells = max_cells + 1;
   const int ntiles = (ncells + kTile - 1) / kTile;
   const int gz = std::min(std::max((ncells + 255) / 256, 1), 4 * L.num_sms);
@@ -193,4 +193,5 @@ void launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int 
   sort_apply<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_scatter<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
   sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
+  return 7;
 }

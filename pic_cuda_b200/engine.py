@@ -162,6 +162,14 @@ class Engine:
     def sync(self) -> None:
         L.check(L.lib().pic_sync(self.h), "pic_sync")
 
+    def profile(self, enable: bool = True) -> None:
+        L.check(L.lib().pic_engine_profile(self.h, 1 if enable else 0), "pic_engine_profile")
+
+    def stats(self, reset: bool = False) -> dict:
+        st = L.EngineStats()
+        L.check(L.lib().pic_engine_get_stats(self.h, C.byref(st), 1 if reset else 0), "pic_engine_get_stats")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
     def close(self) -> None:
         if self.h:
             L.lib().pic_engine_destroy(self.h)
