@@ -163,6 +163,8 @@ typedef struct pic_engine_stats {
   int64_t vcycles;           /* V-cycle launches since the last reset                      */
   int64_t mover_launches;    /* fused particle passes timed (profiling on)                 */
   double mover_ms;           /* their summed CUDA-event time on the launching stream       */
+  double phase_ms[4];        /* summed event time per phase: sort, particle pass,          */
+                             /* compaction + ionisation, field solve (profiling on)        */
 } pic_engine_stats;
 
 typedef struct pic_engine pic_engine;

@@ -58,7 +58,7 @@ class Diagnostics(C.Structure):
 
 class EngineStats(C.Structure):
     _fields_ = [("kernel_launches", C.c_int64), ("steps", C.c_int64), ("vcycles", C.c_int64),
-                ("mover_launches", C.c_int64), ("mover_ms", C.c_double)]
+                ("mover_launches", C.c_int64), ("mover_ms", C.c_double), ("phase_ms", C.c_double * 4)]
 
 
 class PicError(RuntimeError):

@@ -18,7 +18,7 @@
 
 #define PIC_CELL_OUT 0xFFFFFFFFu
 #define PIC_MAX_LEVELS 14
-#define PIC_COARSE_MAX 129          // levels with n <= this are solved by one CTA in smem
+#define PIC_COARSE_MAX 33           // levels with n <= this are solved by one CTA in smem
 #define PIC_CHUNK 1024              // particles per mover work item (256 threads x 4)
 #define PIC_MOVER_THREADS 256
 #define PIC_FIX_SHIFT 40            // int64 deposit: 2^40 per unit deposit charge
@@ -89,6 +89,7 @@ struct JobDev {
   int ion_e_species, ion_i_species;
   uint64_t seed;
   int slot0, nslots;
+  int sort_every;
   // ionisation events
   struct Event* events;
   int event_capacity;

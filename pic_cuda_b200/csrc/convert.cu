@@ -151,20 +151,30 @@ __global__ void step_end_kernel(JobState* st, int njobs, const uint8_t* job_mask
   st[j].kick_pending = set_pending;
 }
 
-// Sum of rho (charge units) in FP64 with a fixed reduction order (one CTA).
-__global__ void __launch_bounds__(1024) rho_sum_kernel(const JobDev* __restrict__ jd, JobState* st) {
+// Sum of rho (charge units) in FP64 with a fixed reduction order: per-CTA partial sums,
+// then one CTA adds them in index order.
+__global__ void __launch_bounds__(256) rho_sum_partial_kernel(const JobDev* __restrict__ jd, double* part) {
   const JobDev& J = *jd;
   const int64_t N = (int64_t)J.nx * J.ny;
   double s = 0.0;
-  for (int64_t k = threadIdx.x; k < N; k += blockDim.x) s += rho_at(J, k);
-  __shared__ double sh[1024];
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x)
+    s += rho_at(J, k);
+  __shared__ double sh[256];
   sh[threadIdx.x] = s;
   __syncthreads();
-  for (int o = 512; o; o >>= 1) {
+  for (int o = 128; o; o >>= 1) {
     if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) st->total_charge = sh[0] * J.qref;
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void rho_sum_final_kernel(const JobDev* __restrict__ jd, const double* part, int nparts, JobState* st) {
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int k = 0; k < nparts; ++k) s += part[k];
+    st->total_charge = s * jd->qref;
+  }
 }
 
 __global__ void zero_rho_all_kernel(const JobDev* __restrict__ jobs, int njobs) {
@@ -237,4 +247,7 @@ int launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s) {
   zero_rho_all_kernel<<<dim3(gx, L.njobs), 256, 0, s>>>(L.jobs, L.njobs);
   return 1;
 }
-void launch_rho_sum(const JobDev* jd, JobState* st, cudaStream_t s) { rho_sum_kernel<<<1, 1024, 0, s>>>(jd, st); }
+void launch_rho_sum(const JobDev* jd, JobState* st, double* scratch, int nparts, cudaStream_t s) {
+  rho_sum_partial_kernel<<<nparts, 256, 0, s>>>(jd, scratch);
+  rho_sum_final_kernel<<<1, 32, 0, s>>>(jd, scratch, nparts, st);
+}

@@ -207,6 +207,7 @@ struct pic_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
   int num_sms = 148;
+  int mover_bps = 4;
   int64_t pool_bytes = 0, used_bytes = 0;
   std::vector<JobHost> jobs;
   int njobs_hw = 0;
@@ -216,22 +217,32 @@ struct pic_engine {
   int *d_counts = nullptr, *d_hits = nullptr, *d_aux = nullptr, *d_chunk = nullptr, *d_running = nullptr;
   uint8_t *d_active = nullptr, *d_mask = nullptr;
   int* h_pinned = nullptr;
+  double* d_diag = nullptr;  // per-CTA partial sums of the diagnostics reductions
   MgBuild mg_all;
   bool mg_dirty = true;
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
   std::vector<uint8_t> h_active;
   int max_nu_pre = 0, max_nu_post = 0;
-  // CUDA graph of one step (pic_step_graph)
+  // CUDA graphs of one step (pic_step_graph): without and with the counting sort
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraphExec_t graph_exec_sort = nullptr;
   bool graph_dirty = true;
+  cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+  int* d_loop = nullptr;                    // [0] iterations of the current solve
+  unsigned long long* d_loop_total = nullptr;  // V-cycle iterations run by graph launches
+  int64_t graph_fixed_launches[2] = {0, 0};
+  int64_t graph_body_launches = 0;
+  int64_t graph_steps = 0;
   std::mutex mu;
   // statistics and optional timing of the particle pass
   int64_t launches = 0, steps_taken = 0, vcycles = 0;
   bool profile = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> mover_events;
   size_t mover_events_used = 0;
+  // per-phase timing (profile mode): sort, mover, compaction+ionisation, field solve
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> phase_events[4];
+  size_t phase_used[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -250,7 +261,7 @@ EngineLaunch make_launch(pic_engine* E, const uint8_t* active) {
   L.nslots = E->njobs_hw * kSlotsPerJob;
   L.njobs = E->njobs_hw;
   L.num_sms = E->num_sms;
-  L.mover_grid = E->num_sms * 8;
+  L.mover_grid = E->num_sms * E->mover_bps;
   L.running = E->d_running;
   L.absorbed = E->d_aux + 4 * kMaxJobs * kSlotsPerJob;
   return L;
@@ -393,6 +404,25 @@ int job_mask(pic_engine* E, int job, cudaStream_t s) {
 
 cudaStream_t pick(pic_engine* E, void* s) { return s ? (cudaStream_t)s : E->stream; }
 
+// Begin/end of a timed phase (profile mode only).
+int phase_mark(pic_engine* E, int ph, bool begin, cudaStream_t s) {
+  if (!E->profile) return PIC_OK;
+  auto& v = E->phase_events[ph];
+  if (begin) {
+    if (E->phase_used[ph] == v.size()) {
+      std::pair<cudaEvent_t, cudaEvent_t> ev;
+      CK(cudaEventCreate(&ev.first));
+      CK(cudaEventCreate(&ev.second));
+      v.push_back(ev);
+    }
+    CK(cudaEventRecord(v[E->phase_used[ph]].first, s));
+  } else {
+    CK(cudaEventRecord(v[E->phase_used[ph]].second, s));
+    E->phase_used[ph]++;
+  }
+  return PIC_OK;
+}
+
 int flush(pic_engine* E, cudaStream_t s) {
   bool any = false;
   for (int j = 0; j < E->njobs_hw; ++j) any |= E->jobs[j].alive && E->jobs[j].pending;
@@ -442,7 +472,9 @@ int step_once(pic_engine* E, cudaStream_t s) {
   }
   if (any) {
     CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
+    phase_mark(E, 0, true, s);
     E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+    phase_mark(E, 0, false, s);
   }
   E->launches += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
   int max_nodes = 0;
@@ -463,15 +495,112 @@ int step_once(pic_engine* E, cudaStream_t s) {
   E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I |
                                      PIC_PHASE_DEPOSIT_I | PIC_PHASE_GATED_I, 0, s);
   L.ev_mover_begin = L.ev_mover_end = nullptr;
+  phase_mark(E, 2, true, s);
   E->launches += launch_compact(L, s);
   E->launches += launch_ionize(L, true, s);
+  phase_mark(E, 2, false, s);
+  phase_mark(E, 3, true, s);
   int rc = solve(E, E->mg_all, nullptr, s);
   if (rc) return rc;
+  phase_mark(E, 3, false, s);
   E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
   E->steps_taken++;
   for (int j = 0; j < E->njobs_hw; ++j)
     if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; }
   CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+// Records one full step of every live job into a CUDA graph.  The V-cycle loop of the field
+// solve is a conditional WHILE node: its body is the V-cycle plus a one-thread kernel that
+// keeps the loop going while any job is still iterating (bounded by max_cycles), so a step
+// runs without any host synchronisation.
+int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_t* fixed_launches) {
+  cudaStream_t s = E->cap_stream;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  EngineLaunch L = make_launch(E, nullptr);
+  int64_t n = 0;
+  int max_nodes = 0;
+  for (int j = 0; j < E->njobs_hw; ++j)
+    if (E->jobs[j].alive) max_nodes = std::max(max_nodes, E->jobs[j].dev.nx * E->jobs[j].dev.ny);
+  cudaError_t err = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) { cudaGraphDestroy(g); return fail(PIC_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(err)); }
+  if (with_sort) {
+    int max_cells = 0;
+    int64_t max_p = 0;
+    for (int j = 0; j < E->njobs_hw; ++j) {
+      JobHost& J = E->jobs[j];
+      if (!J.alive || J.cfg.sort_every <= 0) continue;
+      for (int k = 0; k < J.cfg.n_species; ++k) max_p = std::max<int64_t>(max_p, J.cfg.species[k].capacity);
+      max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
+    }
+    n += launch_sort_mask(L, E->d_mask, s);
+    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+  }
+  n += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
+  n += launch_zero_rho_all(L, max_nodes, s);
+  n += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
+                           PIC_PHASE_GATED_I, 0, s);
+  n += launch_compact(L, s);
+  n += launch_ionize(L, true, s);
+  n += launch_mg_init(L, E->mg_all.L, s);
+  cudaMemsetAsync(E->d_loop, 0, sizeof(int), s);
+  // conditional WHILE node for the V-cycles
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+  cudaGraphConditionalHandle h;
+  if (err == cudaSuccess) err = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
+  cudaGraphNode_t cnode = nullptr;
+  alignas(cudaGraphNodeParams) unsigned char pbuf[sizeof(cudaGraphNodeParams)];
+  std::memset(pbuf, 0, sizeof(pbuf));
+  cudaGraphNodeParams& p = *reinterpret_cast<cudaGraphNodeParams*>(pbuf);
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  if (err == cudaSuccess) err = cudaGraphAddNode(&cnode, cg, deps, ndeps, &p);
+  int64_t body = 0;
+  if (err == cudaSuccess) {
+    cudaGraph_t bg = p.conditional.phGraph_out[0];
+    err = cudaStreamBeginCaptureToGraph(E->body_stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      EngineLaunch LB = L;
+      body += launch_mg_vcycle(LB, E->mg_all.L, E->body_stream);
+      body += launch_vcycle_condition(h, E->d_running, E->d_loop, E->mg_all.max_cycles, E->d_loop_total,
+                                      E->body_stream);
+      cudaGraph_t tmp = nullptr;
+      err = cudaStreamEndCapture(E->body_stream, &tmp);
+    }
+  }
+  if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+  if (err == cudaSuccess) n += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
+  cudaGraph_t done = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(s, &done);
+  if (err == cudaSuccess) err = e2;
+  if (err == cudaSuccess) err = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (err != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PIC_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(err));
+  }
+  *fixed_launches = n;
+  E->graph_body_launches = body;
+  return PIC_OK;
+}
+
+int ensure_graphs(pic_engine* E) {
+  if (!E->graph_dirty && E->graph_exec && E->graph_exec_sort) return PIC_OK;
+  if (E->graph_exec) { cudaGraphExecDestroy(E->graph_exec); E->graph_exec = nullptr; }
+  if (E->graph_exec_sort) { cudaGraphExecDestroy(E->graph_exec_sort); E->graph_exec_sort = nullptr; }
+  int rc = build_step_graph(E, false, &E->graph_exec, &E->graph_fixed_launches[0]);
+  if (rc) return rc;
+  rc = build_step_graph(E, true, &E->graph_exec_sort, &E->graph_fixed_launches[1]);
+  if (rc) return rc;
+  E->graph_dirty = false;
   return PIC_OK;
 }
 
@@ -515,6 +644,7 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
   E->device = device;
   E->pool_bytes = pool_bytes;
   cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, device);
+  E->mover_bps = mover_blocks_per_sm();
   const int nslots = kMaxJobs * kSlotsPerJob;
   cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_jobs, sizeof(JobDev) * kMaxJobs);
@@ -528,6 +658,12 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
   if (e == cudaSuccess) e = cudaMalloc(&E->d_active, nslots);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_mask, nslots);
   if (e == cudaSuccess) e = cudaHostAlloc(&E->h_pinned, 64, cudaHostAllocDefault);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_diag, sizeof(double) * 1024);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_loop, sizeof(int) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&E->d_loop_total, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(E->d_loop_total, 0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(E->d_counts, 0, sizeof(int) * nslots);
   if (e == cudaSuccess) e = cudaMemset(E->d_hits, 0, sizeof(int) * nslots);
   if (e == cudaSuccess) e = cudaMemset(E->d_aux, 0, sizeof(int) * 5 * nslots);
@@ -555,10 +691,17 @@ int pic_engine_destroy(pic_engine* E) {
   E->mg_all.release();
   if (E->graph_exec) cudaGraphExecDestroy(E->graph_exec);
   if (E->graph_exec_sort) cudaGraphExecDestroy(E->graph_exec_sort);
+  if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
+  if (E->body_stream) cudaStreamDestroy(E->body_stream);
+  if (E->d_loop) cudaFree(E->d_loop);
+  if (E->d_loop_total) cudaFree(E->d_loop_total);
   cudaFree(E->d_jobs); cudaFree(E->d_st); cudaFree(E->d_slots); cudaFree(E->d_counts); cudaFree(E->d_hits);
   cudaFree(E->d_aux); cudaFree(E->d_chunk); cudaFree(E->d_running); cudaFree(E->d_active); cudaFree(E->d_mask);
+  cudaFree(E->d_diag);
   if (E->d_stage) cudaFree(E->d_stage);
   for (auto& ev : E->mover_events) { cudaEventDestroy(ev.first); cudaEventDestroy(ev.second); }
+  for (int ph = 0; ph < 4; ++ph)
+    for (auto& ev : E->phase_events[ph]) { cudaEventDestroy(ev.first); cudaEventDestroy(ev.second); }
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (E->stream) cudaStreamDestroy(E->stream);
   delete E;
@@ -624,6 +767,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   D.seed = c.seed;
   D.slot0 = id * kSlotsPerJob;
   D.nslots = c.n_species;
+  D.sort_every = c.sort_every;
   const int64_t N = (int64_t)c.nx * c.ny;
   auto A = [&](void** p, size_t b) { return dev_alloc(E, J, p, b); };
 #define ALLOC(ptr, bytes)                                  \
@@ -917,7 +1061,31 @@ int pic_step(pic_engine* E, int nsteps, void* stream) {
   return PIC_OK;
 }
 
-int pic_step_graph(pic_engine* E, int nsteps, void* stream) { return pic_step(E, nsteps, stream); }
+int pic_step_graph(pic_engine* E, int nsteps, void* stream) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  if (nsteps < 0) return fail(PIC_ERR_ARG, "negative nsteps");
+  std::lock_guard<std::mutex> lk(E->mu);
+  CK(cudaSetDevice(E->device));
+  int rc = ensure_mg_all(E);
+  if (rc) return rc;
+  rc = ensure_graphs(E);
+  if (rc) return rc;
+  cudaStream_t s = pick(E, stream);
+  for (int k = 0; k < nsteps; ++k) {
+    bool sort_due = false;
+    for (int j = 0; j < E->njobs_hw; ++j) {
+      const JobHost& J = E->jobs[j];
+      if (J.alive && J.cfg.sort_every > 0 && J.steps % J.cfg.sort_every == 0) sort_due = true;
+    }
+    CK(cudaGraphLaunch(sort_due ? E->graph_exec_sort : E->graph_exec, s));
+    E->launches += E->graph_fixed_launches[sort_due ? 1 : 0];
+    E->graph_steps++;
+    E->steps_taken++;
+    for (int j = 0; j < E->njobs_hw; ++j)
+      if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; }
+  }
+  return PIC_OK;
+}
 
 int pic_engine_profile(pic_engine* E, int enable) {
   if (!E) return fail(PIC_ERR_ARG, "null engine");
@@ -929,9 +1097,11 @@ int pic_engine_get_stats(pic_engine* E, pic_engine_stats* out, int reset) {
   if (!E || !out) return fail(PIC_ERR_ARG, "null argument");
   CK(cudaSetDevice(E->device));
   std::memset(out, 0, sizeof(*out));
-  out->kernel_launches = E->launches;
+  unsigned long long loops = 0;
+  CK(cudaMemcpy(&loops, E->d_loop_total, sizeof(loops), cudaMemcpyDeviceToHost));
+  out->kernel_launches = E->launches + (int64_t)loops * E->graph_body_launches;
   out->steps = E->steps_taken;
-  out->vcycles = E->vcycles;
+  out->vcycles = E->vcycles + (int64_t)loops;
   double ms = 0.0;
   for (size_t k = 0; k < E->mover_events_used; ++k) {
     CK(cudaEventSynchronize(E->mover_events[k].second));
@@ -941,9 +1111,22 @@ int pic_engine_get_stats(pic_engine* E, pic_engine_stats* out, int reset) {
   }
   out->mover_launches = (int64_t)E->mover_events_used;
   out->mover_ms = ms;
+  for (int ph = 0; ph < 4; ++ph) {
+    double t = 0.0;
+    for (size_t k = 0; k < E->phase_used[ph]; ++k) {
+      CK(cudaEventSynchronize(E->phase_events[ph][k].second));
+      float x = 0.f;
+      CK(cudaEventElapsedTime(&x, E->phase_events[ph][k].first, E->phase_events[ph][k].second));
+      t += x;
+    }
+    out->phase_ms[ph] = t;
+  }
+  out->phase_ms[1] = ms;
   if (reset) {
     E->launches = E->steps_taken = E->vcycles = 0;
+    CK(cudaMemset(E->d_loop_total, 0, sizeof(unsigned long long)));
     E->mover_events_used = 0;
+    for (int ph = 0; ph < 4; ++ph) E->phase_used[ph] = 0;
   }
   return PIC_OK;
 }
@@ -963,7 +1146,7 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
   CK(cudaSetDevice(E->device));
   cudaStream_t s = E->stream;
   CK(cudaDeviceSynchronize());
-  launch_rho_sum(E->d_jobs + job, E->d_st + job, s);
+  launch_rho_sum(E->d_jobs + job, E->d_st + job, E->d_diag, std::min(1024, 2 * E->num_sms), s);
   JobState T;
   int cnt[kSlotsPerJob], ab[kSlotsPerJob];
   CK(cudaMemcpyAsync(&T, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost, s));

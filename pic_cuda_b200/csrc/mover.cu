@@ -149,195 +149,292 @@ __device__ __forceinline__ void warp_deposit(const JobDev& J, const SlotDev& S, 
   }
 }
 
-__global__ void __launch_bounds__(PIC_MOVER_THREADS)
+constexpr int kTileCap = 8192;   // phi tile (floats) staged per chunk
+constexpr int kRounds = PIC_CHUNK / PIC_MOVER_THREADS;
+constexpr int kWarps = PIC_MOVER_THREADS / 32;
+
+// One real-or-null collision of a null-collision candidate (Vahedi & Surendra 1995): the
+// candidate's process is chosen with u1 * nu_max against the cumulative n sigma_j(E) v.
+__device__ void collide(const JobDev& J, const SlotDev& S, const SlotDev* slots, JobState& T, uint32_t pid,
+                        uint32_t cell, float fx, float fy, float& vx, float& vy, float& vz, const float u[4],
+                        uint32_t step, unsigned* proc_count) {
+  const float v2 = vx * vx + vy * vy + vz * vz;
+  const float sp = sqrtf(v2);
+  const float E = S.half_m_over_e * v2;
+  const float target = u[1] * S.numax;
+  float acc = 0.f;
+  int chosen = -1;
+  for (int q = 0; q < S.n_proc; ++q) {
+    acc += J.gas_density * xs_lookup(J.procs[S.first_proc + q], E) * sp;
+    if (target < acc) { chosen = q; break; }
+  }
+  if (chosen < 0) return;
+  const ProcDev& P = J.procs[S.first_proc + chosen];
+  float d[3];
+  if (P.type == PIC_PROC_ELASTIC) {
+    iso_dir(u[2], u[3], d);
+    const float cosx = sp > 0.f ? (vx * d[0] + vy * d[1] + vz * d[2]) / sp : 1.f;
+    const float Ep = E * (1.f - 2.f * S.mass / J.gas_mass * (1.f - cosx));
+    const float vn = sqrtf(fmaxf(0.f, Ep) / S.half_m_over_e);
+    vx = vn * d[0]; vy = vn * d[1]; vz = vn * d[2];
+  } else if (P.type == PIC_PROC_EXCITATION) {
+    if (E < P.threshold) return;
+    iso_dir(u[2], u[3], d);
+    const float vn = sqrtf((E - P.threshold) / S.half_m_over_e);
+    vx = vn * d[0]; vy = vn * d[1]; vz = vn * d[2];
+  } else if (P.type == PIC_PROC_IONIZATION) {
+    if (E < P.threshold) return;
+    float u2[4];
+    draw4(J.seed, pid, step, 1u, u2);
+    const float Er = E - P.threshold, B = 10.f;
+    const float Eej = B * tanf(u2[0] * atanf(Er / (2.f * B)));
+    const float Esc = fmaxf(0.f, Er - Eej);
+    iso_dir(u[2], u[3], d);
+    const float vs = sqrtf(Esc / S.half_m_over_e);
+    Event ev;
+    ev.parent_pid = pid; ev.cell = cell; ev.fx = fx; ev.fy = fy;
+    float d2[3];
+    iso_dir(u2[1], u2[2], d2);
+    const SlotDev& SE = slots[J.slot0 + J.ion_e_species];
+    const float ve = sqrtf(Eej / SE.half_m_over_e);
+    ev.ve[0] = ve * d2[0]; ev.ve[1] = ve * d2[1]; ev.ve[2] = ve * d2[2];
+    neutral_velocity(J.seed, pid, step, J.vth_neutral, ev.vi);
+    const int k = atomicAdd(&T.event_count, 1);
+    if (k < J.event_capacity) J.events[k] = ev;
+    else atomicOr(&T.status, PIC_ST_EVENTS);
+    vx = vs * d[0]; vy = vs * d[1]; vz = vs * d[2];
+  } else if (P.type == PIC_PROC_CHARGE_EXCHANGE) {
+    float vn[3];
+    neutral_velocity(J.seed, pid, step, J.vth_neutral, vn);
+    vx = vn[0]; vy = vn[1]; vz = vn[2];
+  }
+  atomicAdd(&proc_count[chosen & 7], 1u);
+}
+
+// E at the four nodes of cell (i,j) from a phi tile (rows ty0.., cols tx0.., width tw) in
+// shared memory; same stencils as gather_dphi.
+__device__ __forceinline__ void gather_tile(const float* tile, int tw, int tx0, int ty0, int nx, int ny, int i, int j,
+                                            float fx, float fy, float& gx, float& gy) {
+  const int xl = i > 0 ? i - 1 : 0, xr = (i + 2 < nx) ? i + 2 : nx - 1;
+  const float sx0 = i > 0 ? 0.5f : 1.0f, sx1 = (i + 2 < nx) ? 0.5f : 1.0f;
+  const int yl = j > 0 ? j - 1 : 0, yr = (j + 2 < ny) ? j + 2 : ny - 1;
+  const float sy0 = j > 0 ? 0.5f : 1.0f, sy1 = (j + 2 < ny) ? 0.5f : 1.0f;
+  const float* r0 = tile + (j - ty0) * tw - tx0;
+  const float* r1 = r0 + tw;
+  const float a_l = r0[xl], a_0 = r0[i], a_1 = r0[i + 1], a_r = r0[xr];
+  const float b_l = r1[xl], b_0 = r1[i], b_1 = r1[i + 1], b_r = r1[xr];
+  const float* rl = tile + (yl - ty0) * tw - tx0;
+  const float* rr = tile + (yr - ty0) * tw - tx0;
+  const float c_0 = rl[i], c_1 = rl[i + 1], d_0 = rr[i], d_1 = rr[i + 1];
+  const float ex00 = (a_l - a_1) * sx0, ex10 = (a_0 - a_r) * sx1;
+  const float ex01 = (b_l - b_1) * sx0, ex11 = (b_0 - b_r) * sx1;
+  const float ey00 = (c_0 - b_0) * sy0, ey10 = (c_1 - b_1) * sy0;
+  const float ey01 = (a_0 - d_0) * sy1, ey11 = (a_1 - d_1) * sy1;
+  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+  gx = w00 * ex00 + w10 * ex10 + w01 * ex01 + w11 * ex11;
+  gy = w00 * ey00 + w10 * ey10 + w01 * ey01 + w11 * ey11;
+}
+
+// One chunk = PIC_CHUNK particles of one slot; thread t handles particles base + r*256 + t.
+//  pass A  kick (phi tile staged in shared memory when the chunk's cells fit) and the
+//          null-collision candidate test; velocities are stored, candidates (~nu_max dt of
+//          the particles) are listed per warp and collided by that warp's lanes afterwards,
+//          so the long collision code runs once per list instead of once per divergent lane
+//  pass B  drift, absorption, hit list and CIC deposit, re-reading the chunk from L1/L2
+// The slot and job tables are copied to shared memory per chunk: every parameter read in
+// the per-particle code is a shared-memory load.
+__global__ void __launch_bounds__(PIC_MOVER_THREADS, 4)
 mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
              const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ chunk_prefix,
              int nslots, int flags, uint32_t explicit_step) {
+  __shared__ float tile[kTileCap];
+  __shared__ int wlist[kWarps][PIC_CHUNK / kWarps];
+  __shared__ int wcount[kWarps];
+  __shared__ int bb[4];
+  __shared__ unsigned proc_count[8];
+  __shared__ double ke_sh[kWarps];
+  __shared__ SlotDev sS;
+  __shared__ JobDev sJ;
+  __shared__ int cur_slot;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int total = chunk_prefix[nslots];
+  if (t == 0) cur_slot = -1;
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    // chunk -> slot (binary search on the exclusive prefix)
     int lo = 0, hi = nslots - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (chunk_prefix[mid] <= g) lo = mid; else hi = mid - 1;
     }
     const int s = lo;
-    const SlotDev& S = slots[s];
-    const JobDev& J = jobs[S.job];
+    __syncthreads();
+    if (cur_slot != s) {  // copy the slot and job tables to shared memory
+      const int* srcS = reinterpret_cast<const int*>(slots + s);
+      const int* srcJ = reinterpret_cast<const int*>(jobs + slots[s].job);
+      int* dS = reinterpret_cast<int*>(&sS);
+      int* dJ = reinterpret_cast<int*>(&sJ);
+      for (int k = t; k < (int)(sizeof(SlotDev) / 4); k += PIC_MOVER_THREADS) dS[k] = srcS[k];
+      for (int k = t; k < (int)(sizeof(JobDev) / 4); k += PIC_MOVER_THREADS) dJ[k] = srcJ[k];
+    }
+    __syncthreads();
+    if (t == 0) cur_slot = s;
+    const SlotDev& S = sS;
+    const JobDev& J = sJ;
     JobState& T = st[S.job];
     const int n = counts[s];
-    const int base = (g - chunk_prefix[s]) * PIC_CHUNK + 4 * threadIdx.x;
-
+    const int base = (g - chunk_prefix[s]) * PIC_CHUNK;
     const bool gated = flags & PIC_PHASE_GATED_I;
     const bool pending = T.kick_pending != 0;
     const bool do_kick = (flags & PIC_PHASE_KICK_I) && (!gated || pending);
-    const bool do_mcc = (flags & PIC_PHASE_MCC_I) && (!gated || pending) && J.mcc_mode != 0 &&
-                        (J.mcc_mode == 2 ? S.n_proc > 0 : S.n_proc > 0);
+    const bool do_mcc = (flags & PIC_PHASE_MCC_I) && (!gated || pending) && J.mcc_mode != 0 && S.n_proc > 0;
     const bool do_drift = flags & PIC_PHASE_DRIFT_I;
     const bool do_walls = (flags & PIC_PHASE_WALLS_I) && J.wall_mode != 0;
     const bool do_dep = flags & PIC_PHASE_DEPOSIT_I;
     const uint32_t mcc_step = gated ? (uint32_t)(T.step - 1) : explicit_step;
 
-    // vector loads (arrays are allocated in whole chunks, so the tail is in bounds)
-    const uint4 c4 = *reinterpret_cast<const uint4*>(S.cell + base);
-    const float4 fx4 = *reinterpret_cast<const float4*>(S.fx + base);
-    const float4 fy4 = *reinterpret_cast<const float4*>(S.fy + base);
-    float4 vx4 = *reinterpret_cast<const float4*>(S.vx + base);
-    float4 vy4 = *reinterpret_cast<const float4*>(S.vy + base);
-    float4 vz4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    uint4 pid4 = make_uint4(0, 0, 0, 0);
-    if (do_mcc) {
-      vz4 = *reinterpret_cast<const float4*>(S.vz + base);
-      pid4 = *reinterpret_cast<const uint4*>(S.pid + base);
-    }
-    uint32_t cl[4] = {c4.x, c4.y, c4.z, c4.w};
-    float px[4] = {fx4.x, fx4.y, fx4.z, fx4.w}, py[4] = {fy4.x, fy4.y, fy4.z, fy4.w};
-    float vx[4] = {vx4.x, vx4.y, vx4.z, vx4.w}, vy[4] = {vy4.x, vy4.y, vy4.z, vy4.w};
-    float vz[4] = {vz4.x, vz4.y, vz4.z, vz4.w};
-    const uint32_t pd[4] = {pid4.x, pid4.y, pid4.z, pid4.w};
-    double ke = 0.0;
-    unsigned ncoll[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    PhiGather pg{J.phi32, J.nx, J.ny};
-
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int p = base + r;
-      const bool valid = p < n;
-      uint32_t c = cl[r];
-      const bool in_grid = valid && c != PIC_CELL_OUT;
-      const int i = in_grid ? cell_i(c) : 0, j = in_grid ? cell_j(c) : 0;
-      // ---- kick
-      if (do_kick && in_grid) {
-        float gx, gy;
-        gather_dphi(pg, i, j, px[r], py[r], gx, gy);
-        vx[r] += S.kx * gx;
-        vy[r] += S.ky * gy;
-      }
-      // ---- collisions
-      if (do_mcc && valid) {
-        float u[4];
-        draw4(J.seed, pd[r], mcc_step, 0u, u);
-        if (J.mcc_mode == 2) {
-          const ProcDev& P = J.procs[S.first_proc];
-          const float v2 = vx[r] * vx[r] + vy[r] * vy[r];
-          const float sp = sqrtf(v2);
-          const float E = S.half_m_over_e * v2;
-          const float Pc = 1.f - expf(-J.gas_density * xs_lookup(P, E) * sp * J.dt);
-          if (u[0] < Pc) {
-            float sn, cs;
-            sincospif(2.f * u[1], &sn, &cs);
-            vx[r] = sp * cs; vy[r] = sp * sn;
-            ncoll[0]++;
-          }
-        } else if (u[0] < S.pnull) {
-          const float v2 = vx[r] * vx[r] + vy[r] * vy[r] + vz[r] * vz[r];
-          const float sp = sqrtf(v2);
-          const float E = S.half_m_over_e * v2;
-          const float target = u[1] * S.numax;
-          float acc = 0.f;
-          int chosen = -1;
-          for (int q = 0; q < S.n_proc; ++q) {
-            acc += J.gas_density * xs_lookup(J.procs[S.first_proc + q], E) * sp;
-            if (target < acc) { chosen = q; break; }
-          }
-          if (chosen >= 0) {
-            const ProcDev& P = J.procs[S.first_proc + chosen];
-            float d[3];
-            bool real = true;
-            if (P.type == 1) {  // elastic
-              iso_dir(u[2], u[3], d);
-              const float cosx = sp > 0.f ? (vx[r] * d[0] + vy[r] * d[1] + vz[r] * d[2]) / sp : 1.f;
-              const float Ep = E * (1.f - 2.f * S.mass / J.gas_mass * (1.f - cosx));
-              const float vn = sqrtf(fmaxf(0.f, Ep) / S.half_m_over_e);
-              vx[r] = vn * d[0]; vy[r] = vn * d[1]; vz[r] = vn * d[2];
-            } else if (P.type == 2) {  // excitation
-              if (E < P.threshold) real = false;
-              else {
-                iso_dir(u[2], u[3], d);
-                const float vn = sqrtf((E - P.threshold) / S.half_m_over_e);
-                vx[r] = vn * d[0]; vy[r] = vn * d[1]; vz[r] = vn * d[2];
-              }
-            } else if (P.type == 3) {  // ionisation
-              if (E < P.threshold) real = false;
-              else {
-                float u2[4];
-                draw4(J.seed, pd[r], mcc_step, 1u, u2);
-                const float Er = E - P.threshold, B = 10.f;
-                const float Eej = B * tanf(u2[0] * atanf(Er / (2.f * B)));
-                const float Esc = fmaxf(0.f, Er - Eej);
-                iso_dir(u[2], u[3], d);
-                const float vs = sqrtf(Esc / S.half_m_over_e);
-                Event ev;
-                ev.parent_pid = pd[r]; ev.cell = c; ev.fx = px[r]; ev.fy = py[r];
-                float d2[3];
-                iso_dir(u2[1], u2[2], d2);
-                const SlotDev& SE = slots[J.slot0 + J.ion_e_species];
-                const float ve = sqrtf(Eej / SE.half_m_over_e);
-                ev.ve[0] = ve * d2[0]; ev.ve[1] = ve * d2[1]; ev.ve[2] = ve * d2[2];
-                neutral_velocity(J.seed, pd[r], mcc_step, J.vth_neutral, ev.vi);
-                const int k = atomicAdd(&T.event_count, 1);
-                if (k < J.event_capacity) J.events[k] = ev;
-                else atomicOr(&T.status, PIC_ST_EVENTS);
-                vx[r] = vs * d[0]; vy[r] = vs * d[1]; vz[r] = vs * d[2];
-              }
-            } else if (P.type == 4) {  // charge exchange
-              float vn[3];
-              neutral_velocity(J.seed, pd[r], mcc_step, J.vth_neutral, vn);
-              vx[r] = vn[0]; vy[r] = vn[1]; vz[r] = vn[2];
-            }
-            if (real) ncoll[chosen & 7]++;
+    // ---- phi tile of the chunk (bounding box of the cells + 1 node below, 2 above)
+    bool use_tile = false;
+    int tx0 = 0, ty0 = 0, tw = 0;
+    if (do_kick) {
+      int imin = 1 << 30, imax = -1, jmin = 1 << 30, jmax = -1;
+      for (int r = 0; r < kRounds; ++r) {
+        const int p = base + r * PIC_MOVER_THREADS + t;
+        if (p < n) {
+          const uint32_t c = S.cell[p];
+          if (c != PIC_CELL_OUT) {
+            const int i = cell_i(c), j = cell_j(c);
+            imin = min(imin, i); imax = max(imax, i); jmin = min(jmin, j); jmax = max(jmax, j);
           }
         }
       }
-      if (valid && (do_kick || do_mcc)) ke += (double)(vx[r] * vx[r] + vy[r] * vy[r] + vz[r] * vz[r]);
-      // ---- drift + walls
-      bool absorbed = false;
-      float nfx = px[r], nfy = py[r];
-      uint32_t nc = c;
-      if (do_drift && valid) {
-        const Drifted d = drift_particle(J, S, c, px[r], py[r], vx[r], vy[r], do_walls);
-        absorbed = d.absorbed; nc = d.cell; nfx = d.fx; nfy = d.fy;
-      }
-      const int hslot = warp_append(valid && absorbed, hit_counts + s);
-      if (hslot >= 0) S.hits[hslot] = p;
-      // ---- deposit at the new position
-      if (do_dep) warp_deposit(J, S, (valid && !absorbed) ? nc : PIC_CELL_OUT, nfx, nfy);
-      cl[r] = nc; px[r] = nfx; py[r] = nfy;
-    }
-    // ---- write back
-    if (do_drift) {
-      if (base + 3 < n) {
-        *reinterpret_cast<uint4*>(S.cell + base) = make_uint4(cl[0], cl[1], cl[2], cl[3]);
-        *reinterpret_cast<float4*>(S.fx + base) = make_float4(px[0], px[1], px[2], px[3]);
-        *reinterpret_cast<float4*>(S.fy + base) = make_float4(py[0], py[1], py[2], py[3]);
-      } else {
-        for (int r = 0; r < 4; ++r)
-          if (base + r < n) { S.cell[base + r] = cl[r]; S.fx[base + r] = px[r]; S.fy[base + r] = py[r]; }
-      }
-    }
-    if (do_kick || do_mcc) {
-      if (base + 3 < n) {
-        *reinterpret_cast<float4*>(S.vx + base) = make_float4(vx[0], vx[1], vx[2], vx[3]);
-        *reinterpret_cast<float4*>(S.vy + base) = make_float4(vy[0], vy[1], vy[2], vy[3]);
-        if (do_mcc) *reinterpret_cast<float4*>(S.vz + base) = make_float4(vz[0], vz[1], vz[2], vz[3]);
-      } else {
-        for (int r = 0; r < 4; ++r)
-          if (base + r < n) {
-            S.vx[base + r] = vx[r]; S.vy[base + r] = vy[r];
-            if (do_mcc) S.vz[base + r] = vz[r];
+      imin = __reduce_min_sync(0xffffffffu, imin); jmin = __reduce_min_sync(0xffffffffu, jmin);
+      imax = __reduce_max_sync(0xffffffffu, imax); jmax = __reduce_max_sync(0xffffffffu, jmax);
+      if (t == 0) { bb[0] = 1 << 30; bb[1] = -1; bb[2] = 1 << 30; bb[3] = -1; }
+      __syncthreads();
+      if (lane == 0) { atomicMin(&bb[0], imin); atomicMax(&bb[1], imax); atomicMin(&bb[2], jmin); atomicMax(&bb[3], jmax); }
+      __syncthreads();
+      if (bb[1] >= 0) {
+        tx0 = max(bb[0] - 1, 0);
+        ty0 = max(bb[2] - 1, 0);
+        const int tx1 = min(bb[1] + 2, J.nx - 1), ty1 = min(bb[3] + 2, J.ny - 1);
+        tw = tx1 - tx0 + 1;
+        const int th = ty1 - ty0 + 1;
+        use_tile = tw * th <= kTileCap;
+        if (use_tile) {
+          for (int ry = warp; ry < th; ry += kWarps) {
+            const float* src = J.phi32 + (size_t)(ty0 + ry) * J.nx + tx0;
+            for (int rx = lane; rx < tw; rx += 32) tile[ry * tw + rx] = __ldg(src + rx);
           }
+        }
       }
+      __syncthreads();
     }
-    // ---- diagnostics: kinetic energy and collision counts (one atomic per warp)
+    if (t < 8) proc_count[t] = 0u;
+    if (lane == 0) wcount[warp] = 0;
+    __syncwarp();
+
+    // ---- pass A: kick and collisions
     if (do_kick || do_mcc) {
-      for (int o = 16; o; o >>= 1) ke += __shfl_down_sync(0xffffffffu, ke, o);
-      if (lane_id() == 0 && ke != 0.0) atomicAdd(&T.ke[S.species], ke * S.ke_factor);
-    }
-    if (do_mcc) {
-      for (int q = 0; q < S.n_proc && q < 8; ++q) {
-        const unsigned tot = __reduce_add_sync(0xffffffffu, ncoll[q]);
-        if (lane_id() == 0 && tot) atomicAdd(&T.collisions[S.species][q], (unsigned long long)tot);
+      PhiGather pg{J.phi32, J.nx, J.ny};
+      for (int r = 0; r < kRounds; ++r) {
+        const int p = base + r * PIC_MOVER_THREADS + t;
+        const bool valid = p < n;
+        bool cand = false;
+        if (valid) {
+          const uint32_t c = S.cell[p];
+          float vx = S.vx[p], vy = S.vy[p];
+          if (do_kick && c != PIC_CELL_OUT) {
+            float gx, gy;
+            const float fx = S.fx[p], fy = S.fy[p];
+            if (use_tile) gather_tile(tile, tw, tx0, ty0, J.nx, J.ny, cell_i(c), cell_j(c), fx, fy, gx, gy);
+            else gather_dphi(pg, cell_i(c), cell_j(c), fx, fy, gx, gy);
+            vx += S.kx * gx;
+            vy += S.ky * gy;
+          }
+          if (do_mcc) {
+            float u[4];
+            draw4(J.seed, S.pid[p], mcc_step, 0u, u);
+            if (J.mcc_mode == 2) {
+              const ProcDev& P = J.procs[S.first_proc];
+              const float v2 = vx * vx + vy * vy;
+              const float sp = sqrtf(v2);
+              const float Pc = 1.f - expf(-J.gas_density * xs_lookup(P, S.half_m_over_e * v2) * sp * J.dt);
+              if (u[0] < Pc) {
+                float sn, cs;
+                sincospif(2.f * u[1], &sn, &cs);
+                vx = sp * cs; vy = sp * sn;
+                atomicAdd(&proc_count[0], 1u);
+              }
+            } else {
+              cand = u[0] < S.pnull;
+            }
+          }
+          S.vx[p] = vx;
+          S.vy[p] = vy;
+        }
+        // list this warp's candidates (their kicked velocity is already stored)
+        const unsigned m = __ballot_sync(0xffffffffu, cand);
+        if (cand) wlist[warp][wcount[warp] + __popc(m & ((1u << lane) - 1u))] = p;
+        __syncwarp();
+        if (lane == 0) wcount[warp] += __popc(m);
+        __syncwarp();
       }
+      const int nc = wcount[warp];
+      for (int k = lane; k < nc; k += 32) {
+        const int p = wlist[warp][k];
+        float u[4];
+        const uint32_t pid = S.pid[p];
+        draw4(J.seed, pid, mcc_step, 0u, u);
+        float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
+        collide(J, S, slots, T, pid, S.cell[p], S.fx[p], S.fy[p], vx, vy, vz, u, mcc_step, proc_count);
+        S.vx[p] = vx; S.vy[p] = vy; S.vz[p] = vz;
+      }
+      __syncwarp();
+    }
+
+    // ---- pass B: drift, walls, deposit
+    double ke = 0.0;
+    const bool want_ke = do_kick || do_mcc;
+    if (do_drift || do_dep || want_ke) {
+      for (int r = 0; r < kRounds; ++r) {
+        const int p = base + r * PIC_MOVER_THREADS + t;
+        const bool valid = p < n;
+        uint32_t c = PIC_CELL_OUT;
+        float fx = 0.f, fy = 0.f, vx = 0.f, vy = 0.f;
+        if (valid) { c = S.cell[p]; fx = S.fx[p]; fy = S.fy[p]; vx = S.vx[p]; vy = S.vy[p]; }
+        if (valid && want_ke) {
+          const float vz = do_mcc ? S.vz[p] : 0.f;
+          ke += (double)(vx * vx + vy * vy + vz * vz);
+        }
+        bool absorbed = false;
+        uint32_t nc = c;
+        float nfx = fx, nfy = fy;
+        if (do_drift && valid) {
+          const Drifted d = drift_particle(J, S, c, fx, fy, vx, vy, do_walls);
+          absorbed = d.absorbed; nc = d.cell; nfx = d.fx; nfy = d.fy;
+        }
+        if (do_walls) {
+          const int hslot = warp_append(valid && absorbed, hit_counts + s);
+          if (hslot >= 0) S.hits[hslot] = p;
+        }
+        if (do_dep) warp_deposit(J, S, (valid && !absorbed) ? nc : PIC_CELL_OUT, nfx, nfy);
+        if (valid && do_drift) { S.cell[p] = nc; S.fx[p] = nfx; S.fy[p] = nfy; }
+      }
+    }
+    // ---- diagnostics: kinetic energy and collision counts
+    if (want_ke) {
+      for (int o = 16; o; o >>= 1) ke += __shfl_down_sync(0xffffffffu, ke, o);
+      if (lane == 0) ke_sh[warp] = ke;
+    }
+    __syncthreads();
+    if (t == 0) {
+      if (want_ke) {
+        double tk = 0.0;
+        for (int w = 0; w < kWarps; ++w) tk += ke_sh[w];
+        if (tk != 0.0) atomicAdd(&T.ke[S.species], tk * S.ke_factor);
+      }
+      if (do_mcc)
+        for (int q = 0; q < 8; ++q)
+          if (proc_count[q]) atomicAdd(&T.collisions[S.species][q], (unsigned long long)proc_count[q]);
     }
   }
 }
@@ -355,6 +452,15 @@ __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t
     chunk_prefix[nslots] = a;
     acc = a;
   }
+}
+
+int mover_blocks_per_sm() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, 0) != cudaSuccess || b < 1) {
+    cudaGetLastError();
+    b = 1;
+  }
+  return b;
 }
 
 int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t stream) {

@@ -14,7 +14,7 @@
 //              coarse nodes (fine tile + halo 2*nu+2 in shared memory, every sweep done
 //              locally: a node at distance d from the tile edge is exact for d half-sweeps),
 //              then residual + full weighting straight from shared memory
-//   mg_coarse  one CTA per job runs the whole V-cycle below 129x129 in shared memory
+//   mg_coarse  one CTA per job runs the whole V-cycle from 33x33 down in shared memory
 //   mg_up      prolongation + nu_post sweeps on 32x32 tiles; on level 0 also the FP64
 //              update phi += e, the new FP64 residual, phi32 and the norm (last CTA of each
 //              job reduces the per-tile partials in a fixed order: deterministic).
@@ -43,6 +43,22 @@ __device__ double block_sum(double v) {
   if (threadIdx.x == 0)
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += ws[k];
   return t;  // valid in thread 0
+}
+
+// Sum of n partials (stride `stride`, offset `off`) by the whole CTA in a fixed order:
+// thread t adds entries t, t+B, t+2B, ... then a fixed tree combines the threads, so the
+// result does not depend on scheduling.  Valid in thread 0.
+__device__ double ordered_sum(const double* p, int n, int stride, int off) {
+  double s = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) s += p[(size_t)k * stride + off];
+  __shared__ double sh[256];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  return sh[0];
 }
 
 // Last CTA of a job's tiles in this launch?  (threadfence + ticket)
@@ -90,9 +106,11 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     J.partials[2 * (tr.pbase + tr.local)] = sr;
     J.partials[2 * (tr.pbase + tr.local) + 1] = sf;
   }
-  if (last_of_job(T, tr.nlocal) && threadIdx.x == 0) {
-    double r2 = 0.0, f2 = 0.0;
-    for (int t = 0; t < tr.nlocal; ++t) { r2 += J.partials[2 * (tr.pbase + t)]; f2 += J.partials[2 * (tr.pbase + t) + 1]; }
+  if (last_of_job(T, tr.nlocal)) {
+    __threadfence();
+    const double r2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 0);
+    const double f2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 1);
+    if (threadIdx.x != 0) return;
     T.rnorm2 = r2;
     T.fnorm2 = f2;
     T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
@@ -103,21 +121,27 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
 }
 
 // Red-black SOR half-sweeps on a W x W shared tile whose node (0,0) is grid node (gx0,gy0).
-// Only grid-interior nodes that are not on the tile's outer ring are updated.
+// Only grid-interior nodes that are not on the tile's outer ring are updated.  Rows are
+// spread over warps and the nodes of one colour in a row over lanes, so no thread divides
+// or skips nodes of the other colour.
 __device__ __forceinline__ void tile_sweeps(float* e, const float* f, int W, int gx0, int gy0, int n, float h2,
                                             float omega, int nu) {
   const float om1 = 1.f - omega;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int ly_lo = max(1, 1 - gy0), ly_hi = min(W - 2, n - 2 - gy0);   // rows to update
+  const int lx_lo = max(1, 1 - gx0), lx_hi = min(W - 2, n - 2 - gx0);   // columns to update
   for (int it = 0; it < nu; ++it) {
     for (int colour = 1; colour >= 0; --colour) {
-      for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
-        const int lx = k % W, ly = k / W;
-        const int gx = gx0 + lx, gy = gy0 + ly;
-        if (((gx + gy) & 1) != colour) continue;
-        if (gx <= 0 || gx >= n - 1 || gy <= 0 || gy >= n - 1) continue;
-        if (lx == 0 || lx == W - 1 || ly == 0 || ly == W - 1) continue;
-        const float s = e[k + W] + e[k - W] + e[k + 1] + e[k - 1];
-        const float nv = 0.25f * (s - h2 * f[k]);
-        e[k] = fmaf(omega, nv, om1 * e[k]);
+      for (int ly = ly_lo + warp; ly <= ly_hi; ly += nwarp) {
+        // first lx >= lx_lo with (gx0 + lx + gy0 + ly) % 2 == colour
+        const int lx0 = lx_lo + ((colour - gx0 - lx_lo - gy0 - ly) & 1);
+        float* row = e + ly * W;
+        const float* frow = f + ly * W;
+        for (int lx = lx0 + 2 * lane; lx <= lx_hi; lx += 64) {
+          const float s = row[lx + W] + row[lx - W] + row[lx + 1] + row[lx - 1];
+          const float nv = 0.25f * (s - h2 * frow[lx]);
+          row[lx] = fmaf(omega, nv, om1 * row[lx]);
+        }
       }
       __syncthreads();
     }
@@ -141,19 +165,26 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
   float* e = sm;
   float* f = sm + W * W;
   const float* fg = J.f[l];
-  for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
-    const int gx = gx0 + k % W, gy = gy0 + k / W;
-    f[k] = (gx >= 0 && gx < nf && gy >= 0 && gy < nf) ? fg[(size_t)gy * nf + gx] : 0.f;
-    e[k] = 0.f;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 4
+  for (int ly = warp; ly < W; ly += 8) {
+    const int gy = gy0 + ly;
+    const bool rowin = gy >= 0 && gy < nf;
+    for (int lx = lane; lx < W; lx += 32) {
+      const int gx = gx0 + lx;
+      f[ly * W + lx] = (rowin && gx >= 0 && gx < nf) ? __ldg(fg + (size_t)gy * nf + gx) : 0.f;
+      e[ly * W + lx] = 0.f;
+    }
   }
   __syncthreads();
   tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
   // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
   float* eg = J.e[l];
-  for (int k = threadIdx.x; k < 4 * kTC * kTC; k += blockDim.x) {
-    const int ox = k % (2 * kTC), oy = k / (2 * kTC);
-    const int gx = 2 * ic0 + ox, gy = 2 * jc0 + oy;
-    if (gx < nf && gy < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+  for (int oy = warp; oy < 2 * kTC; oy += 8) {
+    const int gy = 2 * jc0 + oy;
+    if (gy >= nf) break;
+    const int gx = 2 * ic0 + lane;
+    if (gx < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
   }
   // residual + full weighting to the owned coarse nodes
   float* fc = J.f[l + 1];
@@ -183,16 +214,17 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
 // ---------------------------------------------------------------- mg_coarse
 __device__ void smem_sweeps(float* e, const float* f, int n, float h2, float omega, int nu) {
   const float om1 = 1.f - omega;
-  const int m = n - 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int it = 0; it < nu; ++it) {
     for (int colour = 1; colour >= 0; --colour) {
-      for (int k = threadIdx.x; k < m * m; k += blockDim.x) {
-        const int i = 1 + k % m, j = 1 + k / m;
-        if (((i + j) & 1) != colour) continue;
-        const int c = j * n + i;
-        const float s = e[c + n] + e[c - n] + e[c + 1] + e[c - 1];
-        const float nv = 0.25f * (s - h2 * f[c]);
-        e[c] = fmaf(omega, nv, om1 * e[c]);
+      for (int j = 1 + warp; j < n - 1; j += nwarp) {
+        const int i0 = 1 + ((colour - 1 - j) & 1);
+        for (int i = i0 + 2 * lane; i < n - 1; i += 64) {
+          const int c = j * n + i;
+          const float s = e[c + n] + e[c - n] + e[c + 1] + e[c - 1];
+          const float nv = 0.25f * (s - h2 * f[c]);
+          e[c] = fmaf(omega, nv, om1 * e[c]);
+        }
       }
       __syncthreads();
     }
@@ -206,73 +238,80 @@ __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__
   const JobDev& J = jobs[job];
   if (st[job].converged) return;
   const int lc = J.lc, L = J.levels;
-  float* E[PIC_MAX_LEVELS];
-  float* F[PIC_MAX_LEVELS];
-  {
-    float* p = sm;
-    for (int l = lc; l < L; ++l) {
-      const int n2 = J.nl[l] * J.nl[l];
-      E[l] = p; p += n2;
-      F[l] = p; p += n2;
-    }
+  // level l occupies [off[l], off[l] + 2 n_l^2) of shared memory: E then F
+  __shared__ int off[PIC_MAX_LEVELS];
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int k = lc; k < L; ++k) { off[k] = o; o += 2 * J.nl[k] * J.nl[k]; }
   }
+  __syncthreads();
+#define E(l) (sm + off[l])
+#define F(l) (sm + off[l] + J.nl[l] * J.nl[l])
   {
     const int n = J.nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F[lc][k] = J.f[lc][k]; E[lc][k] = 0.f; }
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F(lc)[k] = J.f[lc][k]; E(lc)[k] = 0.f; }
   }
   __syncthreads();
   for (int l = lc; l < L - 1; ++l) {
     const int n = J.nl[l], nc = J.nl[l + 1];
     const double hl = J.h * (double)(1 << l);
     const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
-    smem_sweeps(E[l], F[l], n, h2, J.omega, J.nu_pre);
-    const float* e = E[l];
-    const float* f = F[l];
-    for (int k = threadIdx.x; k < nc * nc; k += blockDim.x) {
-      const int ic = k % nc, jc = k / nc;
-      float v = 0.f;
-      if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
-        float r[3][3];
-        for (int dy = -1; dy <= 1; ++dy)
-          for (int dx = -1; dx <= 1; ++dx) {
-            const int q = (2 * jc + dy) * n + (2 * ic + dx);
-            const float lap = (e[q - n] + e[q + n] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
-            r[dy + 1][dx + 1] = f[q] - lap;
-          }
-        v = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] + r[0][2] +
-             r[2][0] + r[2][2]) * 0.0625f;
+    smem_sweeps(E(l), F(l), n, h2, J.omega, J.nu_pre);
+    const float* e = E(l);
+    const float* f = F(l);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int jc = warp; jc < nc; jc += nwarp) {
+      for (int ic = lane; ic < nc; ic += 32) {
+        float v = 0.f;
+        if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
+          float r[3][3];
+#pragma unroll
+          for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int q = (2 * jc + dy) * n + (2 * ic + dx);
+              const float lap = (e[q - n] + e[q + n] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
+              r[dy + 1][dx + 1] = f[q] - lap;
+            }
+          v = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] + r[0][2] +
+               r[2][0] + r[2][2]) * 0.0625f;
+        }
+        F(l + 1)[jc * nc + ic] = v;
+        E(l + 1)[jc * nc + ic] = 0.f;
       }
-      F[l + 1][k] = v;
-      E[l + 1][k] = 0.f;
     }
     __syncthreads();
   }
   {
     const double hl = J.h * (double)(1 << (L - 1));
-    smem_sweeps(E[L - 1], F[L - 1], J.nl[L - 1], (float)(hl * hl), J.omega, J.nu_coarse);
+    smem_sweeps(E(L - 1), F(L - 1), J.nl[L - 1], (float)(hl * hl), J.omega, J.nu_coarse);
   }
   for (int l = L - 2; l >= lc; --l) {
     const int n = J.nl[l], nc = J.nl[l + 1];
-    const float* c = E[l + 1];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
-      const int i = k % n, j = k / n;
-      const int ic = i >> 1, jc = j >> 1;
-      const float* cp = c + jc * nc + ic;
-      float v;
-      if (!(i & 1) && !(j & 1)) v = cp[0];
-      else if ((i & 1) && !(j & 1)) v = 0.5f * (cp[0] + cp[1]);
-      else if (!(i & 1) && (j & 1)) v = 0.5f * (cp[0] + cp[nc]);
-      else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
-      E[l][k] += v;
+    const float* c = E(l + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int j = 1 + warp; j < n - 1; j += nwarp) {   // boundary nodes receive 0 (coarse boundary is 0)
+      for (int i = 1 + lane; i < n - 1; i += 32) {
+        const int ic = i >> 1, jc = j >> 1;
+        const float* cp = c + jc * nc + ic;
+        float v;
+        if (!(i & 1) && !(j & 1)) v = cp[0];
+        else if ((i & 1) && !(j & 1)) v = 0.5f * (cp[0] + cp[1]);
+        else if (!(i & 1) && (j & 1)) v = 0.5f * (cp[0] + cp[nc]);
+        else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
+        E(l)[j * n + i] += v;
+      }
     }
     __syncthreads();
     const double hl = J.h * (double)(1 << l);
-    smem_sweeps(E[l], F[l], n, (float)(hl * hl), J.omega, J.nu_post);
+    smem_sweeps(E(l), F(l), n, (float)(hl * hl), J.omega, J.nu_post);
   }
   {
     const int n = J.nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) J.e[lc][k] = E[lc][k];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) J.e[lc][k] = E(lc)[k];
   }
+#undef E
+#undef F
 }
 
 // ---------------------------------------------------------------- mg_up
@@ -299,21 +338,30 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const bool prolong = mode != 2;
   const int nc = prolong ? J.nl[l + 1] : 0;
   const float* ec = prolong ? J.e[l + 1] : nullptr;
-  for (int k = threadIdx.x; k < W * W; k += blockDim.x) {
-    const int gx = gx0 + k % W, gy = gy0 + k / W;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 2
+  for (int ly = warp; ly < W; ly += 8)
+  for (int lx = lane; lx < W; lx += 32) {
+    const int k = ly * W + lx;
+    const int gx = gx0 + lx, gy = gy0 + ly;
     float ev = 0.f, fv = 0.f;
     if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) {
       const size_t g = (size_t)gy * nf + gx;
-      ev = eg[g];
-      fv = fg[g];
+      ev = __ldg(eg + g);
+      fv = __ldg(fg + g);
       if (prolong) {
+        // bilinear prolongation (Multigrid.cu:378-404) as weights on the 2x2 coarse block
         const float* cp = ec + (size_t)(gy >> 1) * nc + (gx >> 1);
         const bool io = gx & 1, jo = gy & 1;
+        const float c00 = __ldg(cp);
+        const float c10 = io ? __ldg(cp + 1) : 0.f;
+        const float c01 = jo ? __ldg(cp + nc) : 0.f;
+        const float c11 = (io && jo) ? __ldg(cp + nc + 1) : 0.f;
         float v;
-        if (!io && !jo) v = cp[0];
-        else if (io && !jo) v = 0.5f * (cp[0] + cp[1]);
-        else if (!io && jo) v = 0.5f * (cp[0] + cp[nc]);
-        else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
+        if (!io && !jo) v = c00;
+        else if (io && !jo) v = 0.5f * (c00 + c10);
+        else if (!io && jo) v = 0.5f * (c00 + c01);
+        else v = 0.25f * (c00 + c10 + c01 + c11);
         ev += v;
       }
     }
@@ -324,9 +372,9 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   if (nu > 0) tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
   if (mode == 0) {
     float* eo = J.e[l];
-    for (int k = threadIdx.x; k < kTU * kTU; k += blockDim.x) {
-      const int gx = i0 + k % kTU, gy = j0 + k / kTU;
-      if (gx < nf && gy < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+    for (int oy = warp; oy < kTU; oy += 8) {
+      const int gy = j0 + oy, gx = i0 + lane;
+      if (gy < nf && gx < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
     }
     return;
   }
@@ -336,17 +384,18 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const double* pc = J.phi64[cur];
   double* pn = J.phi64[cur ^ 1];
   constexpr int PW = kTU + 2;
-  for (int k = threadIdx.x; k < PW * PW; k += blockDim.x) {
-    const int gx = i0 - 1 + k % PW, gy = j0 - 1 + k / PW;
-    double v = 0.0;
-    if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) v = pc[(size_t)gy * nf + gx] + (double)e[(gy - gy0) * W + (gx - gx0)];
-    P[k] = v;
-  }
+  for (int py = warp; py < PW; py += 8)
+    for (int px = lane; px < PW; px += 32) {
+      const int gx = i0 - 1 + px, gy = j0 - 1 + py;
+      double v = 0.0;
+      if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) v = __ldg(pc + (size_t)gy * nf + gx) + (double)e[(gy - gy0) * W + (gx - gx0)];
+      P[py * PW + px] = v;
+    }
   __syncthreads();
   const double inv_h2 = 1.0 / (J.h * J.h);
   double ar = 0.0;
-  for (int k = threadIdx.x; k < kTU * kTU; k += blockDim.x) {
-    const int ox = k % kTU, oy = k / kTU;
+  for (int oy = warp; oy < kTU; oy += 8) {
+    const int ox = lane;
     const int gx = i0 + ox, gy = j0 + oy;
     if (gx >= nf || gy >= nf) continue;
     const size_t g = (size_t)gy * nf + gx;
@@ -364,9 +413,10 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   }
   const double sr = block_sum(ar);
   if (threadIdx.x == 0) J.partials[2 * (tr.pbase + tr.local)] = sr;
-  if (last_of_job(T, tr.nlocal) && threadIdx.x == 0) {
-    double r2 = 0.0;
-    for (int t = 0; t < tr.nlocal; ++t) r2 += J.partials[2 * (tr.pbase + t)];
+  if (last_of_job(T, tr.nlocal)) {
+    __threadfence();
+    const double r2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 0);
+    if (threadIdx.x != 0) return;
     T.rnorm2 = r2;
     T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
     T.cycles += 1;
@@ -412,4 +462,21 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
     }
   if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
   return k;
+}
+
+namespace {
+// Body-end kernel of the V-cycle WHILE node: loop again while any job is still iterating,
+// never more than max_iterations times per solve.
+__global__ void vcycle_condition_kernel(cudaGraphConditionalHandle h, const int* running, int* iterations,
+                                        int max_iterations, unsigned long long* total) {
+  const int it = ++(*iterations);
+  *total += 1ull;
+  cudaGraphSetConditional(h, (*running > 0 && it < max_iterations) ? 1u : 0u);
+}
+}  // namespace
+
+int launch_vcycle_condition(cudaGraphConditionalHandle h, const int* running, int* iterations, int max_iterations,
+                            unsigned long long* total, cudaStream_t s) {
+  vcycle_condition_kernel<<<1, 1, 0, s>>>(h, running, iterations, max_iterations, total);
+  return 1;
 }

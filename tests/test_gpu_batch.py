@@ -64,3 +64,29 @@ def test_repeat_run_bitwise_identical():
     for s in (0, 1):
         for key in ("pid", "x", "y", "vx", "vy", "vz"):
             assert np.array_equal(r1[0][0][s][key], r2[0][0][s][key])
+
+
+def test_graph_step_equals_stream_step_bitwise():
+    """pic_step_graph (CUDA graph, V-cycle loop as a conditional WHILE node) gives exactly
+    the state pic_step (host-driven loop) gives."""
+    specs = _jobs()
+    res = []
+    for use_graph in (False, True):
+        e = Engine(0)
+        jobs = []
+        for cfg, Ld, Te, seed in specs:
+            j = e.add_job(cfg)
+            n = cfg.species[0].capacity * 4 // 5 - 1024
+            cf.load_plasma(j, int(n), Ld, Te, 0.03, seed=seed)
+            jobs.append(j)
+        for _ in range(7):  # crosses sort steps of every job
+            (e.step_graph if use_graph else e.step)(1)
+        res.append([([_by_pid(j.export_species(s)) for s in (0, 1)], j.get_grid(L.GRID_PHI), j.diagnostics())
+                    for j in jobs])
+        e.close()
+    for a, b in zip(res[0], res[1]):
+        for s in (0, 1):
+            for key in ("pid", "x", "y", "vx", "vy", "vz"):
+                assert np.array_equal(a[0][s][key], b[0][s][key]), (s, key)
+        assert np.array_equal(a[1], b[1])
+        assert a[2]["vcycles"] == b[2]["vcycles"] and a[2]["step"] == b[2]["step"] == 7
