@@ -18,7 +18,7 @@
 
 #define PIC_CELL_OUT 0xFFFFFFFFu
 #define PIC_MAX_LEVELS 14
-#define PIC_COARSE_MAX 33           // levels with n <= this are solved by one CTA in smem
+#define PIC_COARSE_MAX 65           // a first coarse level this small is solved by one CTA in smem
 #define PIC_CHUNK 1024              // particles per mover work item (256 threads x 4)
 #define PIC_MOVER_THREADS 256
 #define PIC_FIX_SHIFT 40            // int64 deposit: 2^40 per unit deposit charge

@@ -170,17 +170,25 @@ struct Layout {  // byte sizes of one job's device state
   int ntiles0;
   int64_t total;
 };
-Layout job_layout(const pic_job_config& c) {
+// First level handled by the coarse solver (levels above it run as tile kernels):
+//  grids <= 65^2 entirely in one CTA (lc = 0); otherwise the first level that fits the
+//  coarse solver, never level 0 (the FP64 defect-correction update lives in the tile
+//  kernels): one CTA up to 65^2, a C-CTA cluster up to cluster_max.
+Layout job_layout(const pic_job_config& c, int cluster_C = 0) {
   Layout L{};
   L.levels = c.mg_levels > 0 ? c.mg_levels : auto_levels(c.nx);
+  const int cluster_max = cluster_C >= 16 ? 513 : cluster_C >= 8 ? 257 : PIC_COARSE_MAX;
   int n = c.nx;
   L.lc = -1;
   for (int l = 0; l < L.levels; ++l) {
     L.nl[l] = n;
-    if (L.lc < 0 && n <= PIC_COARSE_MAX) L.lc = l;
+    if (L.lc < 0) {
+      if (l == 0 && n <= PIC_COARSE_MAX) L.lc = 0;
+      else if (l > 0 && n <= cluster_max) L.lc = l;
+    }
     n = (n + 1) / 2;
   }
-  if (L.lc < 0) L.lc = L.levels - 1;  // finest coarse-able level not reached: solve last level in smem
+  if (L.lc < 0) L.lc = L.levels - 1;
   L.ntiles0 = ((c.nx + 31) / 32) * ((c.ny + 31) / 32);
   const int64_t N = (int64_t)c.nx * c.ny;
   int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16);
@@ -208,6 +216,8 @@ struct pic_engine {
   cudaStream_t stream = nullptr;
   int num_sms = 148;
   int mover_bps = 4;
+  int cluster_C = 0;          // thread-block cluster size of the coarse solver (0: none)
+  size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
   std::vector<JobHost> jobs;
   int njobs_hw = 0;
@@ -295,7 +305,8 @@ void free_job(pic_engine* E, JobHost& J) {
 int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   out.release();
   std::vector<TileRef> init, upd, down[PIC_MAX_LEVELS], up[PIC_MAX_LEVELS];
-  std::vector<int> coarse;
+  std::vector<int> coarse, cluster;
+  size_t cluster_smem = 0;
   int max_depth = 0, max_cycles = 1, nu_pre_max = 1, nu_post_max = 1;
   size_t coarse_smem = 0;
   for (int id : ids) {
@@ -319,10 +330,15 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
       for (int tj = 0; tj < tu; ++tj)
         for (int ti = 0; ti < tu; ++ti) up[l].push_back({id, ti, tj, tj * tu + ti, tu * tu, 0});
     }
-    coarse.push_back(id);
-    size_t b = 0;
-    for (int l = D.lc; l < D.levels; ++l) b += 2ull * D.nl[l] * D.nl[l] * sizeof(float);
-    coarse_smem = std::max(coarse_smem, b);
+    if (E->cluster_C > 0 && D.nl[D.lc] > PIC_COARSE_MAX) {
+      cluster.push_back(id);
+      cluster_smem = std::max(cluster_smem, mg_cluster_smem(D.nl, D.lc, D.levels, E->cluster_C));
+    } else {
+      coarse.push_back(id);
+      size_t b = 0;
+      for (int l = D.lc; l < D.levels; ++l) b += 2ull * D.nl[l] * D.nl[l] * sizeof(float);
+      coarse_smem = std::max(coarse_smem, b);
+    }
   }
   std::vector<TileRef> all;
   size_t off_init = all.size(); all.insert(all.end(), init.begin(), init.end());
@@ -334,9 +350,11 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
     CK(cudaMalloc(&out.d_tiles, all.size() * sizeof(TileRef)));
     CK(cudaMemcpy(out.d_tiles, all.data(), all.size() * sizeof(TileRef), cudaMemcpyHostToDevice));
   }
-  if (!coarse.empty()) {
-    CK(cudaMalloc(&out.d_coarse, coarse.size() * sizeof(int)));
-    CK(cudaMemcpy(out.d_coarse, coarse.data(), coarse.size() * sizeof(int), cudaMemcpyHostToDevice));
+  std::vector<int> lists(coarse);
+  lists.insert(lists.end(), cluster.begin(), cluster.end());
+  if (!lists.empty()) {
+    CK(cudaMalloc(&out.d_coarse, lists.size() * sizeof(int)));
+    CK(cudaMemcpy(out.d_coarse, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   MgLaunch& M = out.L;
   M = MgLaunch{};
@@ -347,13 +365,19 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
     M.up_tiles[l] = out.d_tiles + off_up[l]; M.n_up[l] = (int)up[l].size();
   }
   M.coarse_jobs = out.d_coarse; M.n_coarse = (int)coarse.size();
+  M.cluster_jobs = out.d_coarse + coarse.size(); M.n_cluster = (int)cluster.size();
+  M.cluster_C = E->cluster_C;
+  M.cluster_smem = cluster_smem;
   M.max_depth = max_depth;
   M.coarse_smem = coarse_smem;
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
   out.max_cycles = max_cycles;
   out.valid = true;
-  if (coarse_smem > 227 * 1024) return fail(PIC_ERR_ARG, "coarse multigrid levels exceed shared memory");
+  if (coarse_smem > 227 * 1024 || cluster_smem > 227 * 1024)
+    return fail(PIC_ERR_ARG, "coarse multigrid levels exceed shared memory");
+  if (!cluster.empty() && mg_cluster_supported(E->cluster_C, cluster_smem) <= 0)
+    return fail(PIC_ERR_CUDA, "thread-block cluster of the coarse solver cannot be scheduled");
   mg_configure_coarse(std::max<size_t>(coarse_smem, 48 * 1024));
   return PIC_OK;
 }
@@ -645,6 +669,15 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
   E->pool_bytes = pool_bytes;
   cudaDeviceGetAttribute(&E->num_sms, cudaDevAttrMultiProcessorCount, device);
   E->mover_bps = mover_blocks_per_sm();
+  {
+    // largest cluster the device co-schedules with the shared memory its top level needs
+    const int n16[] = {513, 257, 129, 65, 33, 17, 9, 5, 3};
+    const size_t s16 = mg_cluster_smem(n16, 0, 9, 16);
+    const int n8[] = {257, 129, 65, 33, 17, 9, 5, 3};
+    const size_t s8 = mg_cluster_smem(n8, 0, 8, 8);
+    if (mg_cluster_supported(16, s16) > 0) { E->cluster_C = 16; E->cluster_smem_max = s16; }
+    else if (mg_cluster_supported(8, s8) > 0) { E->cluster_C = 8; E->cluster_smem_max = s8; }
+  }
   const int nslots = kMaxJobs * kSlotsPerJob;
   cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_jobs, sizeof(JobDev) * kMaxJobs);
@@ -735,7 +768,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   for (int j = 0; j < kMaxJobs; ++j)
     if (!E->jobs[j].alive) { id = j; break; }
   if (id < 0) return fail(PIC_ERR_CAPACITY, "engine job table full");
-  const Layout lay = job_layout(*cfg);
+  const Layout lay = job_layout(*cfg, E->cluster_C);
   if (E->pool_bytes > 0 && E->used_bytes + lay.total > E->pool_bytes) return fail(PIC_ERR_OOM, "engine memory budget exceeded");
   JobHost& J = E->jobs[id];
   J = JobHost();

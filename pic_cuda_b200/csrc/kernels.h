@@ -60,7 +60,10 @@ struct MgLaunch {
   const TileRef* down_tiles[PIC_MAX_LEVELS]; int n_down[PIC_MAX_LEVELS];   // coarse 16x16 owned
   const TileRef* up_tiles[PIC_MAX_LEVELS]; int n_up[PIC_MAX_LEVELS];       // fine 32x32 owned
   const TileRef* upd_tiles; int n_upd;                   // level-0 update for jobs with lc == 0
-  const int* coarse_jobs; int n_coarse;
+  const int* coarse_jobs; int n_coarse;                  // single-CTA coarse solve
+  const int* cluster_jobs; int n_cluster;                // thread-block-cluster coarse solve
+  int cluster_C;
+  size_t cluster_smem;
   int max_depth;                                         // max lc over jobs
   size_t coarse_smem;
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
@@ -68,6 +71,10 @@ struct MgLaunch {
 int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 void mg_configure_coarse(size_t smem_bytes);
+size_t mg_cluster_smem(const int* nl, int lc, int levels, int C);
+int mg_cluster_supported(int C, size_t smem);
+int launch_mg_cluster(const int* job_list, int njobs, int C, size_t smem, const JobDev* jobs, const JobState* st,
+                      cudaStream_t s);
 
 // Conversions between the public FP64 domain-unit layout and the engine layout.
 void launch_load_species(const SlotDev* slot_dev, const JobDev* job_dev, int64_t n, const double* x,

@@ -15,6 +15,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "particle_ops.cuh"
+#include "tma.cuh"
 
 namespace {
 
@@ -235,19 +236,58 @@ __device__ __forceinline__ void gather_tile(const float* tile, int tw, int tx0, 
   gy = w00 * ey00 + w10 * ey10 + w01 * ey01 + w11 * ey11;
 }
 
-// One chunk = PIC_CHUNK particles of one slot; thread t handles particles base + r*256 + t.
+// Particle arrays of one chunk staged in shared memory.
+enum { A_CELL = 0, A_FX, A_FY, A_VX, A_VY, A_VZ, A_PID, kNArr };
+constexpr int kChunkBytes = PIC_CHUNK * 4;
+constexpr size_t kMoverDynSmem = 2ull * kNArr * kChunkBytes + kTileCap * sizeof(float);
+
+__device__ __forceinline__ int chunk_slot(const int* __restrict__ chunk_prefix, int nslots, int g) {
+  int lo = 0, hi = nslots - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (chunk_prefix[mid] <= g) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Issue the bulk copies of chunk g into buffer b (one thread).  vz and pid are staged only
+// for jobs with collisions.
+__device__ __forceinline__ void issue_chunk(const JobDev* __restrict__ jobs, const SlotDev* __restrict__ slots,
+                                            const int* __restrict__ chunk_prefix, int nslots, int g, uint32_t* buf,
+                                            uint64_t* mbar) {
+  const int s = chunk_slot(chunk_prefix, nslots, g);
+  const SlotDev& S = slots[s];
+  const size_t base = (size_t)(g - chunk_prefix[s]) * PIC_CHUNK;
+  const bool mcc = jobs[S.job].mcc_mode != 0 && S.n_proc > 0;
+  tma::mbar_arrive_expect_tx(mbar, (uint32_t)(kChunkBytes * (mcc ? 7 : 5)));
+  tma::bulk_g2s(buf + A_CELL * PIC_CHUNK, S.cell + base, kChunkBytes, mbar);
+  tma::bulk_g2s(buf + A_FX * PIC_CHUNK, S.fx + base, kChunkBytes, mbar);
+  tma::bulk_g2s(buf + A_FY * PIC_CHUNK, S.fy + base, kChunkBytes, mbar);
+  tma::bulk_g2s(buf + A_VX * PIC_CHUNK, S.vx + base, kChunkBytes, mbar);
+  tma::bulk_g2s(buf + A_VY * PIC_CHUNK, S.vy + base, kChunkBytes, mbar);
+  if (mcc) {
+    tma::bulk_g2s(buf + A_VZ * PIC_CHUNK, S.vz + base, kChunkBytes, mbar);
+    tma::bulk_g2s(buf + A_PID * PIC_CHUNK, S.pid + base, kChunkBytes, mbar);
+  }
+}
+
+// One chunk = PIC_CHUNK particles of one slot; thread t handles chunk entries r*256 + t.
+// Chunks reach shared memory through bulk asynchronous copies, double buffered: while the
+// CTA works on chunk k, chunk k+1 is in flight, so HBM latency is covered by the copy engine
+// rather than by resident warps; results return with bulk stores.
 //  pass A  kick (phi tile staged in shared memory when the chunk's cells fit) and the
-//          null-collision candidate test; velocities are stored, candidates (~nu_max dt of
-//          the particles) are listed per warp and collided by that warp's lanes afterwards,
-//          so the long collision code runs once per list instead of once per divergent lane
-//  pass B  drift, absorption, hit list and CIC deposit, re-reading the chunk from L1/L2
+//          null-collision candidate test; candidates (~nu_max dt of the particles) are listed
+//          per warp and collided by that warp's lanes afterwards
+//  pass B  drift, absorption, hit list and CIC deposit
 // The slot and job tables are copied to shared memory per chunk: every parameter read in
 // the per-particle code is a shared-memory load.
-__global__ void __launch_bounds__(PIC_MOVER_THREADS, 4)
+__global__ void __launch_bounds__(PIC_MOVER_THREADS, 2)
 mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
              const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ chunk_prefix,
              int nslots, int flags, uint32_t explicit_step) {
-  __shared__ float tile[kTileCap];
+  extern __shared__ __align__(128) uint32_t dsm[];
+  float* tile = reinterpret_cast<float*>(dsm + 2 * kNArr * PIC_CHUNK);
+  __shared__ __align__(8) uint64_t mbar[2];
   __shared__ int wlist[kWarps][PIC_CHUNK / kWarps];
   __shared__ int wcount[kWarps];
   __shared__ int bb[4];
@@ -256,26 +296,46 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
   __shared__ SlotDev sS;
   __shared__ JobDev sJ;
   __shared__ int cur_slot;
+  __shared__ int abort_flag;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int total = chunk_prefix[nslots];
-  if (t == 0) cur_slot = -1;
-  for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    int lo = 0, hi = nslots - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (chunk_prefix[mid] <= g) lo = mid; else hi = mid - 1;
+  if (t == 0) {
+    cur_slot = -1;
+    abort_flag = 0;
+    tma::mbar_init(&mbar[0], 1);
+    tma::mbar_init(&mbar[1], 1);
+    tma::fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t parity[2] = {0u, 0u};
+  if (t == 0 && (int)blockIdx.x < total) issue_chunk(jobs, slots, chunk_prefix, nslots, blockIdx.x, dsm, &mbar[0]);
+  int k = 0;
+  for (int g = blockIdx.x; g < total; g += gridDim.x, ++k) {
+    const int b = k & 1;
+    uint32_t* buf = dsm + b * kNArr * PIC_CHUNK;
+    // prefetch the next chunk into the other buffer (after its last bulk store has been read)
+    if (t == 0 && g + (int)gridDim.x < total) {
+      tma::bulk_wait_read_all();
+      issue_chunk(jobs, slots, chunk_prefix, nslots, g + gridDim.x, dsm + (b ^ 1) * kNArr * PIC_CHUNK, &mbar[b ^ 1]);
     }
-    const int s = lo;
+    const int s = chunk_slot(chunk_prefix, nslots, g);
     __syncthreads();
     if (cur_slot != s) {  // copy the slot and job tables to shared memory
       const int* srcS = reinterpret_cast<const int*>(slots + s);
       const int* srcJ = reinterpret_cast<const int*>(jobs + slots[s].job);
       int* dS = reinterpret_cast<int*>(&sS);
       int* dJ = reinterpret_cast<int*>(&sJ);
-      for (int k = t; k < (int)(sizeof(SlotDev) / 4); k += PIC_MOVER_THREADS) dS[k] = srcS[k];
-      for (int k = t; k < (int)(sizeof(JobDev) / 4); k += PIC_MOVER_THREADS) dJ[k] = srcJ[k];
+      for (int q = t; q < (int)(sizeof(SlotDev) / 4); q += PIC_MOVER_THREADS) dS[q] = srcS[q];
+      for (int q = t; q < (int)(sizeof(JobDev) / 4); q += PIC_MOVER_THREADS) dJ[q] = srcJ[q];
     }
+    // wait for this chunk's data (bounded)
+    if (!tma::mbar_wait(&mbar[b], parity[b])) atomicOr(&abort_flag, 1);
+    parity[b] ^= 1u;
     __syncthreads();
+    if (abort_flag) {
+      if (t == 0) atomicOr(&st[slots[s].job].status, PIC_ST_TIMEOUT);
+      break;
+    }
     if (t == 0) cur_slot = s;
     const SlotDev& S = sS;
     const JobDev& J = sJ;
@@ -290,6 +350,13 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     const bool do_walls = (flags & PIC_PHASE_WALLS_I) && J.wall_mode != 0;
     const bool do_dep = flags & PIC_PHASE_DEPOSIT_I;
     const uint32_t mcc_step = gated ? (uint32_t)(T.step - 1) : explicit_step;
+    uint32_t* s_cell = buf + A_CELL * PIC_CHUNK;
+    float* s_fx = reinterpret_cast<float*>(buf + A_FX * PIC_CHUNK);
+    float* s_fy = reinterpret_cast<float*>(buf + A_FY * PIC_CHUNK);
+    float* s_vx = reinterpret_cast<float*>(buf + A_VX * PIC_CHUNK);
+    float* s_vy = reinterpret_cast<float*>(buf + A_VY * PIC_CHUNK);
+    float* s_vz = reinterpret_cast<float*>(buf + A_VZ * PIC_CHUNK);
+    const uint32_t* s_pid = buf + A_PID * PIC_CHUNK;
 
     // ---- phi tile of the chunk (bounding box of the cells + 1 node below, 2 above)
     bool use_tile = false;
@@ -297,9 +364,9 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     if (do_kick) {
       int imin = 1 << 30, imax = -1, jmin = 1 << 30, jmax = -1;
       for (int r = 0; r < kRounds; ++r) {
-        const int p = base + r * PIC_MOVER_THREADS + t;
-        if (p < n) {
-          const uint32_t c = S.cell[p];
+        const int q = r * PIC_MOVER_THREADS + t;
+        if (base + q < n) {
+          const uint32_t c = s_cell[q];
           if (c != PIC_CELL_OUT) {
             const int i = cell_i(c), j = cell_j(c);
             imin = min(imin, i); imax = max(imax, i); jmin = min(jmin, j); jmax = max(jmax, j);
@@ -336,15 +403,15 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     if (do_kick || do_mcc) {
       PhiGather pg{J.phi32, J.nx, J.ny};
       for (int r = 0; r < kRounds; ++r) {
-        const int p = base + r * PIC_MOVER_THREADS + t;
-        const bool valid = p < n;
+        const int q = r * PIC_MOVER_THREADS + t;
+        const bool valid = base + q < n;
         bool cand = false;
         if (valid) {
-          const uint32_t c = S.cell[p];
-          float vx = S.vx[p], vy = S.vy[p];
+          const uint32_t c = s_cell[q];
+          float vx = s_vx[q], vy = s_vy[q];
           if (do_kick && c != PIC_CELL_OUT) {
             float gx, gy;
-            const float fx = S.fx[p], fy = S.fy[p];
+            const float fx = s_fx[q], fy = s_fy[q];
             if (use_tile) gather_tile(tile, tw, tx0, ty0, J.nx, J.ny, cell_i(c), cell_j(c), fx, fy, gx, gy);
             else gather_dphi(pg, cell_i(c), cell_j(c), fx, fy, gx, gy);
             vx += S.kx * gx;
@@ -352,7 +419,7 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
           }
           if (do_mcc) {
             float u[4];
-            draw4(J.seed, S.pid[p], mcc_step, 0u, u);
+            draw4(J.seed, s_pid[q], mcc_step, 0u, u);
             if (J.mcc_mode == 2) {
               const ProcDev& P = J.procs[S.first_proc];
               const float v2 = vx * vx + vy * vy;
@@ -368,25 +435,24 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
               cand = u[0] < S.pnull;
             }
           }
-          S.vx[p] = vx;
-          S.vy[p] = vy;
+          s_vx[q] = vx;
+          s_vy[q] = vy;
         }
-        // list this warp's candidates (their kicked velocity is already stored)
         const unsigned m = __ballot_sync(0xffffffffu, cand);
-        if (cand) wlist[warp][wcount[warp] + __popc(m & ((1u << lane) - 1u))] = p;
+        if (cand) wlist[warp][wcount[warp] + __popc(m & ((1u << lane) - 1u))] = q;
         __syncwarp();
         if (lane == 0) wcount[warp] += __popc(m);
         __syncwarp();
       }
-      const int nc = wcount[warp];
-      for (int k = lane; k < nc; k += 32) {
-        const int p = wlist[warp][k];
+      const int ncand = wcount[warp];
+      for (int c = lane; c < ncand; c += 32) {
+        const int q = wlist[warp][c];
         float u[4];
-        const uint32_t pid = S.pid[p];
+        const uint32_t pid = s_pid[q];
         draw4(J.seed, pid, mcc_step, 0u, u);
-        float vx = S.vx[p], vy = S.vy[p], vz = S.vz[p];
-        collide(J, S, slots, T, pid, S.cell[p], S.fx[p], S.fy[p], vx, vy, vz, u, mcc_step, proc_count);
-        S.vx[p] = vx; S.vy[p] = vy; S.vz[p] = vz;
+        float vx = s_vx[q], vy = s_vy[q], vz = s_vz[q];
+        collide(J, S, slots, T, pid, s_cell[q], s_fx[q], s_fy[q], vx, vy, vz, u, mcc_step, proc_count);
+        s_vx[q] = vx; s_vy[q] = vy; s_vz[q] = vz;
       }
       __syncwarp();
     }
@@ -396,13 +462,13 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     const bool want_ke = do_kick || do_mcc;
     if (do_drift || do_dep || want_ke) {
       for (int r = 0; r < kRounds; ++r) {
-        const int p = base + r * PIC_MOVER_THREADS + t;
-        const bool valid = p < n;
+        const int q = r * PIC_MOVER_THREADS + t;
+        const bool valid = base + q < n;
         uint32_t c = PIC_CELL_OUT;
         float fx = 0.f, fy = 0.f, vx = 0.f, vy = 0.f;
-        if (valid) { c = S.cell[p]; fx = S.fx[p]; fy = S.fy[p]; vx = S.vx[p]; vy = S.vy[p]; }
+        if (valid) { c = s_cell[q]; fx = s_fx[q]; fy = s_fy[q]; vx = s_vx[q]; vy = s_vy[q]; }
         if (valid && want_ke) {
-          const float vz = do_mcc ? S.vz[p] : 0.f;
+          const float vz = do_mcc ? s_vz[q] : 0.f;
           ke += (double)(vx * vx + vy * vy + vz * vz);
         }
         bool absorbed = false;
@@ -414,29 +480,42 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
         }
         if (do_walls) {
           const int hslot = warp_append(valid && absorbed, hit_counts + s);
-          if (hslot >= 0) S.hits[hslot] = p;
+          if (hslot >= 0) S.hits[hslot] = base + q;
         }
         if (do_dep) warp_deposit(J, S, (valid && !absorbed) ? nc : PIC_CELL_OUT, nfx, nfy);
-        if (valid && do_drift) { S.cell[p] = nc; S.fx[p] = nfx; S.fy[p] = nfy; }
+        if (valid && do_drift) { s_cell[q] = nc; s_fx[q] = nfx; s_fy[q] = nfy; }
       }
     }
-    // ---- diagnostics: kinetic energy and collision counts
+    // ---- results back to global memory with bulk stores
+    tma::fence_proxy_async();
     if (want_ke) {
       for (int o = 16; o; o >>= 1) ke += __shfl_down_sync(0xffffffffu, ke, o);
       if (lane == 0) ke_sh[warp] = ke;
     }
     __syncthreads();
     if (t == 0) {
+      if (do_drift) {
+        tma::bulk_s2g(S.cell + base, s_cell, kChunkBytes);
+        tma::bulk_s2g(S.fx + base, s_fx, kChunkBytes);
+        tma::bulk_s2g(S.fy + base, s_fy, kChunkBytes);
+      }
+      if (do_kick || do_mcc) {
+        tma::bulk_s2g(S.vx + base, s_vx, kChunkBytes);
+        tma::bulk_s2g(S.vy + base, s_vy, kChunkBytes);
+      }
+      if (do_mcc) tma::bulk_s2g(S.vz + base, s_vz, kChunkBytes);
+      tma::bulk_commit();
       if (want_ke) {
         double tk = 0.0;
         for (int w = 0; w < kWarps; ++w) tk += ke_sh[w];
         if (tk != 0.0) atomicAdd(&T.ke[S.species], tk * S.ke_factor);
       }
       if (do_mcc)
-        for (int q = 0; q < 8; ++q)
-          if (proc_count[q]) atomicAdd(&T.collisions[S.species][q], (unsigned long long)proc_count[q]);
+        for (int p = 0; p < 8; ++p)
+          if (proc_count[p]) atomicAdd(&T.collisions[S.species][p], (unsigned long long)proc_count[p]);
     }
   }
+  if (t == 0) tma::bulk_wait_all();
 }
 
 // Exclusive prefix of mover chunks per slot (one CTA; slots are few).
@@ -455,8 +534,10 @@ __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t
 }
 
 int mover_blocks_per_sm() {
+  cudaFuncSetAttribute(mover_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMoverDynSmem);
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, 0) != cudaSuccess || b < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, kMoverDynSmem) != cudaSuccess ||
+      b < 1) {
     cudaGetLastError();
     b = 1;
   }
@@ -466,8 +547,9 @@ int mover_blocks_per_sm() {
 int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t stream) {
   chunk_table_kernel<<<1, 32, 0, stream>>>(L.counts, L.active, L.chunk_prefix, L.nslots);
   if (L.ev_mover_begin) cudaEventRecord(L.ev_mover_begin, stream);
-  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, 0, stream>>>(L.jobs, L.st, L.slots, L.counts, L.hit_counts,
-                                                              L.chunk_prefix, L.nslots, flags, explicit_step);
+  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, kMoverDynSmem, stream>>>(L.jobs, L.st, L.slots, L.counts,
+                                                                          L.hit_counts, L.chunk_prefix, L.nslots, flags,
+                                                                          explicit_step);
   if (L.ev_mover_end) cudaEventRecord(L.ev_mover_end, stream);
   return 2;
 }

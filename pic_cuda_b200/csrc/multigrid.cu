@@ -14,7 +14,8 @@
 //              coarse nodes (fine tile + halo 2*nu+2 in shared memory, every sweep done
 //              locally: a node at distance d from the tile edge is exact for d half-sweeps),
 //              then residual + full weighting straight from shared memory
-//   mg_coarse  one CTA per job runs the whole V-cycle from 33x33 down in shared memory
+//   mg_coarse  one CTA per job runs the whole V-cycle from <= 65x65 down in shared memory
+//   (levels 129^2-513^2 and below run in one thread-block cluster, mg_cluster.cu)
 //   mg_up      prolongation + nu_post sweeps on 32x32 tiles; on level 0 also the FP64
 //              update phi += e, the new FP64 residual, phi32 and the norm (last CTA of each
 //              job reduces the per-tile partials in a fixed order: deterministic).
@@ -455,6 +456,7 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   for (int l = 0; l < M.max_depth; ++l)
     if (M.n_down[l]) { mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l); ++k; }
   if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
+  if (M.n_cluster) k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s);
   for (int l = M.max_depth - 1; l >= 0; --l)
     if (M.n_up[l]) {
       mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0, L.running);

@@ -65,8 +65,9 @@ def test_deposit_matches_oracle(engine, orc, mode):
 
 
 @pytest.mark.parametrize("n,levels,omega,nu,tol_cycles", [
-    (129, 0, 1.0, (2, 2, 2), 6), (257, 0, 1.0, (2, 2, 2), 6), (129, 5, 1.25, (3, 3, 20), 4),
-    (1025, 0, 1.0, (2, 2, 2), 5)])
+    (33, 0, 1.0, (2, 2, 2), 5), (65, 0, 1.0, (2, 2, 2), 5), (129, 0, 1.0, (2, 2, 2), 6),
+    (257, 0, 1.0, (2, 2, 2), 6), (129, 5, 1.25, (3, 3, 20), 4), (513, 0, 1.0, (2, 2, 2), 4),
+    (513, 6, 1.25, (3, 3, 20), 3), (1025, 0, 1.0, (2, 2, 2), 5)])
 def test_multigrid_cycles_match_oracle(orc, n, levels, omega, nu, tol_cycles):
     import torch
     h = 1.0 / (n - 1)
