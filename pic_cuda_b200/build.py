@@ -36,7 +36,9 @@ def _sources() -> list[Path]:
 
 
 def _headers() -> list[Path]:
-    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [HERE.parent / "include" / "pic_b200.h"]
+    inc = HERE.parent / "include"
+    return sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(inc.glob("*.h")) + sorted(
+        (inc / "compat").glob("*"))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

@@ -62,3 +62,35 @@ def test_config_validation_is_host_side():
         assert e.code == _lib.PIC_ERR_ARG
     else:
         raise AssertionError("bad grid accepted")
+
+
+COMPAT_SYMBOLS = [
+    "Grid2D::Grid2D(int, int, double, double)", "Grid2D::~Grid2D()", "Grid2D::debugGrid()",
+    "Particles2D::Particles2D(int)", "Particles2D::~Particles2D()", "Particles2D::add_species(double, double)",
+    "Particles2D::change_species(int, double, double)", "Particles2D::debugParticles(int)",
+    "Particles2D::removeCollidedParticles()", "Boundaries2D::~Boundaries2D()",
+    "Boundaries2D::add_wall(double, double, double, double)", "Boundaries2D::compile_walls()",
+    "solve_multigrid(double*, double*, int, int, int, double, double)",
+    "elasticCollisions(Particles2D&, double, double, cross_sections&)",
+    "updateSimulationCUDA(Particles2D&, Grid2D&, Boundaries2D&, int&, double, int, SimulationTiming&)",
+]
+
+
+def test_library_exports_reference_host_api():
+    """The drop-in classes and functions of include/compat are defined in libpic_b200.so."""
+    import subprocess
+    from pic_cuda_b200 import _lib
+    so = _lib.lib()._name
+    out = subprocess.run(["nm", "-DC", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    for sym in COMPAT_SYMBOLS:
+        assert sym in out, sym
+    assert "read_cross_section(" in out
+
+
+def test_program_written_against_reference_headers_links(tmp_path):
+    """A program using the reference's API (set-up of main.cu, updateSimulationCUDA,
+    removeCollidedParticles, elasticCollisions, solve_multigrid) compiles against
+    include/compat and links to libpic_b200.so."""
+    import compat_io
+    exe = compat_io.build_driver(tmp_path)
+    assert exe.exists()
