@@ -230,6 +230,30 @@ int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int 
 int pic_efield_f64(const double* phi, double* E_xy, int nx, int ny, double dx, double dy,
                    void* stream);
 
+/* No counterpart in the reference.  pic_solve_multigrid_f64 with the same arguments,
+ * arithmetic and return codes, for callers that must not allocate device memory: all
+ * working memory is a fixed array compiled into the library (704 KiB per device), so
+ * grids are limited to PIC_STATIC_MG_MAX_SIDE nodes per side; larger grids return
+ * PIC_ERR_ARG.  Callers that cannot allocate: code whose device memory is all reserved by
+ * its own pool allocator (a cudaMalloc outside the pool may fail or fragment it), and
+ * code in a time-critical loop that must not stall other streams (cudaMalloc/cudaFree may
+ * synchronise the whole device; the other entry point's first call per shape also builds
+ * an internal engine).
+ * - The first call on each device looks up the array's address for that device
+ *   (cudaGetSymbolAddress, with that device current); make that first call before any
+ *   stream capture.
+ * - Nothing needs to be zero beforehand: each call clears the correction on every level
+ *   and recomputes every scratch value before reading it.
+ * - The array is shared by all calls on a device: calls that overlap in time (on
+ *   different streams, or from several threads without ordering) race on it and corrupt
+ *   each other's result.  Issue them on one stream or otherwise one after another.
+ * - The call waits for its stream to finish (it reads the cycle count and residual back). */
+#define PIC_STATIC_MG_MAX_SIDE 257
+int pic_solve_multigrid_f64_static(double* phi, const double* rho, int nx, int ny, int levels,
+                                   double h, double omega, int nu_pre, int nu_post, int nu_coarse,
+                                   double tol, int max_cycles, void* stream,
+                                   int* cycles_out, double* relres_out);
+
 /* ---- misc ---- */
 const char* pic_last_error(void);
 int pic_version(void);

@@ -98,6 +98,8 @@ _SIGS = {
     "pic_solve_multigrid_f64": (_I, [_VP, _VP, _I, _I, _I, C.c_double, C.c_double, _I, _I, _I, C.c_double, _I,
                                      _VP, C.POINTER(_I), _D]),
     "pic_efield_f64": (_I, [_VP, _VP, _I, _I, C.c_double, C.c_double, _VP]),
+    "pic_solve_multigrid_f64_static": (_I, [_VP, _VP, _I, _I, _I, C.c_double, C.c_double, _I, _I, _I, C.c_double,
+                                            _I, _VP, C.POINTER(_I), _D]),
     "pic_last_error": (C.c_char_p, []),
     "pic_version": (_I, []),
     "pic_abi_sizes": (_I, [C.POINTER(_I64)]),

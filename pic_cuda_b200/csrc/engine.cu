@@ -27,6 +27,12 @@ int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+}  // namespace
+
+// Records a failure for pic_last_error() from the other translation units of the library.
+int pic_fail(int code, const char* msg) { return fail(code, msg); }
+
+namespace {
 #define CK(call)                                                                              \
   do {                                                                                        \
     cudaError_t e_ = (call);                                                                  \
