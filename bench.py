@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--step-path", choices=["graph", "stream"], default="graph",
+                    help="timed steps as CUDA-graph launches (default) or stream-ordered launches")
     return ap.parse_args()
 
 
@@ -122,7 +125,7 @@ def workload(args):
     n = args.n_per_species or w["n"]
     dep = L.DEPOSIT_I64 if args.deposit == "i64" else L.DEPOSIT_F32
     cfg = w["builder"](n_per_species=n, deposit=dep) if args.workload != "plain_small" else cf.plasma(
-        129, 0.01, n, tol=1e-6, deposit=dep)
+        129, 0.01, n, tol=1e-6, deposit=dep, warm_start=1)
     steps_job = {"plain_small": 100, "mcc_mixed": 500, "large": 200}[args.workload]
     return cfg, n, w["Te"], w["Ti"], cfg.Lx, steps_job
 
@@ -164,6 +167,65 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# The reference's demo species and walls: Particles2D's default species (q=0.1, m=1,
+# particles.cu:146-149), the species main.cu:188 adds (m=1, q=-1), the domain box plus the
+# two interior walls of main.cu:193-194; main.cu's solver settings (main.cu:113,
+# Multigrid.cu:573) and time step (main.cu:150).
+REF_Q, REF_M = [0.1, -1.0], [1.0, 1.0]
+REF_WALLS = [[0, 0, 1, 0], [1, 0, 1, 1], [1, 1, 0, 1], [0, 1, 0, 0], [0.25, 0.25, 0.25, 0.75],
+             [0.75, 0.25, 0.75, 0.75]]
+
+
+def reference_cuda(local, n_per_species=100_000, grid=129, steps=100, warmup=3):
+    """The reference's own CUDA step (its kernels built from its sources into oracle/_ref,
+    re-sequenced headless as main.cu:60-135, CUDA events around the step loop) and this
+    engine on the same seeded state, grid, species, walls and solver settings, in the
+    reference's units.  The reference's multigrid cannot run at 1025^2 (its cooperative
+    launch fails there), so the comparison is made on the 129^2 configuration."""
+    import numpy as np
+    import torch
+    from oracle import refh
+    from pic_cuda_b200 import _lib as L
+    from pic_cuda_b200 import configs as cf
+    from pic_cuda_b200.engine import Engine
+    if not refh.LIB.exists():
+        return {"unavailable": "oracle/_ref/libpicref.so not built"}
+    rng = np.random.default_rng(1234)
+    N = 2 * n_per_species
+    x, y = rng.uniform(0.2, 0.8, N), rng.uniform(0.2, 0.8, N)  # main.cu:20-21
+    vx, vy = rng.uniform(-0.01, 0.01, N), rng.uniform(-0.01, 0.01, N)
+    t = np.repeat(np.arange(2, dtype=np.int32), n_per_species)
+    dt = 0.01
+    refh.steps(warmup, x, y, vx, vy, t, REF_Q, REF_M, grid, grid, 1.0, 1.0, REF_WALLS, dt)
+    ref = refh.steps(steps, x, y, vx, vy, t, REF_Q, REF_M, grid, grid, 1.0, 1.0, REF_WALLS, dt)
+    cfg = cf.make_config(grid, 1.0, dt, [(REF_Q[0], REF_M[0], 1.0, N), (REF_Q[1], REF_M[1], 1.0, N)],
+                         units=L.UNITS_REF, walls=L.WALLS_SEGMENTS, wall_segments=REF_WALLS, levels=5, omega=1.25,
+                         nu_pre=3, nu_post=3, nu_coarse=20, tol=1e-5)
+    eng = Engine(local)
+    job = eng.add_job(cfg)
+    for s in (0, 1):
+        sel = t == s
+        job.load_species(s, x[sel], y[sel], vx[sel], vy[sel])
+    stream = torch.cuda.Stream()
+    eng.step_graph(warmup, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    eng.step_graph(steps, stream=stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ours = ev0.elapsed_time(ev1) / steps
+    job.destroy()
+    eng.close()
+    return {"config": f"{grid}x{grid}, {N} particles (2 species), reference units, main.cu demo walls, "
+                      f"5-level V-cycles omega 1.25 3/3/20 to 1e-5, dt {dt}, {steps} steps, no MCC",
+            "reference_ms_per_step": ref["ms_per_step"], "ours_ms_per_step": ours,
+            "reference_particle_steps_per_s": N / (ref["ms_per_step"] / 1000.0),
+            "ours_particle_steps_per_s": N / (ours / 1000.0),
+            "speedup": ref["ms_per_step"] / ours,
+            "timing": "CUDA events around each implementation's step loop on the same B200"}
+
+
 def run_ours(args):
     import torch
     from pic_cuda_b200 import _lib as L
@@ -188,7 +250,8 @@ def run_ours(args):
     cf.load_plasma(job, n, Ld, Te, Ti, seed=1234 + 17 * rank, device=dev)
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
-    eng.step_graph(args.warmup, stream=sptr)
+    run_steps = eng.step_graph if args.step_path == "graph" else eng.step
+    run_steps(args.warmup, stream=sptr)
     torch.cuda.synchronize(dev)
     d0 = job.diagnostics()
     n0 = sum(d0["count"])
@@ -200,7 +263,7 @@ def run_ours(args):
     # timed region: whole steps as CUDA graph launches (no host synchronisation inside)
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        eng.step_graph(args.steps, stream=sptr)
+        run_steps(args.steps, stream=sptr)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     if dist:
@@ -260,7 +323,8 @@ def run_ours(args):
                    "l2": "state larger than L2 (no flush needed)",
                    "vcycles_per_step": st["vcycles"] / max(st["steps"], 1),
                    "phase_ms_per_step_stream_ordered": {k: v / prof_steps for k, v in pst["phase_ms"].items()},
-                   "step_path": "pic_step_graph (CUDA graph per step, V-cycle loop as a conditional WHILE node)"},
+                   "step_path": ("pic_step_graph (CUDA graph per step, V-cycle loop as a conditional WHILE node)"
+                                 if args.step_path == "graph" else "pic_step (stream-ordered launches)")},
         "roofline": roofline,
         "gpu_launches": st["kernel_launches"],
         "clocks": clk.summary(),
@@ -269,6 +333,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args, cfg, n, Te, Ti, Ld)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0 and world == 1 and not args.no_ref_cuda:
+        line["reference_cuda"] = reference_cuda(local)
     job.destroy()
     eng.close()
     if dist:

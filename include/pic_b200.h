@@ -141,6 +141,10 @@ typedef struct pic_job_config {
   int ionization_electron_species;  /* species that receives ejected electrons          */
   int ionization_ion_species;       /* species that receives new ions                   */
   uint64_t seed;             /* Philox-4x32-10 key; streams are keyed (seed, pid, step) */
+  /* warm start of each field solve: 0 = the previous step's phi (the reference keeps phi
+   * between steps), 1 = linear extrapolation 2 phi_{k-1} - phi_{k-2} from the last two
+   * solutions (one more FP64 grid; fewer V-cycles to the same tolerance) */
+  int mg_warm_start;
 } pic_job_config;
 
 typedef struct pic_diagnostics {

@@ -422,6 +422,8 @@ struct OracleSim {
   double dx, dy, dt, qref, rhs_scale;
   std::vector<Species> sp;
   std::vector<double> rho, phi, f, Ex, Ey;
+  std::vector<double> phi_prev;   // previous solution (mg_warm_start 1)
+  bool have_prev = false;
   std::vector<Proc> procs;
   std::vector<double> numax;  // per species
   uint32_t next_pid = 0;
@@ -513,6 +515,7 @@ ORC_API void orc_sim_set_grid(void* h, int which, const double* in) {
   std::vector<double>& g = which == PIC_GRID_RHO ? s->rho : which == PIC_GRID_PHI ? s->phi
                            : which == PIC_GRID_EX ? s->Ex : s->Ey;
   std::copy(in, in + g.size(), g.begin());
+  if (which == PIC_GRID_PHI) s->have_prev = false;
 }
 ORC_API void orc_sim_stats(void* h, int64_t* step, int* cycles, double* relres, int64_t* absorbed,
                            int64_t* ncoll, int64_t* nioniz) {
@@ -572,6 +575,19 @@ ORC_API void orc_sim_solve(void* h) {
   OracleSim* s = (OracleSim*)h;
   const pic_job_config& c = s->cfg;
   for (size_t i = 0; i < s->rho.size(); ++i) s->f[i] = s->rhs_scale * s->rho[i];
+  if (c.mg_warm_start) {
+    // initial guess 2 phi_{k-1} - phi_{k-2} once two solutions exist, else phi_{k-1}
+    if (s->have_prev) {
+      for (size_t i = 0; i < s->phi.size(); ++i) {
+        const double g = 2.0 * s->phi[i] - s->phi_prev[i];
+        s->phi_prev[i] = s->phi[i];
+        s->phi[i] = g;
+      }
+    } else {
+      s->phi_prev = s->phi;
+      s->have_prev = true;
+    }
+  }
   s->last_cycles = orc_mg_solve(s->phi.data(), s->f.data(), s->nx, s->ny, c.mg_levels, s->dx, c.omega,
                                 c.nu_pre, c.nu_post, c.nu_coarse, c.tol, c.max_cycles, &s->last_relres);
   orc_efield(s->phi.data(), s->nx, s->ny, s->dx, s->dy, s->Ex.data(), s->Ey.data());

@@ -44,6 +44,7 @@ class JobConfig(C.Structure):
         ("mcc_mode", C.c_int), ("gas_density", C.c_double), ("gas_temperature", C.c_double),
         ("gas_mass", C.c_double), ("n_processes", C.c_int), ("processes", ProcessConfig * MAX_PROCESSES),
         ("ionization_electron_species", C.c_int), ("ionization_ion_species", C.c_int), ("seed", C.c_uint64),
+        ("mg_warm_start", C.c_int),
     ]
 
 

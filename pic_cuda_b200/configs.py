@@ -45,7 +45,7 @@ def make_config(nx: int, L_dom: float, dt: float, species: list[tuple[float, flo
                 units: int = L.UNITS_SI, walls: int = L.WALLS_BOX, wall_segments=(), tol: float = 1e-6,
                 nu_pre: int = 2, nu_post: int = 2, nu_coarse: int = 2, omega: float = 1.0, levels: int = 0,
                 max_cycles: int = 50, deposit: int = L.DEPOSIT_F32, sort_every: int = 10, mcc: dict | None = None,
-                seed: int = 1234) -> L.JobConfig:
+                seed: int = 1234, warm_start: int = 0) -> L.JobConfig:
     """species: (charge C, mass kg, weight, capacity) per species.  mcc: dict with keys
     mode, density, temperature, gas_mass, processes [(type, species, threshold, E, sigma)],
     e_species, i_species."""
@@ -67,6 +67,7 @@ def make_config(nx: int, L_dom: float, dt: float, species: list[tuple[float, flo
     c.deposit_mode = deposit
     c.sort_every = sort_every
     c.seed = seed
+    c.mg_warm_start = warm_start
     keep = []
     if mcc:
         c.mcc_mode = mcc.get("mode", L.MCC_NULL_COLLISION)
@@ -111,17 +112,20 @@ def plasma(nx: int, L_dom: float, n_per_species: int, *, n0: float = 1e15, capac
 
 def plain_small(**kw) -> L.JobConfig:
     kw.setdefault("tol", 1e-6)
+    kw.setdefault("warm_start", 1)
     return plasma(129, 0.01, 100_000, **kw)
 
 
 def mcc_mixed(n_per_species: int = 10_000_000, **kw) -> L.JobConfig:
     kw.setdefault("tol", 1e-9)
+    kw.setdefault("warm_start", 1)
     kw.setdefault("mcc", argon_mcc(3.2e21))
     return plasma(1025, 0.05, n_per_species, **kw)
 
 
 def large(n_per_species: int = 100_000_000, deposit: int = L.DEPOSIT_F32, **kw) -> L.JobConfig:
     kw.setdefault("tol", 1e-9)
+    kw.setdefault("warm_start", 1)
     kw.setdefault("mcc", argon_mcc(3.2e21))
     return plasma(4097, 0.05 * 4, n_per_species, deposit=deposit, **kw)
 

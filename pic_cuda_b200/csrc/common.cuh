@@ -19,7 +19,9 @@
 #define PIC_CELL_OUT 0xFFFFFFFFu
 #define PIC_MAX_LEVELS 14
 #define PIC_COARSE_MAX 65           // a first coarse level this small is solved by one CTA in smem
-#define PIC_CHUNK 1024              // particles per mover work item (256 threads x 4)
+#ifndef PIC_CHUNK
+#define PIC_CHUNK 512               // particles per mover work item (256 threads x 2)
+#endif
 #define PIC_MOVER_THREADS 256
 #define PIC_FIX_SHIFT 40            // int64 deposit: 2^40 per unit deposit charge
 
@@ -71,7 +73,7 @@ struct JobDev {
   long long* rho_i;       // deposit_mode I64
   const double* rho_d;    // deposit_mode 2: caller-owned FP64 charge (stateless solver)
   float* phi32;
-  double* phi64[2];
+  double* phi64[3];       // FP64 iterates: DC ping-pong pair, + previous solution (warm_start 1)
   double* partials;       // per-CTA FP64 partial sums (norms)
   double h;               // grid spacing (dx == dy)
   float dt;
@@ -94,6 +96,7 @@ struct JobDev {
   struct Event* events;
   int event_capacity;
   int up_tiles0;          // number of CTAs of the level-0 update kernel (partials)
+  int warm_start;         // 1: extrapolate the initial guess from the last two solutions
 };
 
 struct Event {            // one ionisation: parent state at collision time + products
@@ -115,6 +118,8 @@ struct JobState {
   int event_count;
   int ticket;              // last-CTA-done counter for deterministic reductions
   int ionizations;
+  int phi_nxt;             // phi64 buffer the next defect-correction update writes
+  int phi_prev1;           // 1 + buffer holding the previous step's solution (0: none)
   int pad;
   unsigned long long collisions[PIC_MAX_SPECIES][8];
   double ke[PIC_MAX_SPECIES];

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -132,6 +133,7 @@ int validate(const pic_job_config* c, std::string& why) {
   }
   if (!(c->omega > 0 && c->omega < 2)) { why = "omega must be in (0, 2)"; return PIC_ERR_ARG; }
   if (c->max_cycles < 1 || !(c->tol >= 0)) { why = "max_cycles >= 1 and tol >= 0 required"; return PIC_ERR_ARG; }
+  if (c->mg_warm_start != 0 && c->mg_warm_start != 1) { why = "mg_warm_start must be 0 or 1"; return PIC_ERR_ARG; }
   if (c->n_walls < 0 || c->n_walls > PIC_MAX_WALLS) { why = "too many walls"; return PIC_ERR_ARG; }
   if (c->deposit_mode != PIC_DEPOSIT_F32 && c->deposit_mode != PIC_DEPOSIT_I64) { why = "bad deposit_mode"; return PIC_ERR_ARG; }
   if (c->mcc_mode < 0 || c->mcc_mode > 2) { why = "bad mcc_mode"; return PIC_ERR_ARG; }
@@ -180,10 +182,11 @@ struct Layout {  // byte sizes of one job's device state
 //  grids <= 65^2 entirely in one CTA (lc = 0); otherwise the first level that fits the
 //  coarse solver, never level 0 (the FP64 defect-correction update lives in the tile
 //  kernels): one CTA up to 65^2, a C-CTA cluster up to cluster_max.
-Layout job_layout(const pic_job_config& c, int cluster_C = 0) {
+Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 0) {
   Layout L{};
   L.levels = c.mg_levels > 0 ? c.mg_levels : auto_levels(c.nx);
-  const int cluster_max = cluster_C >= 16 ? 513 : cluster_C >= 8 ? 257 : PIC_COARSE_MAX;
+  int cluster_max = cluster_C >= 16 ? 513 : cluster_C >= 8 ? 257 : PIC_COARSE_MAX;
+  if (cluster_top > 0) cluster_max = std::min(cluster_max, std::max(cluster_top, PIC_COARSE_MAX));
   int n = c.nx;
   L.lc = -1;
   for (int l = 0; l < L.levels; ++l) {
@@ -197,7 +200,7 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0) {
   if (L.lc < 0) L.lc = L.levels - 1;
   L.ntiles0 = ((c.nx + 31) / 32) * ((c.ny + 31) / 32);
   const int64_t N = (int64_t)c.nx * c.ny;
-  int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16);
+  int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16 + (c.mg_warm_start ? 8 : 0));
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
   b += 16ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
@@ -223,6 +226,11 @@ struct pic_engine {
   int num_sms = 148;
   int mover_bps = 4;
   int cluster_C = 0;          // thread-block cluster size of the coarse solver (0: none)
+  // Largest level side given to the cluster coarse solver.  Measured on B200 (1025^2 job):
+  // tile kernels over all SMs for every level above 65^2 and one CTA below beat the
+  // 16-CTA cluster from 513^2 down (V-cycle 0.20 -> 0.18 ms), so by default the cluster is
+  // not used; PIC_MG_CLUSTER_TOP=<side> selects it for levels up to that side.
+  int cluster_top = PIC_COARSE_MAX;
   size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
   std::vector<JobHost> jobs;
@@ -683,6 +691,7 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
     const size_t s8 = mg_cluster_smem(n8, 0, 8, 8);
     if (mg_cluster_supported(16, s16) > 0) { E->cluster_C = 16; E->cluster_smem_max = s16; }
     else if (mg_cluster_supported(8, s8) > 0) { E->cluster_C = 8; E->cluster_smem_max = s8; }
+    if (const char* v = std::getenv("PIC_MG_CLUSTER_TOP")) E->cluster_top = std::atoi(v);
   }
   const int nslots = kMaxJobs * kSlotsPerJob;
   cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
@@ -774,7 +783,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   for (int j = 0; j < kMaxJobs; ++j)
     if (!E->jobs[j].alive) { id = j; break; }
   if (id < 0) return fail(PIC_ERR_CAPACITY, "engine job table full");
-  const Layout lay = job_layout(*cfg, E->cluster_C);
+  const Layout lay = job_layout(*cfg, E->cluster_C, E->cluster_top);
   if (E->pool_bytes > 0 && E->used_bytes + lay.total > E->pool_bytes) return fail(PIC_ERR_OOM, "engine memory budget exceeded");
   JobHost& J = E->jobs[id];
   J = JobHost();
@@ -818,6 +827,8 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   ALLOC(D.phi32, N * 4);
   ALLOC(D.phi64[0], N * 8);
   ALLOC(D.phi64[1], N * 8);
+  if (c.mg_warm_start) ALLOC(D.phi64[2], N * 8);
+  D.warm_start = c.mg_warm_start;
   for (int l = 0; l < lay.levels; ++l) {
     ALLOC(D.e[l], 4ll * lay.nl[l] * lay.nl[l]);
     ALLOC(D.f[l], 4ll * lay.nl[l] * lay.nl[l]);
@@ -922,6 +933,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
 #undef ALLOC
   CK(cudaMemset(D.phi64[0], 0, N * 8));
   CK(cudaMemset(D.phi64[1], 0, N * 8));
+  if (D.phi64[2]) CK(cudaMemset(D.phi64[2], 0, N * 8));
   CK(cudaMemset(D.phi32, 0, N * 4));
   if (D.rho_f) CK(cudaMemset(D.rho_f, 0, N * 4));
   if (D.rho_i) CK(cudaMemset(D.rho_i, 0, N * 8));
@@ -1325,6 +1337,8 @@ int pic_job_set_grid(pic_engine* E, int job, int which, const double* in, int me
     src = (const double*)E->d_stage;
   }
   launch_grid_import(E->d_jobs + job, E->d_st + job, which, src, J.dev.nx, J.dev.ny, s);
+  // a phi written from outside has no history: the next warm start is phi itself
+  if (which == PIC_GRID_PHI) CK(cudaMemsetAsync(&E->d_st[job].phi_prev1, 0, sizeof(int), s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   return PIC_OK;

@@ -83,7 +83,18 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
   const int nx = J.nx, ny = J.ny;
-  const double* phi = J.phi64[T.phi_cur];
+  const int cur = T.phi_cur;
+  const double* phi = J.phi64[cur];
+  // warm_start 1: the initial guess 2 phi_{k-1} - phi_{k-2} goes to a third buffer (phi_{k-1}
+  // is kept as the next step's history), the defect correction then alternates between that
+  // buffer and the one phi_{k-2} held
+  const bool xs = J.warm_start != 0;
+  const int prev = T.phi_prev1 - 1;
+  const bool hist = xs && prev >= 0;
+  const int tgt = hist ? 3 - cur - prev : (cur + 1) % 3;
+  const double* pp = hist ? J.phi64[prev] : phi;
+  double* guess = xs ? J.phi64[tgt] : nullptr;
+  const double a = hist ? 2.0 : 1.0, b = hist ? 1.0 : 0.0;
   const double inv_h2 = 1.0 / (J.h * J.h);
   double ar = 0.0, af = 0.0;
   for (int k = threadIdx.x; k < kTI * kTI; k += blockDim.x) {
@@ -92,12 +103,16 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     const size_t c = (size_t)j * nx + i;
     const double F = J.rhs_scale * rho_at(J, c);
     double r = 0.0;
+    const double g0 = a * phi[c] - b * pp[c];
     if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
-      const double lap = (phi[c - nx] + phi[c + nx] + phi[c - 1] + phi[c + 1] - 4.0 * phi[c]) * inv_h2;
+      const double gs = (a * phi[c - nx] - b * pp[c - nx]) + (a * phi[c + nx] - b * pp[c + nx]) +
+                        (a * phi[c - 1] - b * pp[c - 1]) + (a * phi[c + 1] - b * pp[c + 1]);
+      const double lap = (gs - 4.0 * g0) * inv_h2;
       r = F - lap;
     }
+    if (xs) guess[c] = g0;
     J.f[0][c] = (float)r;
-    J.phi32[c] = (float)phi[c];
+    J.phi32[c] = (float)g0;
     ar += r * r;
     af += F * F;
   }
@@ -117,6 +132,13 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
     T.cycles = 0;
     T.converged = 0;
+    if (xs) {
+      T.phi_prev1 = cur + 1;
+      T.phi_cur = tgt;
+      T.phi_nxt = hist ? prev : (cur + 2) % 3;
+    } else {
+      T.phi_nxt = cur ^ 1;
+    }
     atomicAdd(running, 1);
   }
 }
@@ -381,9 +403,9 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   }
   // ---- level-0 FP64 update and new residual
   __shared__ double P[(kTU + 2) * (kTU + 2)];
-  const int cur = T.phi_cur;
+  const int cur = T.phi_cur, nxt = T.phi_nxt;
   const double* pc = J.phi64[cur];
-  double* pn = J.phi64[cur ^ 1];
+  double* pn = J.phi64[nxt];
   constexpr int PW = kTU + 2;
   for (int py = warp; py < PW; py += 8)
     for (int px = lane; px < PW; px += 32) {
@@ -421,7 +443,8 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
     T.rnorm2 = r2;
     T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
     T.cycles += 1;
-    T.phi_cur = cur ^ 1;
+    T.phi_cur = nxt;
+    T.phi_nxt = cur;
     if (T.relres < J.tol) { T.converged = 1; atomicSub(running, 1); }
     else if (T.cycles >= J.max_cycles) { T.converged = 2; atomicSub(running, 1); }
   }

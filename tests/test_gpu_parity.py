@@ -91,6 +91,27 @@ def test_multigrid_cycles_match_oracle(orc, n, levels, omega, nu, tol_cycles):
     assert orc.relres(dphi.cpu().numpy(), f, h) < 1.5e-9
 
 
+@pytest.mark.parametrize("n", [257, 513, 1025])
+def test_multigrid_cluster_coarse_solver_matches_oracle(orc, monkeypatch, n):
+    """The thread-block-cluster coarse solver (levels up to 513^2 in one 16-CTA cluster),
+    selected with PIC_MG_CLUSTER_TOP, gives the oracle's V-cycles.  nu_coarse = 4 keys a
+    solver instance of its own, created while the variable is set."""
+    import torch
+    from pic_cuda_b200.engine import solve_multigrid_f64
+    monkeypatch.setenv("PIC_MG_CLUSTER_TOP", "513")
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(n + 1)
+    f = rng.standard_normal((n, n))
+    phi0 = np.zeros((n, n))
+    phi0[:, 0] = -0.25
+    dphi = torch.tensor(phi0, device="cuda")
+    drho = torch.tensor(f, device="cuda")
+    cyc, rel, ok = solve_multigrid_f64(dphi, drho, n, n, 0, h, 1.0, 2, 2, 4, tol=0.0, max_cycles=4)
+    assert cyc == 4 and not ok
+    ref = orc.mg_vcycles(phi0, f, h, 4, levels=0, omega=1.0, nu1=2, nu2=2, nuc=4)
+    assert rel_l2(dphi.cpu().numpy(), ref) < 1e-6
+
+
 def test_manufactured_solution_second_order_gpu(orc):
     import math
     import torch
@@ -191,3 +212,31 @@ def test_multi_step_conservation_and_sort(engine):
         assert d["step"] == 5
     finally:
         job.destroy()
+
+
+def test_extrapolated_warm_start_matches_oracle(engine, orc):
+    """mg_warm_start = 1: per step, the engine's V-cycle count follows the oracle's, and phi
+    agrees with a run using the reference's warm start to the solver tolerance."""
+    n = 30_000
+    runs = {}
+    for ws in (0, 1):
+        cfg = cf.plasma(129, 0.01, n, tol=1e-9, warm_start=ws, deposit=L.DEPOSIT_I64)
+        job = engine.add_job(cfg)
+        cf.load_plasma(job, n, 0.01, 2.0, 0.03, seed=21)
+        sim = orc.Sim(cfg)
+        for s in (0, 1):
+            d = _state(job, s)
+            sim.load(s, d["x"], d["y"], d["vx"], d["vy"], d["vz"], d["pid"])
+        cyc_e, cyc_o = [], []
+        for _ in range(6):
+            engine.step(1)
+            sim.step(1)
+            cyc_e.append(job.diagnostics()["vcycles"])
+            cyc_o.append(sim.stats()["cycles"])
+            assert job.diagnostics()["relres"] < 1e-9
+        runs[ws] = (cyc_e, job.get_grid(L.GRID_PHI))
+        assert all(abs(a - b) <= 1 for a, b in zip(cyc_e, cyc_o)), (cyc_e, cyc_o)
+        assert rel_l2(job.get_grid(L.GRID_PHI), sim.grid(L.GRID_PHI)) < 1e-5
+        job.destroy()
+    assert sum(runs[1][0][2:]) < sum(runs[0][0][2:])
+    assert rel_l2(runs[1][1], runs[0][1]) < 1e-6

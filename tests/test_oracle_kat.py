@@ -213,3 +213,25 @@ def test_oracle_sim_step_conserves_and_absorbs(orc):
     assert ne < 5000 and ni <= 5000 and st["relres"] < 1e-9
     w = cfg.species[0].weight
     assert abs(s.total_charge() - cf.QE * w * (ni - ne)) < 1e-9 * cf.QE * w * 5000
+
+
+def test_oracle_extrapolated_warm_start(orc):
+    """mg_warm_start = 1 (guess 2 phi_{k-1} - phi_{k-2}) reaches the same tolerance in fewer
+    V-cycles than the previous solution as the guess (the reference's warm start)."""
+    from pic_cuda_b200 import _lib as L
+    from pic_cuda_b200 import configs as cf
+    res = {}
+    for ws in (0, 1):
+        cfg = cf.plasma(65, 0.005, 20_000, tol=1e-9, warm_start=ws)
+        s = orc.Sim(cfg)
+        s.load(0, *cf.maxwellian_state(20_000, 0.005, 3.0, cf.ME, 7))
+        s.load(1, *cf.maxwellian_state(20_000, 0.005, 0.03, cf.M_AR, 8))
+        cyc = []
+        for _ in range(8):
+            s.step(1)
+            st = s.stats()
+            assert st["relres"] < 1e-9
+            cyc.append(st["cycles"])
+        res[ws] = (cyc, s.grid(L.GRID_PHI))
+    assert sum(res[1][0][2:]) < sum(res[0][0][2:])
+    assert np.linalg.norm(res[1][1] - res[0][1]) <= 1e-6 * np.linalg.norm(res[0][1])
