@@ -18,7 +18,9 @@
 
 #define PIC_CELL_OUT 0xFFFFFFFFu
 #define PIC_MAX_LEVELS 14
+#ifndef PIC_COARSE_MAX
 #define PIC_COARSE_MAX 65           // a first coarse level this small is solved by one CTA in smem
+#endif
 #ifndef PIC_CHUNK
 #define PIC_CHUNK 512               // particles per mover work item (256 threads x 2)
 #endif
@@ -67,8 +69,12 @@ struct JobDev {
   int nx, ny, ncx, ncy;   // nodes and cells
   int levels, lc;         // multigrid levels; first level solved by the coarse kernel
   int nl[PIC_MAX_LEVELS]; // level sizes (square)
-  float* e[PIC_MAX_LEVELS];
+  float* e[PIC_MAX_LEVELS];   // down leg: pre-smoothed correction (coarse solver output at lc)
   float* f[PIC_MAX_LEVELS];
+  // Up-leg outputs go to separate arrays: an up kernel reads its level's e and f with halos
+  // that other CTAs of the same launch own, so it must not overwrite them in place.
+  float* eu[PIC_MAX_LEVELS];  // up leg: post-smoothed correction of levels 1 .. lc-1
+  float* f0b;                 // second level-0 right-hand side (new defect), see JobState::fsel
   float* rho_f;           // deposit_mode F32
   long long* rho_i;       // deposit_mode I64
   const double* rho_d;    // deposit_mode 2: caller-owned FP64 charge (stateless solver)
@@ -120,7 +126,7 @@ struct JobState {
   int ionizations;
   int phi_nxt;             // phi64 buffer the next defect-correction update writes
   int phi_prev1;           // 1 + buffer holding the previous step's solution (0: none)
-  int pad;
+  int fsel;                // level-0 right-hand side in use: 0 = JobDev::f[0], 1 = JobDev::f0b
   unsigned long long collisions[PIC_MAX_SPECIES][8];
   double ke[PIC_MAX_SPECIES];
   double total_charge;     // filled on request (diagnostics)

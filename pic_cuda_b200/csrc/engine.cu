@@ -202,6 +202,8 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   const int64_t N = (int64_t)c.nx * c.ny;
   int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16 + (c.mg_warm_start ? 8 : 0));
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
+  for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
+  b += 4 * N;                                                         // second level-0 rhs
   b += 16ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
   for (int s = 0; s < c.n_species; ++s) {
@@ -832,7 +834,9 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   for (int l = 0; l < lay.levels; ++l) {
     ALLOC(D.e[l], 4ll * lay.nl[l] * lay.nl[l]);
     ALLOC(D.f[l], 4ll * lay.nl[l] * lay.nl[l]);
+    if (l > 0) ALLOC(D.eu[l], 4ll * lay.nl[l] * lay.nl[l]);
   }
+  ALLOC(D.f0b, N * 4);
   ALLOC(D.partials, 16ll * lay.ntiles0);
   if (c.n_walls > 0) {
     std::vector<double> w(4 * c.n_walls);
@@ -940,7 +944,9 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   for (int l = 0; l < lay.levels; ++l) {
     CK(cudaMemset(D.e[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
     CK(cudaMemset(D.f[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
+    if (D.eu[l]) CK(cudaMemset(D.eu[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
   }
+  CK(cudaMemset(D.f0b, 0, N * 4));
   CK(cudaMemcpy(E->d_jobs + id, &D, sizeof(JobDev), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(E->d_slots + id * kSlotsPerJob, J.slot, sizeof(SlotDev) * kSlotsPerJob, cudaMemcpyHostToDevice));
   CK(cudaMemset(E->d_st + id, 0, sizeof(JobState)));

@@ -150,16 +150,14 @@ __device__ __forceinline__ void warp_deposit(const JobDev& J, const SlotDev& S, 
   }
 }
 
-// 512-particle chunks, a 2048-float phi tile and 4 CTAs (32 warps) per SM: 40 KB of shared
-// memory per CTA.  Measured on B200 against 1024-particle chunks with an 8192-float tile at
-// 2 CTAs per SM: 15% less time per particle pass.
-#ifndef PIC_MOVER_TILE_CAP
-#define PIC_MOVER_TILE_CAP 2048
-#endif
+// 512-particle chunks and 4 CTAs (32 warps) per SM.  Measured on B200 against 1024-particle
+// chunks at 2 CTAs per SM: 15% less time per particle pass.
 #ifndef PIC_MOVER_MIN_BLOCKS
 #define PIC_MOVER_MIN_BLOCKS 4
 #endif
-constexpr int kTileCap = PIC_MOVER_TILE_CAP;   // phi tile (floats) staged per chunk
+// Field nodes (float2 E) a warp stages for its particles' cells; a warp whose cells need more
+// falls back to the gather from global memory.
+constexpr int kWarpField = 96;
 constexpr int kRounds = PIC_CHUNK / PIC_MOVER_THREADS;
 constexpr int kWarps = PIC_MOVER_THREADS / 32;
 
@@ -221,34 +219,21 @@ __device__ void collide(const JobDev& J, const SlotDev& S, const SlotDev* slots,
   atomicAdd(&proc_count[chosen & 7], 1u);
 }
 
-// E at the four nodes of cell (i,j) from a phi tile (rows ty0.., cols tx0.., width tw) in
-// shared memory; same stencils as gather_dphi.
-__device__ __forceinline__ void gather_tile(const float* tile, int tw, int tx0, int ty0, int nx, int ny, int i, int j,
-                                            float fx, float fy, float& gx, float& gy) {
-  const int xl = i > 0 ? i - 1 : 0, xr = (i + 2 < nx) ? i + 2 : nx - 1;
-  const float sx0 = i > 0 ? 0.5f : 1.0f, sx1 = (i + 2 < nx) ? 0.5f : 1.0f;
-  const int yl = j > 0 ? j - 1 : 0, yr = (j + 2 < ny) ? j + 2 : ny - 1;
-  const float sy0 = j > 0 ? 0.5f : 1.0f, sy1 = (j + 2 < ny) ? 0.5f : 1.0f;
-  const float* r0 = tile + (j - ty0) * tw - tx0;
-  const float* r1 = r0 + tw;
-  const float a_l = r0[xl], a_0 = r0[i], a_1 = r0[i + 1], a_r = r0[xr];
-  const float b_l = r1[xl], b_0 = r1[i], b_1 = r1[i + 1], b_r = r1[xr];
-  const float* rl = tile + (yl - ty0) * tw - tx0;
-  const float* rr = tile + (yr - ty0) * tw - tx0;
-  const float c_0 = rl[i], c_1 = rl[i + 1], d_0 = rr[i], d_1 = rr[i + 1];
-  const float ex00 = (a_l - a_1) * sx0, ex10 = (a_0 - a_r) * sx1;
-  const float ex01 = (b_l - b_1) * sx0, ex11 = (b_0 - b_r) * sx1;
-  const float ey00 = (c_0 - b_0) * sy0, ey10 = (c_1 - b_1) * sy0;
-  const float ey01 = (a_0 - d_0) * sy1, ey11 = (a_1 - d_1) * sy1;
-  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-  gx = w00 * ex00 + w10 * ex10 + w01 * ex01 + w11 * ex11;
-  gy = w00 * ey00 + w10 * ey10 + w01 * ey01 + w11 * ey11;
+// E (per unit cell, -dphi) at node (i, j) from phi through the computeElectricField stencils
+// (kernels.cu:134-191): central differences inside, one-sided on the edges.
+__device__ __forceinline__ float2 node_field(const float* __restrict__ phi, int nx, int ny, int i, int j) {
+  const float* row = phi + (size_t)j * nx;
+  const int il = i > 0 ? i - 1 : 0, ir = i < nx - 1 ? i + 1 : nx - 1;
+  const int jl = j > 0 ? j - 1 : 0, jr = j < ny - 1 ? j + 1 : ny - 1;
+  const float sx = (i > 0 && i < nx - 1) ? 0.5f : 1.0f, sy = (j > 0 && j < ny - 1) ? 0.5f : 1.0f;
+  return make_float2((__ldg(row + il) - __ldg(row + ir)) * sx,
+                     (__ldg(phi + (size_t)jl * nx + i) - __ldg(phi + (size_t)jr * nx + i)) * sy);
 }
 
 // Particle arrays of one chunk staged in shared memory.
 enum { A_CELL = 0, A_FX, A_FY, A_VX, A_VY, A_VZ, A_PID, kNArr };
 constexpr int kChunkBytes = PIC_CHUNK * 4;
-constexpr size_t kMoverDynSmem = 2ull * kNArr * kChunkBytes + kTileCap * sizeof(float);
+constexpr size_t kMoverDynSmem = 2ull * kNArr * kChunkBytes;
 
 __device__ __forceinline__ int chunk_slot(const int* __restrict__ chunk_prefix, int nslots, int g) {
   int lo = 0, hi = nslots - 1;
@@ -280,26 +265,29 @@ __device__ __forceinline__ void issue_chunk(const JobDev* __restrict__ jobs, con
   }
 }
 
-// One chunk = PIC_CHUNK particles of one slot; thread t handles chunk entries r*256 + t.
+// One chunk = PIC_CHUNK particles of one slot; warp w owns the contiguous entries
+// [w * kPerWarp, (w + 1) * kPerWarp), lane l handles w * kPerWarp + r * 32 + l.
 // Chunks reach shared memory through bulk asynchronous copies, double buffered: while the
 // CTA works on chunk k, chunk k+1 is in flight, so HBM latency is covered by the copy engine
 // rather than by resident warps; results return with bulk stores.
-//  pass A  kick (phi tile staged in shared memory when the chunk's cells fit) and the
-//          null-collision candidate test; candidates (~nu_max dt of the particles) are listed
-//          per warp and collided by that warp's lanes afterwards
+//  pass A  kick and the null-collision candidate test.  Each warp stages E at the nodes of its
+//          own cells (particles are cell-sorted, so a warp's 64 particles touch a few cells)
+//          and gathers from there; candidates (~nu_max dt of the particles) are listed per
+//          warp and collided by that warp's lanes afterwards
 //  pass B  drift, absorption, hit list and CIC deposit
-// The slot and job tables are copied to shared memory per chunk: every parameter read in
-// the per-particle code is a shared-memory load.
+// Two block barriers per chunk (chunk data ready; results complete before the bulk stores),
+// a third only when the chunk starts a new slot and the slot and job tables are copied to
+// shared memory (every parameter read in the per-particle code is a shared-memory load).
 __global__ void __launch_bounds__(PIC_MOVER_THREADS, PIC_MOVER_MIN_BLOCKS)
 mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
              const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ chunk_prefix,
              int nslots, int flags, uint32_t explicit_step) {
   extern __shared__ __align__(128) uint32_t dsm[];
-  float* tile = reinterpret_cast<float*>(dsm + 2 * kNArr * PIC_CHUNK);
+  constexpr int kPerWarp = PIC_CHUNK / kWarps;
   __shared__ __align__(8) uint64_t mbar[2];
-  __shared__ int wlist[kWarps][PIC_CHUNK / kWarps];
+  __shared__ int wlist[kWarps][kPerWarp];
   __shared__ int wcount[kWarps];
-  __shared__ int bb[4];
+  __shared__ float2 wfield[kWarps][kWarpField];
   __shared__ unsigned proc_count[8];
   __shared__ double ke_sh[kWarps];
   __shared__ SlotDev sS;
@@ -307,6 +295,7 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
   __shared__ int cur_slot;
   __shared__ int abort_flag;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int wbase = warp * kPerWarp;
   const int total = chunk_prefix[nslots];
   if (t == 0) {
     cur_slot = -1;
@@ -315,6 +304,7 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     tma::mbar_init(&mbar[1], 1);
     tma::fence_mbar_init();
   }
+  if (t < 8) proc_count[t] = 0u;
   __syncthreads();
   uint32_t parity[2] = {0u, 0u};
   if (t == 0 && (int)blockIdx.x < total) issue_chunk(jobs, slots, chunk_prefix, nslots, blockIdx.x, dsm, &mbar[0]);
@@ -322,14 +312,16 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
   for (int g = blockIdx.x; g < total; g += gridDim.x, ++k) {
     const int b = k & 1;
     uint32_t* buf = dsm + b * kNArr * PIC_CHUNK;
-    // prefetch the next chunk into the other buffer (after its last bulk store has been read)
+    // prefetch the next chunk into the other buffer, once the bulk stores of the chunk that
+    // used it have read their source (every thread finished with that buffer before the
+    // previous iteration's second barrier)
     if (t == 0 && g + (int)gridDim.x < total) {
       tma::bulk_wait_read_all();
       issue_chunk(jobs, slots, chunk_prefix, nslots, g + gridDim.x, dsm + (b ^ 1) * kNArr * PIC_CHUNK, &mbar[b ^ 1]);
     }
     const int s = chunk_slot(chunk_prefix, nslots, g);
-    __syncthreads();
-    if (cur_slot != s) {  // copy the slot and job tables to shared memory
+    if (cur_slot != s) {  // uniform: cur_slot changed before the previous iteration's last barrier
+      __syncthreads();    // thread 0 may still read the old tables for the previous chunk's stores
       const int* srcS = reinterpret_cast<const int*>(slots + s);
       const int* srcJ = reinterpret_cast<const int*>(jobs + slots[s].job);
       int* dS = reinterpret_cast<int*>(&sS);
@@ -367,52 +359,46 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     float* s_vz = reinterpret_cast<float*>(buf + A_VZ * PIC_CHUNK);
     const uint32_t* s_pid = buf + A_PID * PIC_CHUNK;
 
-    // ---- phi tile of the chunk (bounding box of the cells + 1 node below, 2 above)
-    bool use_tile = false;
-    int tx0 = 0, ty0 = 0, tw = 0;
-    if (do_kick) {
-      int imin = 1 << 30, imax = -1, jmin = 1 << 30, jmax = -1;
-      for (int r = 0; r < kRounds; ++r) {
-        const int q = r * PIC_MOVER_THREADS + t;
-        if (base + q < n) {
-          const uint32_t c = s_cell[q];
-          if (c != PIC_CELL_OUT) {
-            const int i = cell_i(c), j = cell_j(c);
-            imin = min(imin, i); imax = max(imax, i); jmin = min(jmin, j); jmax = max(jmax, j);
-          }
-        }
-      }
-      imin = __reduce_min_sync(0xffffffffu, imin); jmin = __reduce_min_sync(0xffffffffu, jmin);
-      imax = __reduce_max_sync(0xffffffffu, imax); jmax = __reduce_max_sync(0xffffffffu, jmax);
-      if (t == 0) { bb[0] = 1 << 30; bb[1] = -1; bb[2] = 1 << 30; bb[3] = -1; }
-      __syncthreads();
-      if (lane == 0) { atomicMin(&bb[0], imin); atomicMax(&bb[1], imax); atomicMin(&bb[2], jmin); atomicMax(&bb[3], jmax); }
-      __syncthreads();
-      if (bb[1] >= 0) {
-        tx0 = max(bb[0] - 1, 0);
-        ty0 = max(bb[2] - 1, 0);
-        const int tx1 = min(bb[1] + 2, J.nx - 1), ty1 = min(bb[3] + 2, J.ny - 1);
-        tw = tx1 - tx0 + 1;
-        const int th = ty1 - ty0 + 1;
-        use_tile = tw * th <= kTileCap;
-        if (use_tile) {
-          for (int ry = warp; ry < th; ry += kWarps) {
-            const float* src = J.phi32 + (size_t)(ty0 + ry) * J.nx + tx0;
-            for (int rx = lane; rx < tw; rx += 32) tile[ry * tw + rx] = __ldg(src + rx);
-          }
-        }
-      }
-      __syncthreads();
-    }
-    if (t < 8) proc_count[t] = 0u;
-    if (lane == 0) wcount[warp] = 0;
-    __syncwarp();
-
     // ---- pass A: kick and collisions
     if (do_kick || do_mcc) {
+      // E at the nodes of this warp's cells: nodes [i0, i0 + fw) x [j0, j0 + fh)
+      int fi0 = 0, fj0 = 0, fw = 0;
+      bool use_field = false;
+      if (do_kick) {
+        int imin = 1 << 30, imax = -1, jmin = 1 << 30, jmax = -1;
+#pragma unroll
+        for (int r = 0; r < kRounds; ++r) {
+          const int q = wbase + r * 32 + lane;
+          if (base + q < n) {
+            const uint32_t c = s_cell[q];
+            if (c != PIC_CELL_OUT) {
+              const int i = cell_i(c), j = cell_j(c);
+              imin = min(imin, i); imax = max(imax, i); jmin = min(jmin, j); jmax = max(jmax, j);
+            }
+          }
+        }
+        imin = __reduce_min_sync(0xffffffffu, imin); jmin = __reduce_min_sync(0xffffffffu, jmin);
+        imax = __reduce_max_sync(0xffffffffu, imax); jmax = __reduce_max_sync(0xffffffffu, jmax);
+        if (imax >= 0) {
+          fi0 = imin;
+          fj0 = jmin;
+          fw = imax - imin + 2;
+          const int fh = jmax - jmin + 2;
+          use_field = fw * fh <= kWarpField;
+          if (use_field)
+            for (int e = lane; e < fw * fh; e += 32) {
+              const int ej = e / fw;
+              wfield[warp][e] = node_field(J.phi32, J.nx, J.ny, fi0 + (e - ej * fw), fj0 + ej);
+            }
+        }
+        __syncwarp();
+      }
       PhiGather pg{J.phi32, J.nx, J.ny};
+      if (lane == 0) wcount[warp] = 0;
+      __syncwarp();
+#pragma unroll
       for (int r = 0; r < kRounds; ++r) {
-        const int q = r * PIC_MOVER_THREADS + t;
+        const int q = wbase + r * 32 + lane;
         const bool valid = base + q < n;
         bool cand = false;
         if (valid) {
@@ -421,8 +407,16 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
           if (do_kick && c != PIC_CELL_OUT) {
             float gx, gy;
             const float fx = s_fx[q], fy = s_fy[q];
-            if (use_tile) gather_tile(tile, tw, tx0, ty0, J.nx, J.ny, cell_i(c), cell_j(c), fx, fy, gx, gy);
-            else gather_dphi(pg, cell_i(c), cell_j(c), fx, fy, gx, gy);
+            const int i = cell_i(c), j = cell_j(c);
+            if (use_field) {
+              const float2* e0 = &wfield[warp][(j - fj0) * fw + (i - fi0)];
+              const float2 e00 = e0[0], e10 = e0[1], e01 = e0[fw], e11 = e0[fw + 1];
+              const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+              gx = w00 * e00.x + w10 * e10.x + w01 * e01.x + w11 * e11.x;
+              gy = w00 * e00.y + w10 * e10.y + w01 * e01.y + w11 * e11.y;
+            } else {
+              gather_dphi(pg, i, j, fx, fy, gx, gy);
+            }
             vx += S.kx * gx;
             vy += S.ky * gy;
           }
@@ -470,8 +464,9 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     double ke = 0.0;
     const bool want_ke = do_kick || do_mcc;
     if (do_drift || do_dep || want_ke) {
+#pragma unroll
       for (int r = 0; r < kRounds; ++r) {
-        const int q = r * PIC_MOVER_THREADS + t;
+        const int q = wbase + r * 32 + lane;
         const bool valid = base + q < n;
         uint32_t c = PIC_CELL_OUT;
         float fx = 0.f, fy = 0.f, vx = 0.f, vy = 0.f;
@@ -519,9 +514,15 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
         for (int w = 0; w < kWarps; ++w) tk += ke_sh[w];
         if (tk != 0.0) atomicAdd(&T.ke[S.species], tk * S.ke_factor);
       }
-      if (do_mcc)
-        for (int p = 0; p < 8; ++p)
-          if (proc_count[p]) atomicAdd(&T.collisions[S.species][p], (unsigned long long)proc_count[p]);
+      // read and clear the collision counters; the next chunk's collisions start after its
+      // first barrier, which thread 0 reaches only after this
+      for (int p = 0; p < 8; ++p) {
+        const unsigned c = proc_count[p];
+        if (c) {
+          atomicAdd(&T.collisions[S.species][p], (unsigned long long)c);
+          proc_count[p] = 0u;
+        }
+      }
     }
   }
   if (t == 0) tma::bulk_wait_all();

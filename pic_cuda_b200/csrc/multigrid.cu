@@ -33,6 +33,17 @@ __device__ __forceinline__ double rho_at(const JobDev& J, size_t idx) {
   return J.deposit_mode == 0 ? (double)J.rho_f[idx] : J.deposit_mode == 1 ? (double)J.rho_i[idx] * 0x1p-40 : J.rho_d[idx];
 }
 
+// The charge grid of a job, copied to registers (see mg_up_kernel).
+struct RhoSrc {
+  int mode;
+  const float* f;
+  const long long* i;
+  const double* d;
+  __device__ __forceinline__ double operator[](size_t idx) const {
+    return mode == 0 ? (double)f[idx] : mode == 1 ? (double)i[idx] * 0x1p-40 : d[idx];
+  }
+};
+
 __device__ double block_sum(double v) {
   __shared__ double ws[32];
   for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -94,6 +105,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   const int tgt = hist ? 3 - cur - prev : (cur + 1) % 3;
   const double* pp = hist ? J.phi64[prev] : phi;
   double* guess = xs ? J.phi64[tgt] : nullptr;
+  float* const f0 = T.fsel ? J.f0b : J.f[0];
   const double a = hist ? 2.0 : 1.0, b = hist ? 1.0 : 0.0;
   const double inv_h2 = 1.0 / (J.h * J.h);
   double ar = 0.0, af = 0.0;
@@ -111,7 +123,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
       r = F - lap;
     }
     if (xs) guess[c] = g0;
-    J.f[0][c] = (float)r;
+    f0[c] = (float)r;
     J.phi32[c] = (float)g0;
     ar += r * r;
     af += F * F;
@@ -187,7 +199,11 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
   const int W = 2 * kTC + 3 + 2 * H;
   float* e = sm;
   float* f = sm + W * W;
-  const float* fg = J.f[l];
+  const float* fg = (l == 0 && st[tr.job].fsel) ? J.f0b : J.f[l];
+  // parameters read before the first barrier (after it, reads through J would be reloaded)
+  float* const eg = J.e[l];
+  float* const fc = J.f[l + 1];
+  const float omega = J.omega;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll 4
   for (int ly = warp; ly < W; ly += 8) {
@@ -200,9 +216,8 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
     }
   }
   __syncthreads();
-  tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
+  tile_sweeps(e, f, W, gx0, gy0, nf, h2, omega, nu);
   // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
-  float* eg = J.e[l];
   for (int oy = warp; oy < 2 * kTC; oy += 8) {
     const int gy = 2 * jc0 + oy;
     if (gy >= nf) break;
@@ -210,7 +225,6 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
     if (gx < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
   }
   // residual + full weighting to the owned coarse nodes
-  float* fc = J.f[l + 1];
   for (int k = threadIdx.x; k < kTC * kTC; k += blockDim.x) {
     const int ic = ic0 + k % kTC, jc = jc0 + k / kTC;
     if (ic >= nc || jc >= nc) continue;
@@ -260,28 +274,39 @@ __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__
   const int job = job_list[blockIdx.x];
   const JobDev& J = jobs[job];
   if (st[job].converged) return;
+  // The job's parameters are read once, before the first barrier: a barrier also orders the
+  // compiler's view of global memory, so fields read through J afterwards would be reloaded.
   const int lc = J.lc, L = J.levels;
+  const double h = J.h;
+  const float omega = J.omega;
+  const int nu_pre = J.nu_pre, nu_post = J.nu_post, nu_coarse = J.nu_coarse;
+  float* const e_top = J.e[lc];
+  const float* const f_top = (lc == 0 && st[job].fsel) ? J.f0b : J.f[lc];
   // level l occupies [off[l], off[l] + 2 n_l^2) of shared memory: E then F
   __shared__ int off[PIC_MAX_LEVELS];
+  __shared__ int nl[PIC_MAX_LEVELS];
+  if (threadIdx.x < PIC_MAX_LEVELS) nl[threadIdx.x] = J.nl[threadIdx.x];
   if (threadIdx.x == 0) {
     int o = 0;
     for (int k = lc; k < L; ++k) { off[k] = o; o += 2 * J.nl[k] * J.nl[k]; }
   }
   __syncthreads();
 #define E(l) (sm + off[l])
-#define F(l) (sm + off[l] + J.nl[l] * J.nl[l])
+#define F(l) (sm + off[l] + nl[l] * nl[l])
   {
-    const int n = J.nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F(lc)[k] = J.f[lc][k]; E(lc)[k] = 0.f; }
+    const int n = nl[lc];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F(lc)[k] = f_top[k]; E(lc)[k] = 0.f; }
   }
   __syncthreads();
   for (int l = lc; l < L - 1; ++l) {
-    const int n = J.nl[l], nc = J.nl[l + 1];
-    const double hl = J.h * (double)(1 << l);
+    const int n = nl[l], nc = nl[l + 1];
+    const double hl = h * (double)(1 << l);
     const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
-    smem_sweeps(E(l), F(l), n, h2, J.omega, J.nu_pre);
+    smem_sweeps(E(l), F(l), n, h2, omega, nu_pre);
     const float* e = E(l);
     const float* f = F(l);
+    float* fn = F(l + 1);
+    float* en = E(l + 1);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int jc = warp; jc < nc; jc += nwarp) {
       for (int ic = lane; ic < nc; ic += 32) {
@@ -299,19 +324,20 @@ __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__
           v = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] + r[0][2] +
                r[2][0] + r[2][2]) * 0.0625f;
         }
-        F(l + 1)[jc * nc + ic] = v;
-        E(l + 1)[jc * nc + ic] = 0.f;
+        fn[jc * nc + ic] = v;
+        en[jc * nc + ic] = 0.f;
       }
     }
     __syncthreads();
   }
   {
-    const double hl = J.h * (double)(1 << (L - 1));
-    smem_sweeps(E(L - 1), F(L - 1), J.nl[L - 1], (float)(hl * hl), J.omega, J.nu_coarse);
+    const double hl = h * (double)(1 << (L - 1));
+    smem_sweeps(E(L - 1), F(L - 1), nl[L - 1], (float)(hl * hl), omega, nu_coarse);
   }
   for (int l = L - 2; l >= lc; --l) {
-    const int n = J.nl[l], nc = J.nl[l + 1];
+    const int n = nl[l], nc = nl[l + 1];
     const float* c = E(l + 1);
+    float* el = E(l);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int j = 1 + warp; j < n - 1; j += nwarp) {   // boundary nodes receive 0 (coarse boundary is 0)
       for (int i = 1 + lane; i < n - 1; i += 32) {
@@ -322,16 +348,16 @@ __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__
         else if ((i & 1) && !(j & 1)) v = 0.5f * (cp[0] + cp[1]);
         else if (!(i & 1) && (j & 1)) v = 0.5f * (cp[0] + cp[nc]);
         else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
-        E(l)[j * n + i] += v;
+        el[j * n + i] += v;
       }
     }
     __syncthreads();
-    const double hl = J.h * (double)(1 << l);
-    smem_sweeps(E(l), F(l), n, (float)(hl * hl), J.omega, J.nu_post);
+    const double hl = h * (double)(1 << l);
+    smem_sweeps(E(l), F(l), n, (float)(hl * hl), omega, nu_post);
   }
   {
-    const int n = J.nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) J.e[lc][k] = E(lc)[k];
+    const int n = nl[lc];
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) e_top[k] = E(lc)[k];
   }
 #undef E
 #undef F
@@ -356,11 +382,28 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const int W = kTU + 2 * H + 2 * X;
   float* e = sm;
   float* f = sm + W * W;
+  const int fsel = T.fsel;
   const float* eg = J.e[l];
-  const float* fg = J.f[l];
+  const float* fg = (l == 0 && fsel) ? J.f0b : J.f[l];
   const bool prolong = mode != 2;
   const int nc = prolong ? J.nl[l + 1] : 0;
-  const float* ec = prolong ? J.e[l + 1] : nullptr;
+  // the coarser correction: the coarse solver's output at lc, else the up kernel's of l + 1
+  const float* ec = prolong ? (l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1]) : nullptr;
+  // everything else the kernel needs from the job, read before the first barrier (after it,
+  // reads through J and T would be reloaded from global memory)
+  const float omega = J.omega;
+  float* const eo = J.eu[l];
+  const int cur = T.phi_cur, nxt = T.phi_nxt;
+  const double* const pc = J.phi64[cur];
+  double* const pn = J.phi64[nxt];
+  const double inv_h2 = 1.0 / (J.h * J.h);
+  const double rhs_scale = J.rhs_scale;
+  const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
+  float* const phi32 = J.phi32;
+  float* const f0 = fsel ? J.f[0] : J.f0b;   // the new defect goes to the other buffer
+  double* const partials = J.partials;
+  const double tol = J.tol;
+  const int max_cycles = J.max_cycles;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll 2
   for (int ly = warp; ly < W; ly += 8)
@@ -392,9 +435,8 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
     f[k] = fv;
   }
   __syncthreads();
-  if (nu > 0) tile_sweeps(e, f, W, gx0, gy0, nf, h2, J.omega, nu);
+  if (nu > 0) tile_sweeps(e, f, W, gx0, gy0, nf, h2, omega, nu);
   if (mode == 0) {
-    float* eo = J.e[l];
     for (int oy = warp; oy < kTU; oy += 8) {
       const int gy = j0 + oy, gx = i0 + lane;
       if (gy < nf && gx < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
@@ -403,9 +445,6 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   }
   // ---- level-0 FP64 update and new residual
   __shared__ double P[(kTU + 2) * (kTU + 2)];
-  const int cur = T.phi_cur, nxt = T.phi_nxt;
-  const double* pc = J.phi64[cur];
-  double* pn = J.phi64[nxt];
   constexpr int PW = kTU + 2;
   for (int py = warp; py < PW; py += 8)
     for (int px = lane; px < PW; px += 32) {
@@ -415,7 +454,6 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
       P[py * PW + px] = v;
     }
   __syncthreads();
-  const double inv_h2 = 1.0 / (J.h * J.h);
   double ar = 0.0;
   for (int oy = warp; oy < kTU; oy += 8) {
     const int ox = lane;
@@ -423,30 +461,31 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
     if (gx >= nf || gy >= nf) continue;
     const size_t g = (size_t)gy * nf + gx;
     const int q = (oy + 1) * PW + (ox + 1);
-    const double F = J.rhs_scale * rho_at(J, g);
+    const double F = rhs_scale * rho[g];
     double r = 0.0;
     if (gx > 0 && gx < nf - 1 && gy > 0 && gy < nf - 1) {
       const double lap = (P[q - PW] + P[q + PW] + P[q - 1] + P[q + 1] - 4.0 * P[q]) * inv_h2;
       r = F - lap;
     }
     pn[g] = P[q];
-    J.phi32[g] = (float)P[q];
-    J.f[0][g] = (float)r;
+    phi32[g] = (float)P[q];
+    f0[g] = (float)r;
     ar += r * r;
   }
   const double sr = block_sum(ar);
-  if (threadIdx.x == 0) J.partials[2 * (tr.pbase + tr.local)] = sr;
+  if (threadIdx.x == 0) partials[2 * (tr.pbase + tr.local)] = sr;
   if (last_of_job(T, tr.nlocal)) {
     __threadfence();
-    const double r2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 0);
+    const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
     if (threadIdx.x != 0) return;
     T.rnorm2 = r2;
     T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
     T.cycles += 1;
     T.phi_cur = nxt;
     T.phi_nxt = cur;
-    if (T.relres < J.tol) { T.converged = 1; atomicSub(running, 1); }
-    else if (T.cycles >= J.max_cycles) { T.converged = 2; atomicSub(running, 1); }
+    T.fsel = fsel ^ 1;
+    if (T.relres < tol) { T.converged = 1; atomicSub(running, 1); }
+    else if (T.cycles >= max_cycles) { T.converged = 2; atomicSub(running, 1); }
   }
 }
 
