@@ -289,6 +289,7 @@ EngineLaunch make_launch(pic_engine* E, const uint8_t* active) {
   L.num_sms = E->num_sms;
   L.mover_grid = E->num_sms * E->mover_bps;
   L.running = E->d_running;
+  L.gbar = reinterpret_cast<unsigned*>(E->d_running + 2);  // the grid barrier's arrival counter
   L.absorbed = E->d_aux + 4 * kMaxJobs * kSlotsPerJob;
   return L;
 }
@@ -388,6 +389,14 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   M.coarse_smem = coarse_smem;
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
+  // Levels 1..lc as phases of one cooperative launch (PIC_MG_LEVELS_KERNEL=1).  Measured on
+  // B200 (1025^2 job, CUDA-graph step): 1.600 ms per step against 1.555 ms with one launch per
+  // level, because at these sizes each phase waits on its slowest tile either way and the grid
+  // barriers add to that; so it is off by default.
+  const char* lv = std::getenv("PIC_MG_LEVELS_KERNEL");
+  if (cluster.empty() && max_depth >= 2 && lv && std::atoi(lv) == 1)
+    M.levels_grid = mg_levels_configure(E->num_sms, nu_pre_max, nu_post_max, coarse_smem, &M.levels_smem,
+                                        &M.levels_quarter_floats);
   out.max_cycles = max_cycles;
   out.valid = true;
   if (coarse_smem > 227 * 1024 || cluster_smem > 227 * 1024)

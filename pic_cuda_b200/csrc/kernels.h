@@ -36,6 +36,7 @@ struct EngineLaunch {
   int mover_grid;
   int num_sms;
   int* running;           // jobs whose field solve is still iterating
+  unsigned* gbar;         // arrival counter of the grid barriers in mg_levels_kernel
   int* absorbed;          // particles absorbed in the last step, per slot
   cudaEvent_t ev_mover_begin, ev_mover_end;  // optional timing of the particle pass
 };
@@ -67,7 +68,23 @@ struct MgLaunch {
   int max_depth;                                         // max lc over jobs
   size_t coarse_smem;
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
+  int levels_grid;                                       // >0: levels 1..lc in one cooperative launch
+  size_t levels_smem, levels_quarter_floats;
 };
+// Arguments of the cooperative launch that runs levels 1..lc of the V-cycle.
+struct MgLevelsArgs {
+  const TileRef* down_tiles[PIC_MAX_LEVELS]; int n_down[PIC_MAX_LEVELS];
+  const TileRef* up_tiles[PIC_MAX_LEVELS]; int n_up[PIC_MAX_LEVELS];
+  const int* coarse_jobs; int n_coarse;
+  int max_depth;
+  size_t quarter_floats;
+  const JobDev* jobs;
+  JobState* st;
+  unsigned* gbar;
+};
+// Grid size (0: not available) and shared memory of the cooperative levels kernel.
+int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coarse_smem, size_t* smem,
+                        size_t* quarter_floats);
 int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 void mg_configure_coarse(size_t smem_bytes);

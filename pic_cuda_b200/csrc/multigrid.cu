@@ -155,14 +155,29 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   }
 }
 
+// Thread groups a tile is processed by: a whole 256-thread CTA, or one 256-thread quarter of a
+// 1024-thread CTA synchronised by its own hardware barrier (ids 1-4; 0 is __syncthreads).
+struct BlockGroup {
+  static constexpr int kSize = 256;
+  __device__ __forceinline__ int rank() const { return threadIdx.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+struct QuarterGroup {
+  static constexpr int kSize = 256;
+  int q;
+  __device__ __forceinline__ int rank() const { return threadIdx.x & 255; }
+  __device__ __forceinline__ void sync() const { asm volatile("bar.sync %0, 256;" ::"r"(q + 1) : "memory"); }
+};
+
 // Red-black SOR half-sweeps on a W x W shared tile whose node (0,0) is grid node (gx0,gy0).
 // Only grid-interior nodes that are not on the tile's outer ring are updated.  Rows are
 // spread over warps and the nodes of one colour in a row over lanes, so no thread divides
 // or skips nodes of the other colour.
-__device__ __forceinline__ void tile_sweeps(float* e, const float* f, int W, int gx0, int gy0, int n, float h2,
-                                            float omega, int nu) {
+template <class G>
+__device__ __forceinline__ void tile_sweeps(const G& g, float* e, const float* f, int W, int gx0, int gy0, int n,
+                                            float h2, float omega, int nu) {
   const float om1 = 1.f - omega;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int lane = g.rank() & 31, warp = g.rank() >> 5, nwarp = G::kSize >> 5;
   const int ly_lo = max(1, 1 - gy0), ly_hi = min(W - 2, n - 2 - gy0);   // rows to update
   const int lx_lo = max(1, 1 - gx0), lx_hi = min(W - 2, n - 2 - gx0);   // columns to update
   for (int it = 0; it < nu; ++it) {
@@ -178,16 +193,17 @@ __device__ __forceinline__ void tile_sweeps(float* e, const float* f, int W, int
           row[lx] = fmaf(omega, nv, om1 * row[lx]);
         }
       }
-      __syncthreads();
+      g.sync();
     }
   }
 }
 
 // ---------------------------------------------------------------- mg_down
-__global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
-                                                      const JobState* __restrict__ st, int l) {
-  extern __shared__ float sm[];
-  const TileRef tr = tiles[blockIdx.x];
+// Pre-smoothing of one tile of level l (from a zero correction), its residual and the full
+// weighting of it to level l + 1.
+template <class G>
+__device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict__ jobs,
+                          const JobState* __restrict__ st, int l, float* sm) {
   const JobDev& J = jobs[tr.job];
   if (st[tr.job].converged) return;
   const int nf = J.nl[l], nc = J.nl[l + 1];
@@ -204,7 +220,7 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
   float* const eg = J.e[l];
   float* const fc = J.f[l + 1];
   const float omega = J.omega;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lane = g.rank() & 31, warp = g.rank() >> 5;
 #pragma unroll 4
   for (int ly = warp; ly < W; ly += 8) {
     const int gy = gy0 + ly;
@@ -215,8 +231,8 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
       e[ly * W + lx] = 0.f;
     }
   }
-  __syncthreads();
-  tile_sweeps(e, f, W, gx0, gy0, nf, h2, omega, nu);
+  g.sync();
+  tile_sweeps(g, e, f, W, gx0, gy0, nf, h2, omega, nu);
   // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
   for (int oy = warp; oy < 2 * kTC; oy += 8) {
     const int gy = 2 * jc0 + oy;
@@ -225,7 +241,7 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
     if (gx < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
   }
   // residual + full weighting to the owned coarse nodes
-  for (int k = threadIdx.x; k < kTC * kTC; k += blockDim.x) {
+  for (int k = g.rank(); k < kTC * kTC; k += G::kSize) {
     const int ic = ic0 + k % kTC, jc = jc0 + k / kTC;
     if (ic >= nc || jc >= nc) continue;
     float v = 0.f;
@@ -246,6 +262,13 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
     }
     fc[(size_t)jc * nc + ic] = v;
   }
+  g.sync();  // the tile's shared memory is free for the group's next tile
+}
+
+__global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
+                                                      const JobState* __restrict__ st, int l) {
+  extern __shared__ float sm[];
+  down_tile(BlockGroup{}, tiles[blockIdx.x], jobs, st, l, sm);
 }
 
 // ---------------------------------------------------------------- mg_coarse
@@ -268,10 +291,9 @@ __device__ void smem_sweeps(float* e, const float* f, int n, float h2, float ome
   }
 }
 
-__global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
-                                                         const JobState* __restrict__ st) {
-  extern __shared__ float sm[];
-  const int job = job_list[blockIdx.x];
+// The levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.
+__device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, const JobState* __restrict__ st,
+                             float* sm) {
   const JobDev& J = jobs[job];
   if (st[job].converged) return;
   // The job's parameters are read once, before the first barrier: a barrier also orders the
@@ -359,11 +381,76 @@ __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__
     const int n = nl[lc];
     for (int k = threadIdx.x; k < n * n; k += blockDim.x) e_top[k] = E(lc)[k];
   }
+  __syncthreads();  // shared memory is free for the CTA's next job
 #undef E
 #undef F
 }
 
+__global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
+                                                         const JobState* __restrict__ st) {
+  extern __shared__ float sm[];
+  coarse_solve(job_list[blockIdx.x], jobs, st, sm);
+}
+
 // ---------------------------------------------------------------- mg_up
+// Up leg of one tile of level l >= 1: the bilinear prolongation of the coarser correction
+// added to the pre-smoothed one, nu_post sweeps, the result to eu[l].
+template <class G>
+__device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__ jobs, const JobState* __restrict__ st,
+                        int l, float* sm) {
+  const JobDev& J = jobs[tr.job];
+  if (st[tr.job].converged) return;
+  const int nf = J.nl[l];
+  const double hl = J.h * (double)(1 << l);
+  const float h2 = (float)(hl * hl);
+  const int nu = J.nu_post, H = 2 * nu;
+  const int i0 = tr.ti * kTU, j0 = tr.tj * kTU;
+  const int gx0 = i0 - H, gy0 = j0 - H;
+  const int W = kTU + 2 * H;
+  float* e = sm;
+  float* f = sm + W * W;
+  const float* eg = J.e[l];
+  const float* fg = J.f[l];
+  const int nc = J.nl[l + 1];
+  const float* ec = l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1];
+  const float omega = J.omega;
+  float* const eo = J.eu[l];
+  const int lane = g.rank() & 31, warp = g.rank() >> 5;
+#pragma unroll 2
+  for (int ly = warp; ly < W; ly += 8)
+    for (int lx = lane; lx < W; lx += 32) {
+      const int k = ly * W + lx;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      float ev = 0.f, fv = 0.f;
+      if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) {
+        const size_t gi = (size_t)gy * nf + gx;
+        ev = __ldg(eg + gi);
+        fv = __ldg(fg + gi);
+        const float* cp = ec + (size_t)(gy >> 1) * nc + (gx >> 1);
+        const bool io = gx & 1, jo = gy & 1;
+        const float c00 = __ldg(cp);
+        const float c10 = io ? __ldg(cp + 1) : 0.f;
+        const float c01 = jo ? __ldg(cp + nc) : 0.f;
+        const float c11 = (io && jo) ? __ldg(cp + nc + 1) : 0.f;
+        float v;
+        if (!io && !jo) v = c00;
+        else if (io && !jo) v = 0.5f * (c00 + c10);
+        else if (!io && jo) v = 0.5f * (c00 + c01);
+        else v = 0.25f * (c00 + c10 + c01 + c11);
+        ev += v;
+      }
+      e[k] = ev;
+      f[k] = fv;
+    }
+  g.sync();
+  if (nu > 0) tile_sweeps(g, e, f, W, gx0, gy0, nf, h2, omega, nu);
+  for (int oy = warp; oy < kTU; oy += 8) {
+    const int gy = j0 + oy, gx = i0 + lane;
+    if (gy < nf && gx < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+  }
+  g.sync();  // the tile's shared memory is free for the group's next tile
+}
+
 // mode 0: prolong + smooth, write e_l.  mode 1: level 0, prolong + smooth + FP64 update.
 // mode 2: level 0 update only (e_0 produced by the coarse kernel).
 __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
@@ -435,7 +522,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
     f[k] = fv;
   }
   __syncthreads();
-  if (nu > 0) tile_sweeps(e, f, W, gx0, gy0, nf, h2, omega, nu);
+  if (nu > 0) tile_sweeps(BlockGroup{}, e, f, W, gx0, gy0, nf, h2, omega, nu);
   if (mode == 0) {
     for (int oy = warp; oy < kTU; oy += 8) {
       const int gy = j0 + oy, gx = i0 + lane;
@@ -489,6 +576,61 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   }
 }
 
+// ---------------------------------------------------------------- levels 1 .. lc in one launch
+// Every level below the top, and the coarse solve, as phases of one cooperative launch of
+// 1024-thread CTAs (one per SM): each 256-thread quarter of a CTA processes tiles like one
+// CTA of mg_down_kernel / mg_up_kernel, a whole CTA does a job's coarse solve, and grid-wide
+// barriers separate the levels.  Replaces 2 (lc - 1) + 1 launches whose cost at these small
+// sizes is latency, not work.
+constexpr unsigned kGridPolls = 1u << 22;
+
+// Barrier k of a cooperative launch waits for the arrival counter (zeroed before the launch)
+// to reach (k + 1) * gridDim.x.  Bounded: after kGridPolls polls the CTA gives up.
+__device__ bool grid_barrier(unsigned* count, unsigned target) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    int ok = 1;
+    for (unsigned polls = 0; *(volatile unsigned*)count < target; ++polls) {
+      if (polls >= kGridPolls) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+__global__ void __launch_bounds__(1024, 1) mg_levels_kernel(const __grid_constant__ MgLevelsArgs a) {
+  extern __shared__ float sm[];
+  const QuarterGroup g{(int)(threadIdx.x >> 8)};
+  float* qsm = sm + g.q * a.quarter_floats;
+  const int slots = gridDim.x * 4, slot = blockIdx.x * 4 + g.q;
+  unsigned target = 0;
+  bool ok = true;
+  for (int l = 1; ok && l < a.max_depth; ++l) {
+    for (int t = slot; t < a.n_down[l]; t += slots) down_tile(g, a.down_tiles[l][t], a.jobs, a.st, l, qsm);
+    target += gridDim.x;
+    ok = grid_barrier(a.gbar, target);
+  }
+  if (ok)
+    for (int k = blockIdx.x; k < a.n_coarse; k += gridDim.x) coarse_solve(a.coarse_jobs[k], a.jobs, a.st, sm);
+  for (int l = a.max_depth - 1; ok && l >= 1; --l) {
+    target += gridDim.x;
+    ok = grid_barrier(a.gbar, target);
+    if (ok)
+      for (int t = slot; t < a.n_up[l]; t += slots) up_tile(g, a.up_tiles[l][t], a.jobs, a.st, l, qsm);
+  }
+  if (!ok && threadIdx.x == 0)
+    for (int k = 0; k < a.n_coarse; ++k) atomicOr(&a.st[a.coarse_jobs[k]].status, PIC_ST_TIMEOUT);
+}
+
 size_t down_smem(int nu) { const int W = 2 * kTC + 3 + 4 * nu; return (size_t)2 * W * W * sizeof(float); }
 size_t up_smem(int nu) { const int W = kTU + 4 * nu + 2; return (size_t)2 * W * W * sizeof(float); }
 
@@ -513,8 +655,60 @@ int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
 }
 
 
+int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coarse_smem, size_t* smem,
+                        size_t* quarter_floats) {
+  const size_t q = std::max(down_smem(nu_pre_max), up_smem(nu_post_max));
+  *quarter_floats = q / sizeof(float);
+  *smem = std::max(4 * q, coarse_smem);
+  int coop = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  if (!coop || *smem > 227 * 1024) return 0;
+  if (cudaFuncSetAttribute(mg_levels_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mg_levels_kernel, 1024, *smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return b >= 1 ? num_sms : 0;  // one CTA per SM
+}
+
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   int k = 0;
+  if (M.levels_grid > 0 && M.max_depth >= 2 && !M.n_cluster) {
+    if (M.n_down[0]) { mg_down_kernel<<<M.n_down[0], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[0], L.jobs, L.st, 0); ++k; }
+    MgLevelsArgs a{};
+    for (int l = 0; l < PIC_MAX_LEVELS; ++l) {
+      a.down_tiles[l] = M.down_tiles[l]; a.n_down[l] = M.n_down[l];
+      a.up_tiles[l] = M.up_tiles[l]; a.n_up[l] = M.n_up[l];
+    }
+    a.coarse_jobs = M.coarse_jobs; a.n_coarse = M.n_coarse;
+    a.max_depth = M.max_depth;
+    a.quarter_floats = M.levels_quarter_floats;
+    a.jobs = L.jobs; a.st = L.st; a.gbar = L.gbar;
+    cudaMemsetAsync(L.gbar, 0, sizeof(unsigned), s);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(M.levels_grid);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = M.levels_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, mg_levels_kernel, a);
+    ++k;
+    if (M.n_up[0]) {
+      mg_up_kernel<<<M.n_up[0], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[0], L.jobs, L.st, 0, 1, L.running);
+      ++k;
+    }
+    if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
+    return k;
+  }
   for (int l = 0; l < M.max_depth; ++l)
     if (M.n_down[l]) { mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l); ++k; }
   if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }

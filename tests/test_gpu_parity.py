@@ -112,6 +112,26 @@ def test_multigrid_cluster_coarse_solver_matches_oracle(orc, monkeypatch, n):
     assert rel_l2(dphi.cpu().numpy(), ref) < 1e-6
 
 
+@pytest.mark.parametrize("n", [257, 1025])
+def test_multigrid_levels_kernel_matches_oracle(orc, monkeypatch, n):
+    """Levels 1..lc as phases of one cooperative launch (PIC_MG_LEVELS_KERNEL=1) give the
+    oracle's V-cycles.  nu_coarse = 5 keys a solver instance of its own."""
+    import torch
+    from pic_cuda_b200.engine import solve_multigrid_f64
+    monkeypatch.setenv("PIC_MG_LEVELS_KERNEL", "1")
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(n + 2)
+    f = rng.standard_normal((n, n))
+    phi0 = np.zeros((n, n))
+    phi0[-1, :] = 0.75
+    dphi = torch.tensor(phi0, device="cuda")
+    drho = torch.tensor(f, device="cuda")
+    cyc, rel, ok = solve_multigrid_f64(dphi, drho, n, n, 0, h, 1.0, 2, 2, 5, tol=0.0, max_cycles=4)
+    assert cyc == 4 and not ok
+    ref = orc.mg_vcycles(phi0, f, h, 4, levels=0, omega=1.0, nu1=2, nu2=2, nuc=5)
+    assert rel_l2(dphi.cpu().numpy(), ref) < 1e-6
+
+
 def test_manufactured_solution_second_order_gpu(orc):
     import math
     import torch
