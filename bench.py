@@ -46,7 +46,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="mcc_mixed", choices=["plain_small", "mcc_mixed", "large"])
+    ap.add_argument("--workload", default="mcc_mixed", choices=["plain_small", "mcc_mixed", "large", "batched", "served"])
+    ap.add_argument("--jobs", type=int, default=None, help="batched: jobs; served: requests")
+    ap.add_argument("--ppc-scale", type=float, default=None, help="batched/served: particles-per-cell factor")
+    ap.add_argument("--steps-scale", type=float, default=None, help="served: request step-count factor")
+    ap.add_argument("--budget-gb", type=float, default=None, help="batched/served: HBM budget")
     ap.add_argument("--n-per-species", type=int, default=None)
     ap.add_argument("--deposit", choices=["f32", "i64"], default="f32")
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -386,10 +390,74 @@ def run_e2e(args, cfg, n, Te, Ti, Ld, steps_job, local, rank):
                     "pic_job_export_species (pinned host)"}
 
 
+def run_batched_bench(args):
+    """Batched mix in HBM-budgeted waves (one set of launches per step for a wave's jobs,
+    autotuned) against the same jobs one after another with the plain step."""
+    import torch
+    from pic_cuda_b200 import autotune, batch
+    n_jobs = args.jobs or 256
+    scale = args.ppc_scale if args.ppc_scale is not None else 0.02
+    specs = batch.batched_specs(n_jobs, seed=4, ppc_scale=scale, steps=300)
+    budget = int((args.budget_gb or 120.0) * 1e9)
+    torch.cuda.synchronize()
+    tuner = autotune.Tuner()
+    with ClockSampler(0) as clk:
+        b = batch.run_batched(specs, budget, tuner=tuner)
+        seq = batch.run_sequential(specs)
+    line = {"metric": METRIC, "value": b.rate, "unit": UNIT, "n_gpus": 1, "steps": 300, "warmup": 0,
+            "ms_per_step": 1000.0 * b.seconds / 300, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "mode": "batched",
+            "config": {"workload": "batched", "jobs": n_jobs, "ppc_scale": scale,
+                       "grids": "uniform over {65,129,257,513}^2", "ppc": "U[50,400] x ppc_scale per species",
+                       "waves": b.waves, "budget_gb": budget / 1e9, "tuned": tuner.chosen,
+                       "particle_steps": b.particle_steps},
+            "sequential": {"value": seq.rate, "seconds": seq.seconds, "particle_steps": seq.particle_steps},
+            "speedup_vs_sequential": b.rate / seq.rate if seq.rate > 0 else None,
+            "seconds": b.seconds, "wall_seconds": b.wall_seconds, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def run_served_bench(args):
+    """Poisson request stream through the continuous-batching server, against the same
+    stream served one job at a time (each job's measured alone time, replayed FIFO)."""
+    import torch
+    from pic_cuda_b200 import serve
+    from pic_cuda_b200.engine import Engine
+    n_req = args.jobs or 48
+    scale = args.ppc_scale if args.ppc_scale is not None else 0.05
+    sscale = args.steps_scale if args.steps_scale is not None else 0.1
+    reqs = serve.served_requests(n_req, seed=5, ppc_scale=scale, steps_scale=sscale)
+    budget = int((args.budget_gb or 150.0) * 1e9)
+    dev = torch.device("cuda", 0)
+    eng = Engine(0)
+    with ClockSampler(0) as clk:
+        out = serve.Server(engine=eng, budget_bytes=budget, quantum=20, device=dev).run(reqs)
+        eng.close()
+        durations = [serve.run_alone(r.spec)[0] for r in reqs]
+    seq = serve.fifo_replay(reqs, durations)
+    line = {"metric": METRIC, "value": out["rate"], "unit": UNIT, "n_gpus": 1, "steps": None, "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "mode": "served",
+            "config": {"workload": "served", "requests": n_req, "ppc_scale": scale, "steps_scale": sscale,
+                       "grids": "uniform over {129,257,513,1025}^2", "arrivals": "Poisson, 1.5x saturation",
+                       "budget_gb": budget / 1e9, "quantum_steps": 20},
+            "p50_s": out["p50"], "p99_s": out["p99"], "makespan_s": out["makespan"],
+            "server_seconds_in": out["seconds_in"],
+            "sequential": {"value": seq["rate"], "p50_s": seq["p50"], "p99_s": seq["p99"],
+                           "makespan_s": seq["makespan"]},
+            "speedup_vs_sequential": out["rate"] / seq["rate"] if seq["rate"] > 0 else None,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched_bench(args)
+    elif args.workload == "served":
+        run_served_bench(args)
     else:
         run_ours(args)
 

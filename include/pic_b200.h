@@ -208,6 +208,17 @@ int pic_engine_profile(pic_engine* e, int enable);
 int pic_engine_get_stats(pic_engine* e, pic_engine_stats* out, int reset);
 int pic_job_diagnostics(pic_engine* e, int job, pic_diagnostics* out);
 
+/* ---- tuning (no counterpart in the reference: the knobs the autotuner sets) ---- */
+/* PIC_OPT_MG_LEVELS_KERNEL: 1 = multigrid levels 1..lc as phases of one cooperative launch,
+ *   0 = one launch per level (default).  Takes effect at the next field solve.
+ * PIC_OPT_MG_CLUSTER_TOP: largest level side solved by a thread-block cluster (65 = none,
+ *   default); applies to jobs created after the call. */
+enum { PIC_OPT_MG_LEVELS_KERNEL = 1, PIC_OPT_MG_CLUSTER_TOP = 2 };
+int pic_engine_set_option(pic_engine* e, int option, int64_t value);
+int pic_engine_get_option(pic_engine* e, int option, int64_t* value);
+/* Counting-sort cadence of one job (0 = never), from its next step on. */
+int pic_job_set_sort_every(pic_engine* e, int job, int sort_every);
+
 /* ---- individual phases (parity checks, the compatibility layer) ---- */
 int pic_job_run_phases(pic_engine* e, int job, int phase_flags, int64_t step_index, void* stream);
 int pic_job_compact(pic_engine* e, int job, void* stream);

@@ -225,6 +225,9 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
 struct pic_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Job memory comes from a stream-ordered pool that keeps what jobs free for the next ones
+  // (admitting and retiring jobs while others run should not cost a device-wide cudaFree).
+  cudaMemPool_t pool = nullptr;
   int num_sms = 148;
   int mover_bps = 4;
   int cluster_C = 0;          // thread-block cluster size of the coarse solver (0: none)
@@ -233,6 +236,7 @@ struct pic_engine {
   // 16-CTA cluster from 513^2 down (V-cycle 0.20 -> 0.18 ms), so by default the cluster is
   // not used; PIC_MG_CLUSTER_TOP=<side> selects it for levels up to that side.
   int cluster_top = PIC_COARSE_MAX;
+  int levels_kernel = 0;      // multigrid levels 1..lc as one cooperative launch
   size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
   std::vector<JobHost> jobs;
@@ -298,10 +302,12 @@ int dev_alloc(pic_engine* E, JobHost& J, void** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (E->pool_bytes > 0 && E->used_bytes + (int64_t)bytes > E->pool_bytes)
     return fail(PIC_ERR_OOM, "engine memory budget exceeded");
-  const cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = cudaMallocFromPoolAsync(p, bytes, E->pool, E->stream);
+  // usable from any stream and by synchronous copies once the allocation has completed
+  if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return fail(PIC_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return fail(PIC_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
   }
   J.allocs.push_back(*p);
   J.bytes += (int64_t)bytes;
@@ -309,8 +315,12 @@ int dev_alloc(pic_engine* E, JobHost& J, void** p, size_t bytes) {
   return PIC_OK;
 }
 
+// Every stream may still use the job's memory: one device-wide wait, then the blocks go back
+// to the pool in stream order.
 void free_job(pic_engine* E, JobHost& J) {
-  for (void* p : J.allocs) cudaFree(p);
+  cudaDeviceSynchronize();
+  for (void* p : J.allocs) cudaFreeAsync(p, E->stream);
+  cudaStreamSynchronize(E->stream);
   J.allocs.clear();
   E->used_bytes -= J.bytes;
   J.bytes = 0;
@@ -389,12 +399,11 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   M.coarse_smem = coarse_smem;
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
-  // Levels 1..lc as phases of one cooperative launch (PIC_MG_LEVELS_KERNEL=1).  Measured on
+  // Levels 1..lc as phases of one cooperative launch (PIC_OPT_MG_LEVELS_KERNEL).  Measured on
   // B200 (1025^2 job, CUDA-graph step): 1.600 ms per step against 1.555 ms with one launch per
   // level, because at these sizes each phase waits on its slowest tile either way and the grid
   // barriers add to that; so it is off by default.
-  const char* lv = std::getenv("PIC_MG_LEVELS_KERNEL");
-  if (cluster.empty() && max_depth >= 2 && lv && std::atoi(lv) == 1)
+  if (cluster.empty() && max_depth >= 2 && E->levels_kernel)
     M.levels_grid = mg_levels_configure(E->num_sms, nu_pre_max, nu_post_max, coarse_smem, &M.levels_smem,
                                         &M.levels_quarter_floats);
   out.max_cycles = max_cycles;
@@ -703,9 +712,21 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
     if (mg_cluster_supported(16, s16) > 0) { E->cluster_C = 16; E->cluster_smem_max = s16; }
     else if (mg_cluster_supported(8, s8) > 0) { E->cluster_C = 8; E->cluster_smem_max = s8; }
     if (const char* v = std::getenv("PIC_MG_CLUSTER_TOP")) E->cluster_top = std::atoi(v);
+    if (const char* v = std::getenv("PIC_MG_LEVELS_KERNEL")) E->levels_kernel = std::atoi(v) == 1;
   }
   const int nslots = kMaxJobs * kSlotsPerJob;
   cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&E->pool, &props);
+    if (e == cudaSuccess) {
+      uint64_t keep = ~0ull;  // never trim: freed job memory stays for the next jobs
+      e = cudaMemPoolSetAttribute(E->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   if (e == cudaSuccess) e = cudaMalloc(&E->d_jobs, sizeof(JobDev) * kMaxJobs);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_st, sizeof(JobState) * kMaxJobs);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_slots, sizeof(SlotDev) * nslots);
@@ -763,6 +784,7 @@ int pic_engine_destroy(pic_engine* E) {
     for (auto& ev : E->phase_events[ph]) { cudaEventDestroy(ev.first); cudaEventDestroy(ev.second); }
   if (E->h_pinned) cudaFreeHost(E->h_pinned);
   if (E->stream) cudaStreamDestroy(E->stream);
+  if (E->pool) cudaMemPoolDestroy(E->pool);
   delete E;
   return PIC_OK;
 }
@@ -1373,6 +1395,49 @@ int pic_job_get_hits(pic_engine* E, int job, int species, int64_t capacity, int6
   std::vector<int32_t> h(k);
   if (k) CK(cudaMemcpy(h.data(), J.slot[species].hits, sizeof(int32_t) * k, cudaMemcpyDeviceToHost));
   for (int i = 0; i < k; ++i) idx[i] = h[i];
+  return PIC_OK;
+}
+
+// ---------------------------------------------------------------- tuning
+int pic_engine_set_option(pic_engine* E, int option, int64_t value) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  std::lock_guard<std::mutex> lk(E->mu);
+  if (option == PIC_OPT_MG_LEVELS_KERNEL) {
+    if (value != 0 && value != 1) return fail(PIC_ERR_ARG, "PIC_OPT_MG_LEVELS_KERNEL takes 0 or 1");
+    E->levels_kernel = (int)value;
+  } else if (option == PIC_OPT_MG_CLUSTER_TOP) {
+    if (value < 0 || value > 16385) return fail(PIC_ERR_ARG, "PIC_OPT_MG_CLUSTER_TOP out of range");
+    E->cluster_top = (int)value;
+  } else {
+    return fail(PIC_ERR_ARG, "unknown option");
+  }
+  // every multigrid plan (and the step graphs that replay them) is rebuilt on next use
+  E->mg_dirty = true;
+  E->graph_dirty = true;
+  for (auto& J : E->jobs) J.mg.valid = false;
+  return PIC_OK;
+}
+
+int pic_engine_get_option(pic_engine* E, int option, int64_t* value) {
+  if (!E || !value) return fail(PIC_ERR_ARG, "null argument");
+  if (option == PIC_OPT_MG_LEVELS_KERNEL) *value = E->levels_kernel;
+  else if (option == PIC_OPT_MG_CLUSTER_TOP) *value = E->cluster_top;
+  else return fail(PIC_ERR_ARG, "unknown option");
+  return PIC_OK;
+}
+
+int pic_job_set_sort_every(pic_engine* E, int job, int sort_every) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  if (sort_every < 0) return fail(PIC_ERR_ARG, "sort_every must be >= 0");
+  std::lock_guard<std::mutex> lk(E->mu);
+  CK(cudaSetDevice(E->device));
+  JobHost& J = E->jobs[job];
+  J.cfg.sort_every = sort_every;
+  J.dev.sort_every = sort_every;
+  CK(cudaMemcpyAsync(&E->d_jobs[job].sort_every, &J.dev.sort_every, sizeof(int), cudaMemcpyHostToDevice, E->stream));
+  CK(cudaStreamSynchronize(E->stream));
+  E->graph_dirty = true;
   return PIC_OK;
 }
 

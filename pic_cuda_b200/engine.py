@@ -112,6 +112,9 @@ class Job:
     def run_phases(self, flags: int, step: int = 0) -> None:
         L.check(L.lib().pic_job_run_phases(self.engine.h, self.id, flags, step, None), "pic_job_run_phases")
 
+    def set_sort_every(self, n: int) -> None:
+        L.check(L.lib().pic_job_set_sort_every(self.engine.h, self.id, n), "pic_job_set_sort_every")
+
     def compact(self) -> None:
         L.check(L.lib().pic_job_compact(self.engine.h, self.id, None), "pic_job_compact")
 
@@ -158,6 +161,14 @@ class Engine:
 
     def step_graph(self, n: int = 1, stream=None) -> None:
         L.check(L.lib().pic_step_graph(self.h, n, stream), "pic_step_graph")
+
+    def set_option(self, option: int, value: int) -> None:
+        L.check(L.lib().pic_engine_set_option(self.h, option, value), "pic_engine_set_option")
+
+    def get_option(self, option: int) -> int:
+        v = L.C.c_int64()
+        L.check(L.lib().pic_engine_get_option(self.h, option, L.C.byref(v)), "pic_engine_get_option")
+        return v.value
 
     def sync(self) -> None:
         L.check(L.lib().pic_sync(self.h), "pic_sync")
