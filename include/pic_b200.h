@@ -212,8 +212,10 @@ int pic_job_diagnostics(pic_engine* e, int job, pic_diagnostics* out);
 /* PIC_OPT_MG_LEVELS_KERNEL: 1 = multigrid levels 1..lc as phases of one cooperative launch,
  *   0 = one launch per level (default).  Takes effect at the next field solve.
  * PIC_OPT_MG_CLUSTER_TOP: largest level side solved by a thread-block cluster (65 = none,
- *   default); applies to jobs created after the call. */
-enum { PIC_OPT_MG_LEVELS_KERNEL = 1, PIC_OPT_MG_CLUSTER_TOP = 2 };
+ *   default); applies to jobs created after the call.
+ * PIC_OPT_MG_COARSE_TOP: largest level side (3..129) solved inside one CTA's shared memory
+ *   (65 = default); applies to jobs created after the call. */
+enum { PIC_OPT_MG_LEVELS_KERNEL = 1, PIC_OPT_MG_CLUSTER_TOP = 2, PIC_OPT_MG_COARSE_TOP = 3 };
 int pic_engine_set_option(pic_engine* e, int option, int64_t value);
 int pic_engine_get_option(pic_engine* e, int option, int64_t* value);
 /* Counting-sort cadence of one job (0 = never), from its next step on. */

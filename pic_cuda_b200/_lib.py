@@ -22,7 +22,7 @@ PROC_ELASTIC, PROC_EXCITATION, PROC_IONIZATION, PROC_CHARGE_EXCHANGE = 1, 2, 3, 
 PHASE_KICK, PHASE_MCC, PHASE_DRIFT, PHASE_WALLS, PHASE_DEPOSIT = 1, 2, 4, 8, 16
 GRID_RHO, GRID_PHI, GRID_EX, GRID_EY = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
-OPT_MG_LEVELS_KERNEL, OPT_MG_CLUSTER_TOP = 1, 2
+OPT_MG_LEVELS_KERNEL, OPT_MG_CLUSTER_TOP, OPT_MG_COARSE_TOP = 1, 2, 3
 
 
 class SpeciesConfig(C.Structure):

@@ -19,7 +19,7 @@
 #define PIC_CELL_OUT 0xFFFFFFFFu
 #define PIC_MAX_LEVELS 14
 #ifndef PIC_COARSE_MAX
-#define PIC_COARSE_MAX 65           // a first coarse level this small is solved by one CTA in smem
+#define PIC_COARSE_MAX 129          // largest level side the one-CTA coarse solver takes (smem)
 #endif
 #ifndef PIC_CHUNK
 #define PIC_CHUNK 512               // particles per mover work item (256 threads x 2)

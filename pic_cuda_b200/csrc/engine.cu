@@ -178,22 +178,24 @@ struct Layout {  // byte sizes of one job's device state
   int ntiles0;
   int64_t total;
 };
-// First level handled by the coarse solver (levels above it run as tile kernels):
-//  grids <= 65^2 entirely in one CTA (lc = 0); otherwise the first level that fits the
-//  coarse solver, never level 0 (the FP64 defect-correction update lives in the tile
-//  kernels): one CTA up to 65^2, a C-CTA cluster up to cluster_max.
-Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 0) {
+// First level handled by the coarse solver (levels above it run as tile kernels): grids up
+// to coarse_top (<= PIC_COARSE_MAX) entirely in one CTA (lc = 0, the FP64 update then runs
+// as its own tile launch); otherwise the first level that fits one CTA, or a C-CTA cluster
+// when cluster_top asks for one above coarse_top.
+Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 0, int coarse_top = PIC_COARSE_MAX) {
   Layout L{};
   L.levels = c.mg_levels > 0 ? c.mg_levels : auto_levels(c.nx);
-  int cluster_max = cluster_C >= 16 ? 513 : cluster_C >= 8 ? 257 : PIC_COARSE_MAX;
-  if (cluster_top > 0) cluster_max = std::min(cluster_max, std::max(cluster_top, PIC_COARSE_MAX));
+  const int one_cta = std::min(std::max(coarse_top, 3), PIC_COARSE_MAX);
+  int cluster_max = cluster_C >= 16 ? 513 : cluster_C >= 8 ? 257 : 0;
+  cluster_max = std::min(cluster_max, cluster_top);
+  const int top = std::max(one_cta, cluster_max);
   int n = c.nx;
   L.lc = -1;
   for (int l = 0; l < L.levels; ++l) {
     L.nl[l] = n;
     if (L.lc < 0) {
-      if (l == 0 && n <= PIC_COARSE_MAX) L.lc = 0;
-      else if (l > 0 && n <= cluster_max) L.lc = l;
+      if (l == 0 && n <= one_cta) L.lc = 0;
+      else if (l > 0 && n <= top) L.lc = l;
     }
     n = (n + 1) / 2;
   }
@@ -235,7 +237,12 @@ struct pic_engine {
   // tile kernels over all SMs for every level above 65^2 and one CTA below beat the
   // 16-CTA cluster from 513^2 down (V-cycle 0.20 -> 0.18 ms), so by default the cluster is
   // not used; PIC_MG_CLUSTER_TOP=<side> selects it for levels up to that side.
-  int cluster_top = PIC_COARSE_MAX;
+  int cluster_top = 65;
+  // Largest level side solved by the one-CTA coarse solver (jobs created after a change).
+  // Measured on B200 (1025^2 job, ncu): levels 129^2 .. 3^2 in one CTA take 49 us per
+  // V-cycle, bound by that one SM's shared-memory bandwidth (7 accesses per node and
+  // half-sweep), against about 16 us for 129^2 as two tile launches plus 65^2 .. 3^2 in one CTA.
+  int coarse_top = 65;
   int levels_kernel = 0;      // multigrid levels 1..lc as one cooperative launch
   size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
@@ -335,6 +342,7 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   std::vector<int> coarse, cluster;
   size_t cluster_smem = 0;
   int max_depth = 0, max_cycles = 1, nu_pre_max = 1, nu_post_max = 1;
+  int nu_pre_min = 1 << 30, nu_post_min = 1 << 30;
   size_t coarse_smem = 0;
   for (int id : ids) {
     const JobHost& J = E->jobs[id];
@@ -343,6 +351,8 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
     max_cycles = std::max(max_cycles, D.max_cycles);
     nu_pre_max = std::max(nu_pre_max, D.nu_pre);
     nu_post_max = std::max(nu_post_max, D.nu_post);
+    nu_pre_min = std::min(nu_pre_min, D.nu_pre);
+    nu_post_min = std::min(nu_post_min, D.nu_post);
     const int t0 = (D.nx + 31) / 32;
     for (int tj = 0; tj < t0; ++tj)
       for (int ti = 0; ti < t0; ++ti) init.push_back({id, ti, tj, tj * t0 + ti, t0 * t0, 0});
@@ -357,14 +367,12 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
       for (int tj = 0; tj < tu; ++tj)
         for (int ti = 0; ti < tu; ++ti) up[l].push_back({id, ti, tj, tj * tu + ti, tu * tu, 0});
     }
-    if (E->cluster_C > 0 && D.nl[D.lc] > PIC_COARSE_MAX) {
+    if (E->cluster_C > 0 && D.nl[D.lc] > PIC_COARSE_MAX) {   // above one CTA's shared memory
       cluster.push_back(id);
       cluster_smem = std::max(cluster_smem, mg_cluster_smem(D.nl, D.lc, D.levels, E->cluster_C));
     } else {
       coarse.push_back(id);
-      size_t b = 0;
-      for (int l = D.lc; l < D.levels; ++l) b += 2ull * D.nl[l] * D.nl[l] * sizeof(float);
-      coarse_smem = std::max(coarse_smem, b);
+      coarse_smem = std::max(coarse_smem, mg_coarse_smem(D.nl, D.lc, D.levels));
     }
   }
   std::vector<TileRef> all;
@@ -399,6 +407,8 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   M.coarse_smem = coarse_smem;
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
+  M.fast_nu_pre = (!ids.empty() && nu_pre_min == nu_pre_max) ? nu_pre_max : -1;
+  M.fast_nu_post = (!ids.empty() && nu_post_min == nu_post_max) ? nu_post_max : -1;
   // Levels 1..lc as phases of one cooperative launch (PIC_OPT_MG_LEVELS_KERNEL).  Measured on
   // B200 (1025^2 job, CUDA-graph step): 1.600 ms per step against 1.555 ms with one launch per
   // level, because at these sizes each phase waits on its slowest tile either way and the grid
@@ -712,6 +722,7 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
     if (mg_cluster_supported(16, s16) > 0) { E->cluster_C = 16; E->cluster_smem_max = s16; }
     else if (mg_cluster_supported(8, s8) > 0) { E->cluster_C = 8; E->cluster_smem_max = s8; }
     if (const char* v = std::getenv("PIC_MG_CLUSTER_TOP")) E->cluster_top = std::atoi(v);
+    if (const char* v = std::getenv("PIC_MG_COARSE_TOP")) E->coarse_top = std::atoi(v);
     if (const char* v = std::getenv("PIC_MG_LEVELS_KERNEL")) E->levels_kernel = std::atoi(v) == 1;
   }
   const int nslots = kMaxJobs * kSlotsPerJob;
@@ -816,7 +827,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   for (int j = 0; j < kMaxJobs; ++j)
     if (!E->jobs[j].alive) { id = j; break; }
   if (id < 0) return fail(PIC_ERR_CAPACITY, "engine job table full");
-  const Layout lay = job_layout(*cfg, E->cluster_C, E->cluster_top);
+  const Layout lay = job_layout(*cfg, E->cluster_C, E->cluster_top, E->coarse_top);
   if (E->pool_bytes > 0 && E->used_bytes + lay.total > E->pool_bytes) return fail(PIC_ERR_OOM, "engine memory budget exceeded");
   JobHost& J = E->jobs[id];
   J = JobHost();
@@ -1408,6 +1419,9 @@ int pic_engine_set_option(pic_engine* E, int option, int64_t value) {
   } else if (option == PIC_OPT_MG_CLUSTER_TOP) {
     if (value < 0 || value > 16385) return fail(PIC_ERR_ARG, "PIC_OPT_MG_CLUSTER_TOP out of range");
     E->cluster_top = (int)value;
+  } else if (option == PIC_OPT_MG_COARSE_TOP) {
+    if (value < 3 || value > PIC_COARSE_MAX) return fail(PIC_ERR_ARG, "PIC_OPT_MG_COARSE_TOP out of range (3..129)");
+    E->coarse_top = (int)value;
   } else {
     return fail(PIC_ERR_ARG, "unknown option");
   }
@@ -1422,6 +1436,7 @@ int pic_engine_get_option(pic_engine* E, int option, int64_t* value) {
   if (!E || !value) return fail(PIC_ERR_ARG, "null argument");
   if (option == PIC_OPT_MG_LEVELS_KERNEL) *value = E->levels_kernel;
   else if (option == PIC_OPT_MG_CLUSTER_TOP) *value = E->cluster_top;
+  else if (option == PIC_OPT_MG_COARSE_TOP) *value = E->coarse_top;
   else return fail(PIC_ERR_ARG, "unknown option");
   return PIC_OK;
 }

@@ -68,6 +68,7 @@ struct MgLaunch {
   int max_depth;                                         // max lc over jobs
   size_t coarse_smem;
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
+  int fast_nu_pre, fast_nu_post;                         // smoothing counts shared by every job, else -1
   int levels_grid;                                       // >0: levels 1..lc in one cooperative launch
   size_t levels_smem, levels_quarter_floats;
 };
@@ -88,6 +89,8 @@ int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coa
 int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s);
 void mg_configure_coarse(size_t smem_bytes);
+// Shared memory of the one-CTA coarse solver for levels lc .. levels-1.
+size_t mg_coarse_smem(const int* nl, int lc, int levels);
 size_t mg_cluster_smem(const int* nl, int lc, int levels, int C);
 int mg_cluster_supported(int C, size_t smem);
 int launch_mg_cluster(const int* job_list, int njobs, int C, size_t smem, const JobDev* jobs, const JobState* st,

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
+#include "tma.cuh"
 
 namespace {
 
@@ -271,27 +272,145 @@ __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict_
   down_tile(BlockGroup{}, tiles[blockIdx.x], jobs, st, l, sm);
 }
 
+// Bilinear prolongation weights (Multigrid.cu:378-404) without a branch per parity: the
+// absent neighbours enter as +0 and the scale is 1, 1/2 or 1/4, which reproduces
+// c00, (c00 + c10)/2, (c00 + c01)/2 and (c00 + c10 + c01 + c11)/4 exactly.
+__device__ __forceinline__ float prolong_value(const float* cp, int pitch, bool io, bool jo) {
+  const float c00 = cp[0];
+  const float c10 = io ? cp[1] : 0.f;
+  const float c01 = jo ? cp[pitch] : 0.f;
+  const float c11 = (io && jo) ? cp[pitch + 1] : 0.f;
+  const float sc = io ? (jo ? 0.25f : 0.5f) : (jo ? 0.5f : 1.f);
+  return sc * (c00 + c10 + c01 + c11);
+}
+
 // ---------------------------------------------------------------- mg_coarse
-__device__ void smem_sweeps(float* e, const float* f, int n, float h2, float omega, int nu) {
+// Levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.  Level l occupies
+// E then F, n_l rows of pitch n_l + 1 (even).  Every red-black half-sweep, restriction and
+// prolongation maps thread t to column i = 1 + t % (n-2) and walks the rows 1 + t / (n-2)
+// + k G (G = threads / (n-2) row groups), so the lanes of a warp touch consecutive columns:
+// with an even pitch the two colours of a column pair fall into distinct banks, and no
+// lane idles on the other colour.  Levels of side <= kWarpLevelMax run on warp 0 alone
+// (warp barriers instead of block barriers).
+constexpr int kWarpLevelMax = 17;
+
+template <bool WARP>
+__device__ __forceinline__ void group_sync() {
+  if (WARP) __syncwarp(); else __syncthreads();
+}
+
+// nu red-black SOR sweeps (colour (i+j) odd first, Multigrid.cu:246-265) on the interior of
+// an n x n level with row pitch P, by T threads (T >= n - 2).  ZERO: e enters as +0
+// everywhere (pre-smoothing), so the first half-sweep reads no neighbours.
+template <bool WARP, bool ZERO = false>
+__device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, float omega, int nu, int t, int T) {
+  const int m = n - 2;
+  const int G = m > 0 ? T / m : 0;
+  const int i = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  const bool on = g < G;
   const float om1 = 1.f - omega;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  for (int it = 0; it < nu; ++it) {
+  for (int it = 0; it < nu; ++it)
     for (int colour = 1; colour >= 0; --colour) {
-      for (int j = 1 + warp; j < n - 1; j += nwarp) {
-        const int i0 = 1 + ((colour - 1 - j) & 1);
-        for (int i = i0 + 2 * lane; i < n - 1; i += 64) {
-          const int c = j * n + i;
-          const float s = e[c + n] + e[c - n] + e[c + 1] + e[c - 1];
-          const float nv = 0.25f * (s - h2 * f[c]);
-          e[c] = fmaf(omega, nv, om1 * e[c]);
+      if (on) {
+        if (ZERO && it == 0 && colour == 1) {
+          for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
+            const float s = 0.f;
+            const float nv = 0.25f * (s - h2 * f[j * P + i]);
+            e[j * P + i] = fmaf(omega, nv, om1 * 0.f);
+          }
+        } else {
+          for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
+            float* p = e + j * P + i;
+            const float s = p[P] + p[-P] + p[1] + p[-1];
+            const float nv = 0.25f * (s - h2 * f[j * P + i]);
+            *p = fmaf(omega, nv, om1 * *p);
+          }
         }
       }
-      __syncthreads();
+      group_sync<WARP>();
+    }
+}
+
+// Residual of level (e, f, n) and its full weighting (Multigrid.cu:299-349) to the interior
+// of the next level's right-hand side fn (nc x nc, pitch Pc; its boundary stays 0).
+template <bool WARP>
+__device__ void level_restrict(const float* e, const float* f, int n, int P, float inv_h2, float* fn, int nc, int Pc,
+                               int t, int T) {
+  const int m = nc - 2;
+  const int G = m > 0 ? T / m : 0;
+  const int ic = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  if (g < G)
+    for (int jc = 1 + g; jc <= nc - 2; jc += G) {
+      float r[3][3];
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int q = (2 * jc + dy) * P + (2 * ic + dx);
+          const float lap = (e[q - P] + e[q + P] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
+          r[dy + 1][dx + 1] = f[q] - lap;
+        }
+      fn[jc * Pc + ic] = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] +
+                          r[0][2] + r[2][0] + r[2][2]) * 0.0625f;
+    }
+  group_sync<WARP>();
+}
+
+// Bilinear prolongation (Multigrid.cu:351-407) of the coarse correction c (nc x nc, pitch Pc)
+// added to the interior of e (n x n, pitch P).
+template <bool WARP>
+__device__ void level_prolong(float* e, int n, int P, const float* c, int Pc, int t, int T) {
+  const int m = n - 2;
+  const int G = m > 0 ? T / m : 0;
+  const int i = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  if (g < G)
+    for (int j = 1 + g; j <= n - 2; j += G) {
+      e[j * P + i] += prolong_value(c + (j >> 1) * Pc + (i >> 1), Pc, i & 1, j & 1);
+    }
+  group_sync<WARP>();
+}
+
+// Shared-memory bytes of levels lc .. levels-1 in the coarse solver's layout.
+__host__ __device__ inline size_t coarse_layout_bytes(const int* nl, int lc, int levels) {
+  size_t b = 0;
+  for (int l = lc; l < levels; ++l) b += 2ull * nl[l] * (nl[l] + 1) * sizeof(float);
+  return b;
+}
+
+// n*n values between global memory (pitch n) and a shared level (pitch n + 1), 1024 threads,
+// loads of a batch issued before any store.  Row = floor((k + 0.5) / n) in FP32 is exact while
+// n^2 < 2^21: k + 0.5 is representable, and the product's rounding error (< n 2^-22) stays
+// below the fraction's distance from an integer (>= 0.5 / n).
+constexpr int kCoarseBatch = 17;
+__device__ __forceinline__ void coarse_load(float* dst, const float* __restrict__ src, int n) {
+  const int N = n * n;
+  const float inv_n = 1.f / (float)n;
+  for (int k0 = 0; k0 < N; k0 += kCoarseBatch * 1024) {
+    float v[kCoarseBatch];
+#pragma unroll
+    for (int u = 0; u < kCoarseBatch; ++u) {
+      const int k = k0 + (int)threadIdx.x + u * 1024;
+      v[u] = k < N ? __ldg(src + k) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kCoarseBatch; ++u) {
+      const int k = k0 + (int)threadIdx.x + u * 1024;
+      if (k < N) {
+        const int j = (int)(((float)k + 0.5f) * inv_n);
+        dst[j * (n + 1) + (k - j * n)] = v[u];
+      }
     }
   }
 }
+__device__ __forceinline__ void coarse_store(float* __restrict__ dst, const float* src, int n) {
+  const int N = n * n;
+  const float inv_n = 1.f / (float)n;
+  for (int k = threadIdx.x; k < N; k += 1024) {
+    const int j = (int)(((float)k + 0.5f) * inv_n);
+    dst[k] = src[j * (n + 1) + (k - j * n)];
+  }
+}
 
-// The levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.
 __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, const JobState* __restrict__ st,
                              float* sm) {
   const JobDev& J = jobs[job];
@@ -304,86 +423,63 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   const int nu_pre = J.nu_pre, nu_post = J.nu_post, nu_coarse = J.nu_coarse;
   float* const e_top = J.e[lc];
   const float* const f_top = (lc == 0 && st[job].fsel) ? J.f0b : J.f[lc];
-  // level l occupies [off[l], off[l] + 2 n_l^2) of shared memory: E then F
-  __shared__ int off[PIC_MAX_LEVELS];
+  __shared__ int off[PIC_MAX_LEVELS + 1];
   __shared__ int nl[PIC_MAX_LEVELS];
   if (threadIdx.x < PIC_MAX_LEVELS) nl[threadIdx.x] = J.nl[threadIdx.x];
   if (threadIdx.x == 0) {
     int o = 0;
-    for (int k = lc; k < L; ++k) { off[k] = o; o += 2 * J.nl[k] * J.nl[k]; }
+    for (int k = lc; k < L; ++k) { off[k] = o; o += 2 * J.nl[k] * (J.nl[k] + 1); }
+    off[PIC_MAX_LEVELS] = o;
   }
   __syncthreads();
 #define E(l) (sm + off[l])
-#define F(l) (sm + off[l] + nl[l] * nl[l])
+#define F(l) (sm + off[l] + nl[l] * (nl[l] + 1))
+#define PT(l) (nl[l] + 1)
+#define H2(l) ((float)((h * (double)(1 << (l))) * (h * (double)(1 << (l)))))
+#define IH2(l) ((float)(1.0 / ((h * (double)(1 << (l))) * (h * (double)(1 << (l))))))
+  const int t = threadIdx.x;
+  // zero every level (corrections start at 0; coarse right-hand sides keep a zero boundary),
+  // except F(lc), which is loaded whole
   {
     const int n = nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) { F(lc)[k] = f_top[k]; E(lc)[k] = 0.f; }
+    const int f0 = off[lc] + n * (n + 1), f1 = off[lc] + 2 * n * (n + 1);
+    for (int k = t; k < off[PIC_MAX_LEVELS]; k += 1024)
+      if (k < f0 || k >= f1) sm[k] = 0.f;
+    coarse_load(F(lc), f_top, n);
   }
   __syncthreads();
-  for (int l = lc; l < L - 1; ++l) {
-    const int n = nl[l], nc = nl[l + 1];
-    const double hl = h * (double)(1 << l);
-    const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
-    smem_sweeps(E(l), F(l), n, h2, omega, nu_pre);
-    const float* e = E(l);
-    const float* f = F(l);
-    float* fn = F(l + 1);
-    float* en = E(l + 1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int jc = warp; jc < nc; jc += nwarp) {
-      for (int ic = lane; ic < nc; ic += 32) {
-        float v = 0.f;
-        if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
-          float r[3][3];
-#pragma unroll
-          for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll
-            for (int dx = -1; dx <= 1; ++dx) {
-              const int q = (2 * jc + dy) * n + (2 * ic + dx);
-              const float lap = (e[q - n] + e[q + n] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
-              r[dy + 1][dx + 1] = f[q] - lap;
-            }
-          v = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] + r[0][2] +
-               r[2][0] + r[2][2]) * 0.0625f;
-        }
-        fn[jc * nc + ic] = v;
-        en[jc * nc + ic] = 0.f;
+  int l = lc;
+  for (; l < L - 1 && nl[l] > kWarpLevelMax; ++l) {
+    level_sweeps<false, true>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_pre, t, 1024);
+    level_restrict<false>(E(l), F(l), nl[l], PT(l), IH2(l), F(l + 1), nl[l + 1], PT(l + 1), t, 1024);
+  }
+  if (nl[l] > kWarpLevelMax) {  // a large coarsest level (l == L - 1)
+    level_sweeps<false>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_coarse, t, 1024);
+  } else {
+    if (t < 32) {
+      for (int k = l; k < L - 1; ++k) {
+        level_sweeps<true, true>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_pre, t, 32);
+        level_restrict<true>(E(k), F(k), nl[k], PT(k), IH2(k), F(k + 1), nl[k + 1], PT(k + 1), t, 32);
+      }
+      level_sweeps<true>(E(L - 1), F(L - 1), nl[L - 1], PT(L - 1), H2(L - 1), omega, nu_coarse, t, 32);
+      for (int k = L - 2; k >= l; --k) {
+        level_prolong<true>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, 32);
+        level_sweeps<true>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, 32);
       }
     }
     __syncthreads();
   }
-  {
-    const double hl = h * (double)(1 << (L - 1));
-    smem_sweeps(E(L - 1), F(L - 1), nl[L - 1], (float)(hl * hl), omega, nu_coarse);
+  for (int k = l - 1; k >= lc; --k) {
+    level_prolong<false>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, 1024);
+    level_sweeps<false>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, 1024);
   }
-  for (int l = L - 2; l >= lc; --l) {
-    const int n = nl[l], nc = nl[l + 1];
-    const float* c = E(l + 1);
-    float* el = E(l);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int j = 1 + warp; j < n - 1; j += nwarp) {   // boundary nodes receive 0 (coarse boundary is 0)
-      for (int i = 1 + lane; i < n - 1; i += 32) {
-        const int ic = i >> 1, jc = j >> 1;
-        const float* cp = c + jc * nc + ic;
-        float v;
-        if (!(i & 1) && !(j & 1)) v = cp[0];
-        else if ((i & 1) && !(j & 1)) v = 0.5f * (cp[0] + cp[1]);
-        else if (!(i & 1) && (j & 1)) v = 0.5f * (cp[0] + cp[nc]);
-        else v = 0.25f * (cp[0] + cp[1] + cp[nc] + cp[nc + 1]);
-        el[j * n + i] += v;
-      }
-    }
-    __syncthreads();
-    const double hl = h * (double)(1 << l);
-    smem_sweeps(E(l), F(l), n, (float)(hl * hl), omega, nu_post);
-  }
-  {
-    const int n = nl[lc];
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) e_top[k] = E(lc)[k];
-  }
+  coarse_store(e_top, E(lc), nl[lc]);
   __syncthreads();  // shared memory is free for the CTA's next job
 #undef E
 #undef F
+#undef PT
+#undef H2
+#undef IH2
 }
 
 __global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
@@ -576,6 +672,338 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   }
 }
 
+// ---------------------------------------------------------------- tile kernels, compile-time shapes
+// The per-level launches of the V-cycle for a uniform smoothing count NU (0..4): the tile
+// width W is a compile-time constant, so every global input of a tile is requested in one
+// unrolled batch of asynchronous copies (one memory latency per tile instead of one per row),
+// and the sweeps use the column-per-thread red-black mapping of the coarse solver on an even
+// row pitch P (conflict-free, every lane on a node of the current colour).  NT threads per
+// CTA: 256 where a level has enough tiles to fill the GPU, 1024 on small levels, where a
+// tile's latency chain (not the SM's issue rate) sets the time.  Results equal those of
+// mg_down_kernel / mg_up_kernel: the same expressions in the same order at every node.
+constexpr int kMaxFastNu = 4;
+
+// NU red-black SOR sweeps on a W x W tile.  ZERO: the correction enters as 0 (pre-smoothing
+// from a zero guess), so the first half-sweep reads no neighbours (they are all +0).
+template <int W, int P, int NU, int NT, bool ZERO>
+__device__ __forceinline__ void tile_sweeps_cols(float* e, const float* f, int gx0, int gy0, int n, float h2,
+                                                 float omega) {
+  constexpr int kGmin = NT / (W - 2);                           // row groups of an interior tile
+  constexpr int kRows = ((W - 1) / 2 + kGmin - 1) / kGmin;      // rows of one colour per thread, at most
+  const int t = threadIdx.x;
+  const int lx_lo = max(1, 1 - gx0), lx_hi = min(W - 2, n - 2 - gx0);
+  const int ly_lo = max(1, 1 - gy0), ly_hi = min(W - 2, n - 2 - gy0);
+  const int m = lx_hi - lx_lo + 1;
+  const int G = m > 0 ? NT / m : 0;
+  const int lx = lx_lo + (m > 0 ? t % m : 0), g = m > 0 ? t / m : NT;
+  const bool on = g < G && ly_hi >= ly_lo;
+  const int par = gx0 + gy0 + lx;  // node (lx, ly) has colour (par + ly) & 1
+  const float om1 = 1.f - omega;
+#pragma unroll
+  for (int it = 0; it < NU; ++it)
+#pragma unroll
+    for (int colour = 1; colour >= 0; --colour) {
+      if (on) {
+        const int ly0 = ly_lo + ((colour - par - ly_lo) & 1) + 2 * g;
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          const int ly = ly0 + 2 * G * r;
+          if (ly <= ly_hi) {
+            float* p = e + ly * P + lx;
+            if (ZERO && it == 0 && colour == 1) {
+              const float s = 0.f;
+              const float nv = 0.25f * (s - h2 * f[ly * P + lx]);
+              *p = fmaf(omega, nv, om1 * 0.f);
+            } else {
+              const float s = p[P] + p[-P] + p[1] + p[-1];
+              const float nv = 0.25f * (s - h2 * f[ly * P + lx]);
+              *p = fmaf(omega, nv, om1 * *p);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+// Down leg of level l (as mg_down_kernel): NU pre-sweeps from a zero correction on the tile
+// of 16 x 16 coarse nodes, the smoothed fine nodes it owns to e_l, the full-weighted
+// residual to f_{l+1}.
+template <int NU, int NT>
+__global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restrict__ tiles,
+                                                          const JobDev* __restrict__ jobs,
+                                                          const JobState* __restrict__ st, int l) {
+  constexpr int H = 2 * NU, W = 2 * kTC + 3 + 2 * H, P = W + 1;
+  constexpr int NL = (W * W + NT - 1) / NT;
+  __shared__ __align__(16) float e[W * P];
+  __shared__ __align__(16) float f[W * P];
+  const TileRef tr = tiles[blockIdx.x];
+  const JobDev& J = jobs[tr.job];
+  const JobState& T = st[tr.job];
+  if (T.converged) return;
+  const int nf = J.nl[l], nc = J.nl[l + 1];
+  const double hl = J.h * (double)(1 << l);
+  const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
+  const int ic0 = tr.ti * kTC, jc0 = tr.tj * kTC;
+  const int gx0 = 2 * ic0 - 2 - H, gy0 = 2 * jc0 - 2 - H;
+  const float* __restrict__ fg = (l == 0 && T.fsel) ? J.f0b : J.f[l];
+  float* const eg = J.e[l];
+  float* const fc = J.f[l + 1];
+  const float omega = J.omega;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < NL; ++u) {
+    const int q = t + u * NT;
+    if (q < W * W) {
+      const int ly = q / W, lx = q - ly * W;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      const bool in = (unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf;
+      tma::cp_async4(f + ly * P + lx, fg + (in ? gy * nf + gx : 0), in);
+      e[ly * P + lx] = 0.f;
+    }
+  }
+  tma::cp_async_wait_all();
+  __syncthreads();
+  tile_sweeps_cols<W, P, NU, NT, true>(e, f, gx0, gy0, nf, h2, omega);
+  // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
+#pragma unroll
+  for (int u = 0; u < (4 * kTC * kTC) / NT; ++u) {
+    const int k = t + u * NT;
+    const int gy = 2 * jc0 + (k >> 5), gx = 2 * ic0 + (k & 31);
+    if (gy < nf && gx < nf) eg[gy * nf + gx] = e[(gy - gy0) * P + (gx - gx0)];
+  }
+  // residual + full weighting to the owned coarse nodes
+  if (t < kTC * kTC) {
+    const int ic = ic0 + (t & (kTC - 1)), jc = jc0 + t / kTC;
+    if (ic < nc && jc < nc) {
+      float vv = 0.f;
+      if (ic > 0 && ic < nc - 1 && jc > 0 && jc < nc - 1) {
+        const int cx = 2 * ic - gx0, cy = 2 * jc - gy0;
+        float r[3][3];
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int q = (cy + dy) * P + (cx + dx);
+            const float lap = (e[q - P] + e[q + P] + e[q - 1] + e[q + 1] - 4.f * e[q]) * inv_h2;
+            r[dy + 1][dx + 1] = f[q] - lap;
+          }
+        const float sum = 4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] +
+                          r[0][2] + r[2][0] + r[2][2];
+        vv = sum * 0.0625f;
+      }
+      fc[jc * nc + ic] = vv;
+    }
+  }
+}
+
+// Up leg (as mg_up_kernel modes 0 and 1).  MODE 0, level l >= 1: the bilinear prolongation
+// of the coarser correction added to the pre-smoothed one, NU post-sweeps, the owned nodes
+// to eu_l.  MODE 1, level 0 (NT = 256): the same with a one-node halo, then phi <- phi + e in
+// FP64, the new FP64 defect, phi32 and the deterministic norm.  Every global input of the
+// tile (e, f, the coarse tile, and on level 0 phi64 and rho) is requested in one batch.
+template <int NU, int MODE, int NT>
+__global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const TileRef* __restrict__ tiles,
+                                                                      const JobDev* __restrict__ jobs,
+                                                                      JobState* __restrict__ st, int l, int* running) {
+  constexpr int H = 2 * NU, X = MODE, W = kTU + 2 * H + 2 * X, P = W;
+  constexpr int CW = W / 2 + 2, CP = CW + (CW & 1);
+  constexpr int PW = kTU + 2;
+  constexpr int NL = (W * W + NT - 1) / NT;
+  constexpr int NC = (CW * CW + NT - 1) / NT;
+  constexpr int NP = MODE ? (PW * PW + NT - 1) / NT : 0;
+  constexpr int NO = kTU * kTU / NT;
+  __shared__ __align__(16) float e[W * P];
+  __shared__ __align__(16) float f[W * P];
+  __shared__ __align__(16) float cs[CW * CP];
+  __shared__ __align__(16) double P64[MODE ? PW * PW : 1];
+  __shared__ __align__(16) double RH[MODE ? kTU * kTU : 1];   // rho of the owned nodes, raw
+  const TileRef tr = tiles[blockIdx.x];
+  const JobDev& J = jobs[tr.job];
+  JobState& T = st[tr.job];
+  if (T.converged) return;
+  const int nf = J.nl[l];
+  const double hl = J.h * (double)(1 << l);
+  const float h2 = (float)(hl * hl);
+  const int i0 = tr.ti * kTU, j0 = tr.tj * kTU;
+  const int gx0 = i0 - H - X, gy0 = j0 - H - X;
+  const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;   // floor, also for negative origins
+  const int fsel = T.fsel;
+  const float* __restrict__ eg = J.e[l];
+  const float* __restrict__ fg = (l == 0 && fsel) ? J.f0b : J.f[l];
+  const int nc = J.nl[l + 1];
+  const float* __restrict__ ec = l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1];
+  const float omega = J.omega;
+  float* const eo = J.eu[l];
+  const int cur = T.phi_cur, nxt = T.phi_nxt;
+  const double* __restrict__ pc = J.phi64[cur];
+  double* const pn = J.phi64[nxt];
+  const double inv_h2 = 1.0 / (J.h * J.h);
+  const double rhs_scale = J.rhs_scale;
+  const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
+  float* const phi32 = J.phi32;
+  float* const f0 = fsel ? J.f[0] : J.f0b;   // the new defect goes to the other buffer
+  double* const partials = J.partials;
+  const double tol = J.tol;
+  const int max_cycles = J.max_cycles;
+  const int t = threadIdx.x;
+  // ---- one batch of asynchronous copies
+#pragma unroll
+  for (int u = 0; u < NL; ++u) {
+    const int q = t + u * NT;
+    if (q < W * W) {
+      const int ly = q / W, lx = q - ly * W;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      const bool in = (unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf;
+      const int gi = in ? gy * nf + gx : 0;
+      tma::cp_async4(e + ly * P + lx, eg + gi, in);
+      tma::cp_async4(f + ly * P + lx, fg + gi, in);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NC; ++u) {
+    const int q = t + u * NT;
+    if (q < CW * CW) {
+      const int cy = q / CW, cx = q - cy * CW;
+      const int gx = cx0 + cx, gy = cy0 + cy;
+      const bool in = (unsigned)gx < (unsigned)nc && (unsigned)gy < (unsigned)nc;
+      tma::cp_async4(cs + cy * CP + cx, ec + (in ? gy * nc + gx : 0), in);
+    }
+  }
+  if constexpr (MODE == 1) {
+#pragma unroll
+    for (int u = 0; u < NP; ++u) {
+      const int k = t + u * NT;
+      if (k < PW * PW) {
+        const int py = k / PW, px = k - py * PW;
+        const int gx = i0 - 1 + px, gy = j0 - 1 + py;
+        const bool in = (unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf;
+        tma::cp_async8(P64 + k, pc + (in ? gy * nf + gx : 0), in);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < NO; ++u) {
+      const int k = t + u * NT;
+      const int gx = i0 + (k & 31), gy = j0 + (k >> 5);
+      const bool in = gx < nf && gy < nf;
+      const int g = in ? gy * nf + gx : 0;
+      if (rho.mode == 0) tma::cp_async4(reinterpret_cast<float*>(RH) + k, rho.f + g, in);
+      else if (rho.mode == 1) tma::cp_async8(RH + k, rho.i + g, in);
+      else tma::cp_async8(RH + k, rho.d + g, in);
+    }
+  }
+  tma::cp_async_wait_all();
+  __syncthreads();
+  // ---- bilinear prolongation added to the pre-smoothed correction
+#pragma unroll
+  for (int u = 0; u < NL; ++u) {
+    const int q = t + u * NT;
+    if (q < W * W) {
+      const int ly = q / W, lx = q - ly * W;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      if ((unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf) {
+        const float* cp = cs + ((gy >> 1) - cy0) * CP + ((gx >> 1) - cx0);
+        e[ly * P + lx] += prolong_value(cp, CP, gx & 1, gy & 1);
+      }
+    }
+  }
+  __syncthreads();
+  tile_sweeps_cols<W, P, NU, NT, false>(e, f, gx0, gy0, nf, h2, omega);
+  if constexpr (MODE == 0) {
+#pragma unroll
+    for (int u = 0; u < NO; ++u) {
+      const int k = t + u * NT;
+      const int gx = i0 + (k & 31), gy = j0 + (k >> 5);
+      if (gy < nf && gx < nf) eo[gy * nf + gx] = e[(gy - gy0) * P + (gx - gx0)];
+    }
+    return;
+  } else {
+    // ---- level-0 FP64 update and new residual
+#pragma unroll
+    for (int u = 0; u < NP; ++u) {
+      const int k = t + u * NT;
+      if (k < PW * PW) {
+        const int py = k / PW, px = k - py * PW;
+        const int gx = i0 - 1 + px, gy = j0 - 1 + py;
+        if ((unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf)
+          P64[k] += (double)e[(gy - gy0) * P + (gx - gx0)];
+      }
+    }
+    __syncthreads();
+    double ar = 0.0;
+#pragma unroll
+    for (int u = 0; u < NO; ++u) {
+      const int k = t + u * NT;
+      const int ox = k & 31, oy = k >> 5;
+      const int gx = i0 + ox, gy = j0 + oy;
+      if (gx >= nf || gy >= nf) continue;
+      const int g = gy * nf + gx;
+      const int q = (oy + 1) * PW + (ox + 1);
+      const double rv = rho.mode == 0 ? (double)reinterpret_cast<const float*>(RH)[k]
+                        : rho.mode == 1 ? (double)reinterpret_cast<const long long*>(RH)[k] * 0x1p-40 : RH[k];
+      const double F = rhs_scale * rv;
+      double r = 0.0;
+      if (gx > 0 && gx < nf - 1 && gy > 0 && gy < nf - 1) {
+        const double lap = (P64[q - PW] + P64[q + PW] + P64[q - 1] + P64[q + 1] - 4.0 * P64[q]) * inv_h2;
+        r = F - lap;
+      }
+      pn[g] = P64[q];
+      phi32[g] = (float)P64[q];
+      f0[g] = (float)r;
+      ar += r * r;
+    }
+    const double sr = block_sum(ar);
+    if (t == 0) partials[2 * (tr.pbase + tr.local)] = sr;
+    if (last_of_job(T, tr.nlocal)) {
+      __threadfence();
+      const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
+      if (t != 0) return;
+      T.rnorm2 = r2;
+      T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
+      T.cycles += 1;
+      T.phi_cur = nxt;
+      T.phi_nxt = cur;
+      T.fsel = fsel ^ 1;
+      if (T.relres < tol) { T.converged = 1; atomicSub(running, 1); }
+      else if (T.cycles >= max_cycles) { T.converged = 2; atomicSub(running, 1); }
+    }
+  }
+}
+
+template <int NU>
+void launch_down_fast(int grid, bool wide, const TileRef* tiles, const JobDev* jobs, const JobState* st, int l,
+                      cudaStream_t s) {
+  if (wide) mg_down_fast_kernel<NU, 1024><<<grid, 1024, 0, s>>>(tiles, jobs, st, l);
+  else mg_down_fast_kernel<NU, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l);
+}
+template <int NU>
+void launch_up_fast(int grid, bool wide, const TileRef* tiles, const JobDev* jobs, JobState* st, int l, int mode,
+                    int* running, cudaStream_t s) {
+  if (mode == 1) mg_up_fast_kernel<NU, 1, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l, running);
+  else if (wide) mg_up_fast_kernel<NU, 0, 1024><<<grid, 1024, 0, s>>>(tiles, jobs, st, l, running);
+  else mg_up_fast_kernel<NU, 0, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l, running);
+}
+void down_fast(int nu, int grid, bool wide, const TileRef* tiles, const JobDev* jobs, const JobState* st, int l,
+               cudaStream_t s) {
+  switch (nu) {
+    case 0: launch_down_fast<0>(grid, wide, tiles, jobs, st, l, s); break;
+    case 1: launch_down_fast<1>(grid, wide, tiles, jobs, st, l, s); break;
+    case 2: launch_down_fast<2>(grid, wide, tiles, jobs, st, l, s); break;
+    case 3: launch_down_fast<3>(grid, wide, tiles, jobs, st, l, s); break;
+    default: launch_down_fast<4>(grid, wide, tiles, jobs, st, l, s); break;
+  }
+}
+void up_fast(int nu, int grid, bool wide, const TileRef* tiles, const JobDev* jobs, JobState* st, int l, int mode,
+             int* running, cudaStream_t s) {
+  switch (nu) {
+    case 0: launch_up_fast<0>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+    case 1: launch_up_fast<1>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+    case 2: launch_up_fast<2>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+    case 3: launch_up_fast<3>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+    default: launch_up_fast<4>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+  }
+}
+
 // ---------------------------------------------------------------- levels 1 .. lc in one launch
 // Every level below the top, and the coarse solve, as phases of one cooperative launch of
 // 1024-thread CTAs (one per SM): each 256-thread quarter of a CTA processes tiles like one
@@ -636,6 +1064,8 @@ size_t up_smem(int nu) { const int W = kTU + 4 * nu + 2; return (size_t)2 * W * 
 
 }  // namespace
 
+size_t mg_coarse_smem(const int* nl, int lc, int levels) { return coarse_layout_bytes(nl, lc, levels); }
+
 void mg_configure_coarse(size_t smem_bytes) {
   // the attribute only grows, so every launch list built so far stays launchable
   static size_t configured = 0;
@@ -676,10 +1106,28 @@ int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coa
   return b >= 1 ? num_sms : 0;  // one CTA per SM
 }
 
+// Tile launches of one level: the compile-time-shape kernels when every job of the launch
+// has the same smoothing count (<= kMaxFastNu), else the generic ones.
+// 1024-thread CTAs where a level has at most two tiles per SM.
+static void launch_down(const MgLaunch& M, int l, const EngineLaunch& L, cudaStream_t s) {
+  if (M.fast_nu_pre >= 0 && M.fast_nu_pre <= kMaxFastNu)
+    down_fast(M.fast_nu_pre, M.n_down[l], M.n_down[l] <= 2 * L.num_sms, M.down_tiles[l], L.jobs, L.st, l, s);
+  else
+    mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l);
+}
+static void launch_up(const MgLaunch& M, int l, const EngineLaunch& L, cudaStream_t s) {
+  if (M.fast_nu_post >= 0 && M.fast_nu_post <= kMaxFastNu)
+    up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= 2 * L.num_sms, M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
+            L.running, s);
+  else
+    mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
+                                                                L.running);
+}
+
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   int k = 0;
   if (M.levels_grid > 0 && M.max_depth >= 2 && !M.n_cluster) {
-    if (M.n_down[0]) { mg_down_kernel<<<M.n_down[0], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[0], L.jobs, L.st, 0); ++k; }
+    if (M.n_down[0]) { launch_down(M, 0, L, s); ++k; }
     MgLevelsArgs a{};
     for (int l = 0; l < PIC_MAX_LEVELS; ++l) {
       a.down_tiles[l] = M.down_tiles[l]; a.n_down[l] = M.n_down[l];
@@ -702,22 +1150,16 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, mg_levels_kernel, a);
     ++k;
-    if (M.n_up[0]) {
-      mg_up_kernel<<<M.n_up[0], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[0], L.jobs, L.st, 0, 1, L.running);
-      ++k;
-    }
+    if (M.n_up[0]) { launch_up(M, 0, L, s); ++k; }
     if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
     return k;
   }
   for (int l = 0; l < M.max_depth; ++l)
-    if (M.n_down[l]) { mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l); ++k; }
+    if (M.n_down[l]) { launch_down(M, l, L, s); ++k; }
   if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
   if (M.n_cluster) k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s);
   for (int l = M.max_depth - 1; l >= 0; --l)
-    if (M.n_up[l]) {
-      mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0, L.running);
-      ++k;
-    }
+    if (M.n_up[l]) { launch_up(M, l, L, s); ++k; }
   if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
   return k;
 }

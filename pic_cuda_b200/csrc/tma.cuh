@@ -1,5 +1,5 @@
 // tma.cuh — bulk asynchronous copies (cp.async.bulk, the 1-D form of the Tensor Memory
-// Accelerator) and mbarrier helpers, written as inline PTX for sm_100a.
+// Accelerator), per-thread cp.async copies and mbarrier helpers, inline PTX for sm_100a.
 // No multicast form is used anywhere.  Every wait is bounded: after kMaxPolls unsuccessful
 // polls it gives up and reports false, so a kernel can flag PIC_ST_TIMEOUT and leave.
 #pragma once
@@ -65,5 +65,22 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Make this thread's generic-proxy shared-memory writes visible to the async proxy.
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Per-thread asynchronous global -> shared copy of 4 or 8 bytes (cp.async): nothing is held
+// in registers while the copy is in flight.  valid = false reads no global memory and writes
+// zeros (src must still be a valid address: callers pass the array base).
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+// Wait for every cp.async this thread issued (a block barrier must follow before other
+// threads read the data).
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
 
 }  // namespace tma
