@@ -112,7 +112,6 @@ __global__ void grid_import_kernel(const JobDev* __restrict__ jd, const JobState
       else J.rho_i[k] = __double2ll_rn(v * 0x1p40);
     } else {
       J.phi64[st->phi_cur][k] = in[k];
-      J.phi32[k] = (float)in[k];
     }
   }
 }

@@ -202,7 +202,7 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   if (L.lc < 0) L.lc = L.levels - 1;
   L.ntiles0 = ((c.nx + 31) / 32) * ((c.ny + 31) / 32);
   const int64_t N = (int64_t)c.nx * c.ny;
-  int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 4 + 16 + (c.mg_warm_start ? 8 : 0));
+  int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 8 + 16 + (c.mg_warm_start ? 8 : 0));
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
   for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
   b += 4 * N;                                                         // second level-0 rhs
@@ -868,7 +868,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     if (r_) { free_job(E, J); return r_; }                 \
   } while (0)
   if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, N * 4); else ALLOC(D.rho_i, N * 8);
-  ALLOC(D.phi32, N * 4);
+  ALLOC(D.efield, N * 8);
   ALLOC(D.phi64[0], N * 8);
   ALLOC(D.phi64[1], N * 8);
   if (c.mg_warm_start) ALLOC(D.phi64[2], N * 8);
@@ -980,7 +980,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   CK(cudaMemset(D.phi64[0], 0, N * 8));
   CK(cudaMemset(D.phi64[1], 0, N * 8));
   if (D.phi64[2]) CK(cudaMemset(D.phi64[2], 0, N * 8));
-  CK(cudaMemset(D.phi32, 0, N * 4));
+  CK(cudaMemset(D.efield, 0, N * 8));
   if (D.rho_f) CK(cudaMemset(D.rho_f, 0, N * 4));
   if (D.rho_i) CK(cudaMemset(D.rho_i, 0, N * 8));
   for (int l = 0; l < lay.levels; ++l) {

@@ -1,8 +1,9 @@
 // mover.cu — the fused particle pass of one PIC step.
 //
 // One pass over each particle slot does, in the reference's order (main.cu:64-134):
-//   kick     updateParticleVelocities (kernels.cu:71-131) with E = -grad(phi) taken on the
-//            fly from phi32 through the computeElectricField stencils (kernels.cu:134-191)
+//   kick     updateParticleVelocities (kernels.cu:71-131): E bilinearly gathered from the
+//            node field that efield32_kernel computes once per step from the FP64 potential
+//            with the computeElectricField stencils (kernels.cu:134-191)
 //   MCC      null-collision Monte Carlo (or the reference's elastic form, mcc.cu:56-85)
 //   drift    update_coordinates (kernels.cu:8-23) on cell-relative FP32 positions
 //   walls    detect_intersections (collisions.cu:7-54) / box absorption; hits are appended
@@ -12,43 +13,13 @@
 //            then one atomic per node per segment; FP32 or int64 fixed point.
 // The kick + MCC of step k are fused into the pass of step k+1 (the job's kick_pending
 // flag); an explicit flush applies them before any read-back.
+#include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
 #include "particle_ops.cuh"
 #include "tma.cuh"
 
 namespace {
-
-struct PhiGather {
-  const float* phi;
-  int nx, ny;
-};
-
-// E at the four nodes of cell (i,j), interpolated at (fx,fy), returned as the phi
-// difference per unit cell (so dv = k * this).  Edge nodes use one-sided differences,
-// interior nodes central ones, like computeElectricField.
-__device__ __forceinline__ void gather_dphi(const PhiGather& g, int i, int j, float fx, float fy,
-                                            float& gx, float& gy) {
-  const int nx = g.nx;
-  const float* r0 = g.phi + (size_t)j * nx;
-  const float* r1 = r0 + nx;
-  const int xl = i > 0 ? i - 1 : 0, xr = (i + 2 < nx) ? i + 2 : nx - 1;
-  const float sx0 = i > 0 ? 0.5f : 1.0f, sx1 = (i + 2 < nx) ? 0.5f : 1.0f;
-  const float a_l = __ldg(r0 + xl), a_0 = __ldg(r0 + i), a_1 = __ldg(r0 + i + 1), a_r = __ldg(r0 + xr);
-  const float b_l = __ldg(r1 + xl), b_0 = __ldg(r1 + i), b_1 = __ldg(r1 + i + 1), b_r = __ldg(r1 + xr);
-  const int yl = j > 0 ? j - 1 : 0, yr = (j + 2 < g.ny) ? j + 2 : g.ny - 1;
-  const float sy0 = j > 0 ? 0.5f : 1.0f, sy1 = (j + 2 < g.ny) ? 0.5f : 1.0f;
-  const float c_0 = __ldg(g.phi + (size_t)yl * nx + i), c_1 = __ldg(g.phi + (size_t)yl * nx + i + 1);
-  const float d_0 = __ldg(g.phi + (size_t)yr * nx + i), d_1 = __ldg(g.phi + (size_t)yr * nx + i + 1);
-  // -dphi/dx at the four nodes (in units of 1/dx)
-  const float ex00 = (a_l - a_1) * sx0, ex10 = (a_0 - a_r) * sx1;
-  const float ex01 = (b_l - b_1) * sx0, ex11 = (b_0 - b_r) * sx1;
-  const float ey00 = (c_0 - b_0) * sy0, ey10 = (c_1 - b_1) * sy0;
-  const float ey01 = (a_0 - d_0) * sy1, ey11 = (a_1 - d_1) * sy1;
-  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-  gx = w00 * ex00 + w10 * ex10 + w01 * ex01 + w11 * ex11;
-  gy = w00 * ey00 + w10 * ey10 + w01 * ey01 + w11 * ey11;
-}
 
 __device__ __forceinline__ float xs_lookup(const ProcDev& p, float E) {
   const float* e = p.e;
@@ -150,14 +121,12 @@ __device__ __forceinline__ void warp_deposit(const JobDev& J, const SlotDev& S, 
   }
 }
 
-// 512-particle chunks and 4 CTAs (32 warps) per SM.  Measured on B200 against 1024-particle
-// chunks at 2 CTAs per SM: 15% less time per particle pass.
+// 512-particle chunks and 5 CTAs (40 warps) per SM (47 registers, no spills).  Measured on
+// B200 (1025^2, 2e7 particles): 1024-particle chunks at 2 CTAs per SM take 15% longer than
+// 512 at 4, and 5 CTAs per SM take 3% less than 4 (0.574 against 0.593 ms per pass).
 #ifndef PIC_MOVER_MIN_BLOCKS
-#define PIC_MOVER_MIN_BLOCKS 4
+#define PIC_MOVER_MIN_BLOCKS 5
 #endif
-// Field nodes (float2 E) a warp stages for its particles' cells; a warp whose cells need more
-// falls back to the gather from global memory.
-constexpr int kWarpField = 96;
 constexpr int kRounds = PIC_CHUNK / PIC_MOVER_THREADS;
 constexpr int kWarps = PIC_MOVER_THREADS / 32;
 
@@ -219,15 +188,26 @@ __device__ void collide(const JobDev& J, const SlotDev& S, const SlotDev* slots,
   atomicAdd(&proc_count[chosen & 7], 1u);
 }
 
-// E (per unit cell, -dphi) at node (i, j) from phi through the computeElectricField stencils
-// (kernels.cu:134-191): central differences inside, one-sided on the edges.
-__device__ __forceinline__ float2 node_field(const float* __restrict__ phi, int nx, int ny, int i, int j) {
-  const float* row = phi + (size_t)j * nx;
-  const int il = i > 0 ? i - 1 : 0, ir = i < nx - 1 ? i + 1 : nx - 1;
-  const int jl = j > 0 ? j - 1 : 0, jr = j < ny - 1 ? j + 1 : ny - 1;
-  const float sx = (i > 0 && i < nx - 1) ? 0.5f : 1.0f, sy = (j > 0 && j < ny - 1) ? 0.5f : 1.0f;
-  return make_float2((__ldg(row + il) - __ldg(row + ir)) * sx,
-                     (__ldg(phi + (size_t)jl * nx + i) - __ldg(phi + (size_t)jr * nx + i)) * sy);
+// E per unit cell (-dphi across one cell) at every node of every job, from the job's
+// current FP64 potential with the computeElectricField stencils (kernels.cu:134-191):
+// (phi[i-1] - phi[i+1]) / 2 inside, phi[i] - phi[i+1] on the first and phi[i-1] - phi[i]
+// on the last node of a row, the same along columns; rounded to FP32 once.  Job j uses
+// blockIdx.y == j and a grid-stride loop over its nodes.
+__global__ void __launch_bounds__(256) efield32_kernel(const JobDev* __restrict__ jobs, const JobState* __restrict__ st) {
+  const JobDev& J = jobs[blockIdx.y];
+  float2* const out = J.efield;
+  if (!out) return;
+  const double* __restrict__ phi = J.phi64[st[blockIdx.y].phi_cur];
+  const int nx = J.nx, ny = J.ny, N = nx * ny;
+  for (int k = blockIdx.x * 256 + threadIdx.x; k < N; k += gridDim.x * 256) {
+    const int j = k / nx, i = k - j * nx;
+    const int il = i > 0 ? i - 1 : 0, ir = i < nx - 1 ? i + 1 : nx - 1;
+    const int jl = j > 0 ? j - 1 : 0, jr = j < ny - 1 ? j + 1 : ny - 1;
+    const double sx = (i > 0 && i < nx - 1) ? 0.5 : 1.0, sy = (j > 0 && j < ny - 1) ? 0.5 : 1.0;
+    const double ex = (phi[j * nx + il] - phi[j * nx + ir]) * sx;
+    const double ey = (phi[jl * nx + i] - phi[jr * nx + i]) * sy;
+    out[k] = make_float2((float)ex, (float)ey);
+  }
 }
 
 // Particle arrays of one chunk staged in shared memory.
@@ -270,10 +250,10 @@ __device__ __forceinline__ void issue_chunk(const JobDev* __restrict__ jobs, con
 // Chunks reach shared memory through bulk asynchronous copies, double buffered: while the
 // CTA works on chunk k, chunk k+1 is in flight, so HBM latency is covered by the copy engine
 // rather than by resident warps; results return with bulk stores.
-//  pass A  kick and the null-collision candidate test.  Each warp stages E at the nodes of its
-//          own cells (particles are cell-sorted, so a warp's 64 particles touch a few cells)
-//          and gathers from there; candidates (~nu_max dt of the particles) are listed per
-//          warp and collided by that warp's lanes afterwards
+//  pass A  kick and the null-collision candidate test.  E comes from the per-step node field
+//          (float2 loads; particles are cell-sorted, so a warp's loads hit a few cache lines);
+//          candidates (~nu_max dt of the particles) are listed per warp and collided by that
+//          warp's lanes afterwards
 //  pass B  drift, absorption, hit list and CIC deposit
 // Two block barriers per chunk (chunk data ready; results complete before the bulk stores),
 // a third only when the chunk starts a new slot and the slot and job tables are copied to
@@ -287,7 +267,6 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ int wlist[kWarps][kPerWarp];
   __shared__ int wcount[kWarps];
-  __shared__ float2 wfield[kWarps][kWarpField];
   __shared__ unsigned proc_count[8];
   __shared__ double ke_sh[kWarps];
   __shared__ SlotDev sS;
@@ -361,39 +340,8 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
 
     // ---- pass A: kick and collisions
     if (do_kick || do_mcc) {
-      // E at the nodes of this warp's cells: nodes [i0, i0 + fw) x [j0, j0 + fh)
-      int fi0 = 0, fj0 = 0, fw = 0;
-      bool use_field = false;
-      if (do_kick) {
-        int imin = 1 << 30, imax = -1, jmin = 1 << 30, jmax = -1;
-#pragma unroll
-        for (int r = 0; r < kRounds; ++r) {
-          const int q = wbase + r * 32 + lane;
-          if (base + q < n) {
-            const uint32_t c = s_cell[q];
-            if (c != PIC_CELL_OUT) {
-              const int i = cell_i(c), j = cell_j(c);
-              imin = min(imin, i); imax = max(imax, i); jmin = min(jmin, j); jmax = max(jmax, j);
-            }
-          }
-        }
-        imin = __reduce_min_sync(0xffffffffu, imin); jmin = __reduce_min_sync(0xffffffffu, jmin);
-        imax = __reduce_max_sync(0xffffffffu, imax); jmax = __reduce_max_sync(0xffffffffu, jmax);
-        if (imax >= 0) {
-          fi0 = imin;
-          fj0 = jmin;
-          fw = imax - imin + 2;
-          const int fh = jmax - jmin + 2;
-          use_field = fw * fh <= kWarpField;
-          if (use_field)
-            for (int e = lane; e < fw * fh; e += 32) {
-              const int ej = e / fw;
-              wfield[warp][e] = node_field(J.phi32, J.nx, J.ny, fi0 + (e - ej * fw), fj0 + ej);
-            }
-        }
-        __syncwarp();
-      }
-      PhiGather pg{J.phi32, J.nx, J.ny};
+      const float2* __restrict__ ef = J.efield;
+      const int enx = J.nx;
       if (lane == 0) wcount[warp] = 0;
       __syncwarp();
 #pragma unroll
@@ -407,23 +355,18 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
           if (do_kick && c != PIC_CELL_OUT) {
             float gx, gy;
             const float fx = s_fx[q], fy = s_fy[q];
-            const int i = cell_i(c), j = cell_j(c);
-            if (use_field) {
-              const float2* e0 = &wfield[warp][(j - fj0) * fw + (i - fi0)];
-              const float2 e00 = e0[0], e10 = e0[1], e01 = e0[fw], e11 = e0[fw + 1];
-              const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-              gx = w00 * e00.x + w10 * e10.x + w01 * e01.x + w11 * e11.x;
-              gy = w00 * e00.y + w10 * e10.y + w01 * e01.y + w11 * e11.y;
-            } else {
-              gather_dphi(pg, i, j, fx, fy, gx, gy);
-            }
+            const float2* e0 = ef + cell_j(c) * enx + cell_i(c);
+            const float2 e00 = __ldg(e0), e10 = __ldg(e0 + 1), e01 = __ldg(e0 + enx), e11 = __ldg(e0 + enx + 1);
+            const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
+            gx = w00 * e00.x + w10 * e10.x + w01 * e01.x + w11 * e11.x;
+            gy = w00 * e00.y + w10 * e10.y + w01 * e01.y + w11 * e11.y;
             vx += S.kx * gx;
             vy += S.ky * gy;
           }
           if (do_mcc) {
-            float u[4];
-            draw4(J.seed, s_pid[q], mcc_step, 0u, u);
             if (J.mcc_mode == 2) {
+              float u[4];
+              draw4(J.seed, s_pid[q], mcc_step, 0u, u);
               const ProcDev& P = J.procs[S.first_proc];
               const float v2 = vx * vx + vy * vy;
               const float sp = sqrtf(v2);
@@ -435,7 +378,7 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
                 atomicAdd(&proc_count[0], 1u);
               }
             } else {
-              cand = u[0] < S.pnull;
+              cand = draw_first(J.seed, s_pid[q], mcc_step, 0u) < S.pnull;
             }
           }
           s_vx[q] = vx;
@@ -531,7 +474,6 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
 // Exclusive prefix of mover chunks per slot (one CTA; slots are few).
 __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t* __restrict__ active,
                                    int* __restrict__ chunk_prefix, int nslots) {
-  __shared__ int acc;
   if (threadIdx.x == 0) {
     int a = 0;
     for (int s = 0; s < nslots; ++s) {
@@ -539,7 +481,6 @@ __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t
       if (!active || active[s]) a += (counts[s] + PIC_CHUNK - 1) / PIC_CHUNK;
     }
     chunk_prefix[nslots] = a;
-    acc = a;
   }
 }
 
@@ -555,11 +496,18 @@ int mover_blocks_per_sm() {
 }
 
 int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t stream) {
+  int k = 2;
+  if ((flags & PIC_PHASE_KICK_I) && L.njobs > 0) {
+    // the node field of every job's current potential, for the kick
+    const int gx = std::max(1, std::min(4096, 8 * L.num_sms / L.njobs));
+    efield32_kernel<<<dim3(gx, L.njobs), 256, 0, stream>>>(L.jobs, L.st);
+    ++k;
+  }
   chunk_table_kernel<<<1, 32, 0, stream>>>(L.counts, L.active, L.chunk_prefix, L.nslots);
   if (L.ev_mover_begin) cudaEventRecord(L.ev_mover_begin, stream);
   mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, kMoverDynSmem, stream>>>(L.jobs, L.st, L.slots, L.counts,
                                                                           L.hit_counts, L.chunk_prefix, L.nslots, flags,
                                                                           explicit_step);
   if (L.ev_mover_end) cudaEventRecord(L.ev_mover_end, stream);
-  return 2;
+  return k;
 }

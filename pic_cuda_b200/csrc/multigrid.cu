@@ -17,7 +17,7 @@
 //   mg_coarse  one CTA per job runs the whole V-cycle from <= 65x65 down in shared memory
 //   (levels 129^2-513^2 and below run in one thread-block cluster, mg_cluster.cu)
 //   mg_up      prolongation + nu_post sweeps on 32x32 tiles; on level 0 also the FP64
-//              update phi += e, the new FP64 residual, phi32 and the norm (last CTA of each
+//              update phi += e, the new FP64 residual and the norm (last CTA of each
 //              job reduces the per-tile partials in a fixed order: deterministic).
 #include <algorithm>
 #include "common.cuh"
@@ -29,10 +29,6 @@ namespace {
 constexpr int kTI = 32;   // level-0 residual / update tile
 constexpr int kTC = 16;   // down-leg coarse tile
 constexpr int kTU = 32;   // up-leg fine tile
-
-__device__ __forceinline__ double rho_at(const JobDev& J, size_t idx) {
-  return J.deposit_mode == 0 ? (double)J.rho_f[idx] : J.deposit_mode == 1 ? (double)J.rho_i[idx] * 0x1p-40 : J.rho_d[idx];
-}
 
 // The charge grid of a job, copied to registers (see mg_up_kernel).
 struct RhoSrc {
@@ -89,14 +85,23 @@ __device__ bool last_of_job(JobState& T, int nlocal) {
 }
 
 // ---------------------------------------------------------------- mg_init
+// Level-0 defect of the initial guess on a 32 x 32 tile: the potential (and with the
+// extrapolated warm start the previous solution) with a one-node halo and rho arrive in one
+// batch of asynchronous copies; the guess is formed once per node in shared memory.
 __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
                                                       JobState* __restrict__ st, int* running) {
+  constexpr int PW = kTI + 2, NT = 256;
+  constexpr int NP = (PW * PW + NT - 1) / NT;
+  constexpr int NO = kTI * kTI / NT;
+  __shared__ __align__(16) double G[PW * PW];    // guess with halo (the current potential first)
+  __shared__ __align__(16) double Q[PW * PW];    // previous solution with halo (warm start 1)
+  __shared__ __align__(16) double RH[kTI * kTI]; // rho of the owned nodes, raw
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
   const int nx = J.nx, ny = J.ny;
   const int cur = T.phi_cur;
-  const double* phi = J.phi64[cur];
+  const double* __restrict__ phi = J.phi64[cur];
   // warm_start 1: the initial guess 2 phi_{k-1} - phi_{k-2} goes to a third buffer (phi_{k-1}
   // is kept as the next step's history), the defect correction then alternates between that
   // buffer and the one phi_{k-2} held
@@ -104,42 +109,83 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   const int prev = T.phi_prev1 - 1;
   const bool hist = xs && prev >= 0;
   const int tgt = hist ? 3 - cur - prev : (cur + 1) % 3;
-  const double* pp = hist ? J.phi64[prev] : phi;
+  const double* __restrict__ pp = hist ? J.phi64[prev] : phi;
   double* guess = xs ? J.phi64[tgt] : nullptr;
   float* const f0 = T.fsel ? J.f0b : J.f[0];
   const double a = hist ? 2.0 : 1.0, b = hist ? 1.0 : 0.0;
   const double inv_h2 = 1.0 / (J.h * J.h);
+  const double rhs_scale = J.rhs_scale;
+  const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
+  double* const partials = J.partials;
+  const int i0 = tr.ti * kTI, j0 = tr.tj * kTI;
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int u = 0; u < NP; ++u) {
+    const int k = t + u * NT;
+    if (k < PW * PW) {
+      const int py = k / PW, px = k - py * PW;
+      const int gx = i0 - 1 + px, gy = j0 - 1 + py;
+      const bool in = (unsigned)gx < (unsigned)nx && (unsigned)gy < (unsigned)ny;
+      const int g = in ? gy * nx + gx : 0;
+      tma::cp_async8(G + k, phi + g, in);
+      if (hist) tma::cp_async8(Q + k, pp + g, in);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NO; ++u) {
+    const int k = t + u * NT;
+    const int gx = i0 + (k & 31), gy = j0 + (k >> 5);
+    const bool in = gx < nx && gy < ny;
+    const int g = in ? gy * nx + gx : 0;
+    if (rho.mode == 0) tma::cp_async4(reinterpret_cast<float*>(RH) + k, rho.f + g, in);
+    else if (rho.mode == 1) tma::cp_async8(RH + k, rho.i + g, in);
+    else tma::cp_async8(RH + k, rho.d + g, in);
+  }
+  tma::cp_async_wait_all();
+  __syncthreads();
+  if (hist) {
+#pragma unroll
+    for (int u = 0; u < NP; ++u) {
+      const int k = t + u * NT;
+      if (k < PW * PW) G[k] = a * G[k] - b * Q[k];
+    }
+    __syncthreads();
+  }
   double ar = 0.0, af = 0.0;
-  for (int k = threadIdx.x; k < kTI * kTI; k += blockDim.x) {
-    const int i = tr.ti * kTI + (k % kTI), j = tr.tj * kTI + (k / kTI);
+#pragma unroll
+  for (int u = 0; u < NO; ++u) {
+    const int k = t + u * NT;
+    const int ox = k & 31, oy = k >> 5;
+    const int i = i0 + ox, j = j0 + oy;
     if (i >= nx || j >= ny) continue;
-    const size_t c = (size_t)j * nx + i;
-    const double F = J.rhs_scale * rho_at(J, c);
+    const int c = j * nx + i;
+    const int q = (oy + 1) * PW + (ox + 1);
+    const double rv = rho.mode == 0 ? (double)reinterpret_cast<const float*>(RH)[k]
+                      : rho.mode == 1 ? (double)reinterpret_cast<const long long*>(RH)[k] * 0x1p-40 : RH[k];
+    const double F = rhs_scale * rv;
     double r = 0.0;
-    const double g0 = a * phi[c] - b * pp[c];
+    const double g0 = G[q];
     if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
-      const double gs = (a * phi[c - nx] - b * pp[c - nx]) + (a * phi[c + nx] - b * pp[c + nx]) +
-                        (a * phi[c - 1] - b * pp[c - 1]) + (a * phi[c + 1] - b * pp[c + 1]);
+      const double gs = G[q - PW] + G[q + PW] + G[q - 1] + G[q + 1];
       const double lap = (gs - 4.0 * g0) * inv_h2;
       r = F - lap;
     }
     if (xs) guess[c] = g0;
     f0[c] = (float)r;
-    J.phi32[c] = (float)g0;
     ar += r * r;
     af += F * F;
   }
   const double sr = block_sum(ar);
   const double sf = block_sum(af);
-  if (threadIdx.x == 0) {
-    J.partials[2 * (tr.pbase + tr.local)] = sr;
-    J.partials[2 * (tr.pbase + tr.local) + 1] = sf;
+  if (t == 0) {
+    partials[2 * (tr.pbase + tr.local)] = sr;
+    partials[2 * (tr.pbase + tr.local) + 1] = sf;
   }
   if (last_of_job(T, tr.nlocal)) {
     __threadfence();
-    const double r2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 0);
-    const double f2 = ordered_sum(J.partials + 2 * tr.pbase, tr.nlocal, 2, 1);
-    if (threadIdx.x != 0) return;
+    const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
+    const double f2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 1);
+    if (t != 0) return;
     T.rnorm2 = r2;
     T.fnorm2 = f2;
     T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
@@ -285,7 +331,7 @@ __device__ __forceinline__ float prolong_value(const float* cp, int pitch, bool 
 }
 
 // ---------------------------------------------------------------- mg_coarse
-// Levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.  Level l occupies
+// Levels lc .. L-1 of one job in the shared memory of one CTA.  Level l occupies
 // E then F, n_l rows of pitch n_l + 1 (even).  Every red-black half-sweep, restriction and
 // prolongation maps thread t to column i = 1 + t % (n-2) and walks the rows 1 + t / (n-2)
 // + k G (G = threads / (n-2) row groups), so the lanes of a warp touch consecutive columns:
@@ -293,10 +339,30 @@ __device__ __forceinline__ float prolong_value(const float* cp, int pitch, bool 
 // lane idles on the other colour.  Levels of side <= kWarpLevelMax run on warp 0 alone
 // (warp barriers instead of block barriers).
 constexpr int kWarpLevelMax = 17;
+// Threads that work on the larger levels (the CTA may be bigger: the cooperative levels
+// kernel calls the solver with 1024): a 65^2 level then gives each thread a few nodes per
+// half-sweep, and fewer warps issue the per-phase overhead on the one SM.
+constexpr int kCoarseThreads = 256;
 
 template <bool WARP>
 __device__ __forceinline__ void group_sync() {
   if (WARP) __syncwarp(); else __syncthreads();
+}
+
+// Thread t of T on m interior columns: column 1 + t % m, row group t / m of G = T / m.  The
+// quotient comes from (t + 0.5) / m in FP32, exact for t < 2^12 and m < 2^12 (the fraction
+// stays >= 0.5 / m from an integer, far above the rounding error), so no integer division.
+struct ColMap {
+  int col, g, G;
+};
+__device__ __forceinline__ ColMap col_map(int t, int T, int m) {
+  ColMap c;
+  if (m <= 0) { c.col = 1; c.g = 1; c.G = 0; return c; }
+  const float r = 1.f / (float)m;
+  c.G = (int)(((float)T + 0.5f) * r);
+  c.g = (int)(((float)t + 0.5f) * r);
+  c.col = 1 + t - c.g * m;
+  return c;
 }
 
 // nu red-black SOR sweeps (colour (i+j) odd first, Multigrid.cu:246-265) on the interior of
@@ -304,21 +370,22 @@ __device__ __forceinline__ void group_sync() {
 // everywhere (pre-smoothing), so the first half-sweep reads no neighbours.
 template <bool WARP, bool ZERO = false>
 __device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, float omega, int nu, int t, int T) {
-  const int m = n - 2;
-  const int G = m > 0 ? T / m : 0;
-  const int i = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  const ColMap cm = col_map(t, T, n - 2);
+  const int i = cm.col, g = cm.g, G = cm.G;
   const bool on = g < G;
   const float om1 = 1.f - omega;
   for (int it = 0; it < nu; ++it)
     for (int colour = 1; colour >= 0; --colour) {
       if (on) {
         if (ZERO && it == 0 && colour == 1) {
+#pragma unroll 4
           for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
             const float s = 0.f;
             const float nv = 0.25f * (s - h2 * f[j * P + i]);
             e[j * P + i] = fmaf(omega, nv, om1 * 0.f);
           }
         } else {
+#pragma unroll 4
           for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
             float* p = e + j * P + i;
             const float s = p[P] + p[-P] + p[1] + p[-1];
@@ -336,10 +403,10 @@ __device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, f
 template <bool WARP>
 __device__ void level_restrict(const float* e, const float* f, int n, int P, float inv_h2, float* fn, int nc, int Pc,
                                int t, int T) {
-  const int m = nc - 2;
-  const int G = m > 0 ? T / m : 0;
-  const int ic = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  const ColMap cm = col_map(t, T, nc - 2);
+  const int ic = cm.col, g = cm.g, G = cm.G;
   if (g < G)
+#pragma unroll 2
     for (int jc = 1 + g; jc <= nc - 2; jc += G) {
       float r[3][3];
 #pragma unroll
@@ -360,10 +427,10 @@ __device__ void level_restrict(const float* e, const float* f, int n, int P, flo
 // added to the interior of e (n x n, pitch P).
 template <bool WARP>
 __device__ void level_prolong(float* e, int n, int P, const float* c, int Pc, int t, int T) {
-  const int m = n - 2;
-  const int G = m > 0 ? T / m : 0;
-  const int i = m > 0 ? 1 + t % m : 1, g = m > 0 ? t / m : T;
+  const ColMap cm = col_map(t, T, n - 2);
+  const int i = cm.col, g = cm.g, G = cm.G;
   if (g < G)
+#pragma unroll 4
     for (int j = 1 + g; j <= n - 2; j += G) {
       e[j * P + i] += prolong_value(c + (j >> 1) * Pc + (i >> 1), Pc, i & 1, j & 1);
     }
@@ -377,24 +444,24 @@ __host__ __device__ inline size_t coarse_layout_bytes(const int* nl, int lc, int
   return b;
 }
 
-// n*n values between global memory (pitch n) and a shared level (pitch n + 1), 1024 threads,
+// n*n values between global memory (pitch n) and a shared level (pitch n + 1), all threads,
 // loads of a batch issued before any store.  Row = floor((k + 0.5) / n) in FP32 is exact while
 // n^2 < 2^21: k + 0.5 is representable, and the product's rounding error (< n 2^-22) stays
 // below the fraction's distance from an integer (>= 0.5 / n).
 constexpr int kCoarseBatch = 17;
 __device__ __forceinline__ void coarse_load(float* dst, const float* __restrict__ src, int n) {
-  const int N = n * n;
+  const int N = n * n, T = blockDim.x;
   const float inv_n = 1.f / (float)n;
-  for (int k0 = 0; k0 < N; k0 += kCoarseBatch * 1024) {
+  for (int k0 = 0; k0 < N; k0 += kCoarseBatch * T) {
     float v[kCoarseBatch];
 #pragma unroll
     for (int u = 0; u < kCoarseBatch; ++u) {
-      const int k = k0 + (int)threadIdx.x + u * 1024;
+      const int k = k0 + (int)threadIdx.x + u * T;
       v[u] = k < N ? __ldg(src + k) : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < kCoarseBatch; ++u) {
-      const int k = k0 + (int)threadIdx.x + u * 1024;
+      const int k = k0 + (int)threadIdx.x + u * T;
       if (k < N) {
         const int j = (int)(((float)k + 0.5f) * inv_n);
         dst[j * (n + 1) + (k - j * n)] = v[u];
@@ -405,7 +472,7 @@ __device__ __forceinline__ void coarse_load(float* dst, const float* __restrict_
 __device__ __forceinline__ void coarse_store(float* __restrict__ dst, const float* src, int n) {
   const int N = n * n;
   const float inv_n = 1.f / (float)n;
-  for (int k = threadIdx.x; k < N; k += 1024) {
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
     const int j = (int)(((float)k + 0.5f) * inv_n);
     dst[k] = src[j * (n + 1) + (k - j * n)];
   }
@@ -438,23 +505,24 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
 #define H2(l) ((float)((h * (double)(1 << (l))) * (h * (double)(1 << (l)))))
 #define IH2(l) ((float)(1.0 / ((h * (double)(1 << (l))) * (h * (double)(1 << (l))))))
   const int t = threadIdx.x;
+  constexpr int TW = kCoarseThreads;   // threads that work on the levels above kWarpLevelMax
   // zero every level (corrections start at 0; coarse right-hand sides keep a zero boundary),
   // except F(lc), which is loaded whole
   {
     const int n = nl[lc];
     const int f0 = off[lc] + n * (n + 1), f1 = off[lc] + 2 * n * (n + 1);
-    for (int k = t; k < off[PIC_MAX_LEVELS]; k += 1024)
+    for (int k = t; k < off[PIC_MAX_LEVELS]; k += blockDim.x)
       if (k < f0 || k >= f1) sm[k] = 0.f;
     coarse_load(F(lc), f_top, n);
   }
   __syncthreads();
   int l = lc;
   for (; l < L - 1 && nl[l] > kWarpLevelMax; ++l) {
-    level_sweeps<false, true>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_pre, t, 1024);
-    level_restrict<false>(E(l), F(l), nl[l], PT(l), IH2(l), F(l + 1), nl[l + 1], PT(l + 1), t, 1024);
+    level_sweeps<false, true>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_pre, t, TW);
+    level_restrict<false>(E(l), F(l), nl[l], PT(l), IH2(l), F(l + 1), nl[l + 1], PT(l + 1), t, TW);
   }
   if (nl[l] > kWarpLevelMax) {  // a large coarsest level (l == L - 1)
-    level_sweeps<false>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_coarse, t, 1024);
+    level_sweeps<false>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_coarse, t, TW);
   } else {
     if (t < 32) {
       for (int k = l; k < L - 1; ++k) {
@@ -470,8 +538,8 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
     __syncthreads();
   }
   for (int k = l - 1; k >= lc; --k) {
-    level_prolong<false>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, 1024);
-    level_sweeps<false>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, 1024);
+    level_prolong<false>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, TW);
+    level_sweeps<false>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, TW);
   }
   coarse_store(e_top, E(lc), nl[lc]);
   __syncthreads();  // shared memory is free for the CTA's next job
@@ -482,7 +550,7 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
 #undef IH2
 }
 
-__global__ void __launch_bounds__(1024) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
+__global__ void __launch_bounds__(kCoarseThreads) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
                                                          const JobState* __restrict__ st) {
   extern __shared__ float sm[];
   coarse_solve(job_list[blockIdx.x], jobs, st, sm);
@@ -582,7 +650,6 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const double inv_h2 = 1.0 / (J.h * J.h);
   const double rhs_scale = J.rhs_scale;
   const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
-  float* const phi32 = J.phi32;
   float* const f0 = fsel ? J.f[0] : J.f0b;   // the new defect goes to the other buffer
   double* const partials = J.partials;
   const double tol = J.tol;
@@ -651,7 +718,6 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
       r = F - lap;
     }
     pn[g] = P[q];
-    phi32[g] = (float)P[q];
     f0[g] = (float)r;
     ar += r * r;
   }
@@ -800,7 +866,7 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
 // Up leg (as mg_up_kernel modes 0 and 1).  MODE 0, level l >= 1: the bilinear prolongation
 // of the coarser correction added to the pre-smoothed one, NU post-sweeps, the owned nodes
 // to eu_l.  MODE 1, level 0 (NT = 256): the same with a one-node halo, then phi <- phi + e in
-// FP64, the new FP64 defect, phi32 and the deterministic norm.  Every global input of the
+// FP64, the new FP64 defect and the deterministic norm.  Every global input of the
 // tile (e, f, the coarse tile, and on level 0 phi64 and rho) is requested in one batch.
 template <int NU, int MODE, int NT>
 __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const TileRef* __restrict__ tiles,
@@ -841,7 +907,6 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   const double inv_h2 = 1.0 / (J.h * J.h);
   const double rhs_scale = J.rhs_scale;
   const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
-  float* const phi32 = J.phi32;
   float* const f0 = fsel ? J.f[0] : J.f0b;   // the new defect goes to the other buffer
   double* const partials = J.partials;
   const double tol = J.tol;
@@ -948,7 +1013,6 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
         r = F - lap;
       }
       pn[g] = P64[q];
-      phi32[g] = (float)P64[q];
       f0[g] = (float)r;
       ar += r * r;
     }
@@ -1156,7 +1220,7 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   }
   for (int l = 0; l < M.max_depth; ++l)
     if (M.n_down[l]) { launch_down(M, l, L, s); ++k; }
-  if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, 1024, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
+  if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, kCoarseThreads, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
   if (M.n_cluster) k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s);
   for (int l = M.max_depth - 1; l >= 0; --l)
     if (M.n_up[l]) { launch_up(M, l, L, s); ++k; }
