@@ -314,7 +314,7 @@ __device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict
 
 __global__ void __launch_bounds__(256) mg_down_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
                                                       const JobState* __restrict__ st, int l) {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   down_tile(BlockGroup{}, tiles[blockIdx.x], jobs, st, l, sm);
 }
 
@@ -331,46 +331,51 @@ __device__ __forceinline__ float prolong_value(const float* cp, int pitch, bool 
 }
 
 // ---------------------------------------------------------------- mg_coarse
-// Levels lc .. L-1 of one job in the shared memory of one CTA.  Level l occupies
+// Levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.  Level l occupies
 // E then F, n_l rows of pitch n_l + 1 (even).  Every red-black half-sweep, restriction and
 // prolongation maps thread t to column i = 1 + t % (n-2) and walks the rows 1 + t / (n-2)
 // + k G (G = threads / (n-2) row groups), so the lanes of a warp touch consecutive columns:
-// with an even pitch the two colours of a column pair fall into distinct banks, and no
-// lane idles on the other colour.  Levels of side <= kWarpLevelMax run on warp 0 alone
-// (warp barriers instead of block barriers).
-constexpr int kWarpLevelMax = 17;
-// Threads that work on the larger levels (the CTA may be bigger: the cooperative levels
-// kernel calls the solver with 1024): a 65^2 level then gives each thread a few nodes per
-// half-sweep, and fewer warps issue the per-phase overhead on the one SM.
-constexpr int kCoarseThreads = 256;
+// with an even pitch the two colours of a column pair fall into distinct banks, and no lane
+// idles on the other colour.  Every level uses the whole CTA: the small levels are a chain of
+// barrier-separated phases whose length is one node's latency when each thread has at most
+// one node (measured on B200: one warp walking 17^2 .. 3^2 alone took 12 of the solve's 29 us).
+constexpr int kCoarseThreads = 1024;
 
-template <bool WARP>
-__device__ __forceinline__ void group_sync() {
-  if (WARP) __syncwarp(); else __syncthreads();
-}
+// Per-level constants of the coarse solve, computed once per launch (the FP64 divisions stay
+// off the barrier chain).
+struct CoarseLevel {
+  int off;       // first float of E in the shared layout (F follows at off + n (n + 1))
+  int n;         // side
+  float h2;      // h_l^2
+  float ih2;     // 1 / h_l^2
+  float rm;      // 1 / (n - 2) in FP32 (column map), 0 if the level has no interior
+};
 
 // Thread t of T on m interior columns: column 1 + t % m, row group t / m of G = T / m.  The
-// quotient comes from (t + 0.5) / m in FP32, exact for t < 2^12 and m < 2^12 (the fraction
-// stays >= 0.5 / m from an integer, far above the rounding error), so no integer division.
+// quotient comes from (t + 0.5) * (1/m) in FP32, exact for t, T < 2^12 and m < 2^12 (the
+// fraction stays >= 0.5 / m from an integer, far above the rounding error).
 struct ColMap {
   int col, g, G;
 };
-__device__ __forceinline__ ColMap col_map(int t, int T, int m) {
+__device__ __forceinline__ ColMap col_map(int t, int T, int m, float rm) {
   ColMap c;
   if (m <= 0) { c.col = 1; c.g = 1; c.G = 0; return c; }
-  const float r = 1.f / (float)m;
-  c.G = (int)(((float)T + 0.5f) * r);
-  c.g = (int)(((float)t + 0.5f) * r);
+  c.G = (int)(((float)T + 0.5f) * rm);
+  c.g = (int)(((float)t + 0.5f) * rm);
   c.col = 1 + t - c.g * m;
   return c;
 }
 
 // nu red-black SOR sweeps (colour (i+j) odd first, Multigrid.cu:246-265) on the interior of
-// an n x n level with row pitch P, by T threads (T >= n - 2).  ZERO: e enters as +0
-// everywhere (pre-smoothing), so the first half-sweep reads no neighbours.
-template <bool WARP, bool ZERO = false>
-__device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, float omega, int nu, int t, int T) {
-  const ColMap cm = col_map(t, T, n - 2);
+// level L (row pitch n + 1) by the CTA's T threads.  ZERO: e enters as +0 everywhere
+// (pre-smoothing), so the first half-sweep reads no neighbours.
+template <bool ZERO = false>
+__device__ void level_sweeps(float* sm, const CoarseLevel& L, float omega, int nu, int t, int T) {
+  const int n = L.n, P = n + 1;
+  float* const e = sm + L.off;
+  const float* const f = e + n * P;
+  const float h2 = L.h2;
+  const ColMap cm = col_map(t, T, n - 2, L.rm);
   const int i = cm.col, g = cm.g, G = cm.G;
   const bool on = g < G;
   const float om1 = 1.f - omega;
@@ -378,14 +383,12 @@ __device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, f
     for (int colour = 1; colour >= 0; --colour) {
       if (on) {
         if (ZERO && it == 0 && colour == 1) {
-#pragma unroll 4
           for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
             const float s = 0.f;
             const float nv = 0.25f * (s - h2 * f[j * P + i]);
             e[j * P + i] = fmaf(omega, nv, om1 * 0.f);
           }
         } else {
-#pragma unroll 4
           for (int j = 1 + ((colour - i - 1) & 1) + 2 * g; j <= n - 2; j += 2 * G) {
             float* p = e + j * P + i;
             const float s = p[P] + p[-P] + p[1] + p[-1];
@@ -394,19 +397,21 @@ __device__ void level_sweeps(float* e, const float* f, int n, int P, float h2, f
           }
         }
       }
-      group_sync<WARP>();
+      __syncthreads();
     }
 }
 
-// Residual of level (e, f, n) and its full weighting (Multigrid.cu:299-349) to the interior
-// of the next level's right-hand side fn (nc x nc, pitch Pc; its boundary stays 0).
-template <bool WARP>
-__device__ void level_restrict(const float* e, const float* f, int n, int P, float inv_h2, float* fn, int nc, int Pc,
-                               int t, int T) {
-  const ColMap cm = col_map(t, T, nc - 2);
+// Residual of level A and its full weighting (Multigrid.cu:299-349) to the interior of the
+// next level's right-hand side (its boundary stays 0).
+__device__ void level_restrict(float* sm, const CoarseLevel& A, const CoarseLevel& B, int t, int T) {
+  const int n = A.n, P = n + 1, nc = B.n, Pc = nc + 1;
+  const float* const e = sm + A.off;
+  const float* const f = e + n * P;
+  float* const fn = sm + B.off + nc * Pc;
+  const float inv_h2 = A.ih2;
+  const ColMap cm = col_map(t, T, nc - 2, B.rm);
   const int ic = cm.col, g = cm.g, G = cm.G;
   if (g < G)
-#pragma unroll 2
     for (int jc = 1 + g; jc <= nc - 2; jc += G) {
       float r[3][3];
 #pragma unroll
@@ -420,21 +425,21 @@ __device__ void level_restrict(const float* e, const float* f, int n, int P, flo
       fn[jc * Pc + ic] = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] +
                           r[0][2] + r[2][0] + r[2][2]) * 0.0625f;
     }
-  group_sync<WARP>();
+  __syncthreads();
 }
 
-// Bilinear prolongation (Multigrid.cu:351-407) of the coarse correction c (nc x nc, pitch Pc)
-// added to the interior of e (n x n, pitch P).
-template <bool WARP>
-__device__ void level_prolong(float* e, int n, int P, const float* c, int Pc, int t, int T) {
-  const ColMap cm = col_map(t, T, n - 2);
+// Bilinear prolongation (Multigrid.cu:351-407) of level B's correction added to the interior
+// of level A's.
+__device__ void level_prolong(float* sm, const CoarseLevel& A, const CoarseLevel& B, int t, int T) {
+  const int n = A.n, P = n + 1, Pc = B.n + 1;
+  float* const e = sm + A.off;
+  const float* const c = sm + B.off;
+  const ColMap cm = col_map(t, T, n - 2, A.rm);
   const int i = cm.col, g = cm.g, G = cm.G;
   if (g < G)
-#pragma unroll 4
-    for (int j = 1 + g; j <= n - 2; j += G) {
+    for (int j = 1 + g; j <= n - 2; j += G)
       e[j * P + i] += prolong_value(c + (j >> 1) * Pc + (i >> 1), Pc, i & 1, j & 1);
-    }
-  group_sync<WARP>();
+  __syncthreads();
 }
 
 // Shared-memory bytes of levels lc .. levels-1 in the coarse solver's layout.
@@ -444,11 +449,11 @@ __host__ __device__ inline size_t coarse_layout_bytes(const int* nl, int lc, int
   return b;
 }
 
-// n*n values between global memory (pitch n) and a shared level (pitch n + 1), all threads,
-// loads of a batch issued before any store.  Row = floor((k + 0.5) / n) in FP32 is exact while
-// n^2 < 2^21: k + 0.5 is representable, and the product's rounding error (< n 2^-22) stays
-// below the fraction's distance from an integer (>= 0.5 / n).
-constexpr int kCoarseBatch = 17;
+// n*n values from global memory (pitch n) to a shared level (pitch n + 1), all threads, the
+// loads of a batch issued before any store.  Row = floor((k + 0.5) / n) in FP32 is exact
+// while n^2 < 2^21: k + 0.5 is representable, and the product's rounding error
+// (< n 2^-22) stays below the fraction's distance from an integer (>= 0.5 / n).
+constexpr int kCoarseBatch = 5;
 __device__ __forceinline__ void coarse_load(float* dst, const float* __restrict__ src, int n) {
   const int N = n * n, T = blockDim.x;
   const float inv_n = 1.f / (float)n;
@@ -490,69 +495,48 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   const int nu_pre = J.nu_pre, nu_post = J.nu_post, nu_coarse = J.nu_coarse;
   float* const e_top = J.e[lc];
   const float* const f_top = (lc == 0 && st[job].fsel) ? J.f0b : J.f[lc];
-  __shared__ int off[PIC_MAX_LEVELS + 1];
-  __shared__ int nl[PIC_MAX_LEVELS];
-  if (threadIdx.x < PIC_MAX_LEVELS) nl[threadIdx.x] = J.nl[threadIdx.x];
-  if (threadIdx.x == 0) {
+  __shared__ CoarseLevel lv[PIC_MAX_LEVELS];
+  __shared__ int total;
+  const int t = threadIdx.x, T = blockDim.x;
+  if (t < PIC_MAX_LEVELS) {
+    const int l = t;
+    const int n = (l >= lc && l < L) ? J.nl[l] : 0;
+    const double hl = h * (double)(1 << l);
+    lv[l].n = n;
+    lv[l].h2 = (float)(hl * hl);
+    lv[l].ih2 = (float)(1.0 / (hl * hl));
+    lv[l].rm = n > 2 ? 1.f / (float)(n - 2) : 0.f;
+  }
+  __syncthreads();
+  if (t == 0) {
     int o = 0;
-    for (int k = lc; k < L; ++k) { off[k] = o; o += 2 * J.nl[k] * (J.nl[k] + 1); }
-    off[PIC_MAX_LEVELS] = o;
+    for (int l = lc; l < L; ++l) { lv[l].off = o; o += 2 * lv[l].n * (lv[l].n + 1); }
+    total = o;
   }
   __syncthreads();
-#define E(l) (sm + off[l])
-#define F(l) (sm + off[l] + nl[l] * (nl[l] + 1))
-#define PT(l) (nl[l] + 1)
-#define H2(l) ((float)((h * (double)(1 << (l))) * (h * (double)(1 << (l)))))
-#define IH2(l) ((float)(1.0 / ((h * (double)(1 << (l))) * (h * (double)(1 << (l))))))
-  const int t = threadIdx.x;
-  constexpr int TW = kCoarseThreads;   // threads that work on the levels above kWarpLevelMax
-  // zero every level (corrections start at 0; coarse right-hand sides keep a zero boundary),
-  // except F(lc), which is loaded whole
-  {
-    const int n = nl[lc];
-    const int f0 = off[lc] + n * (n + 1), f1 = off[lc] + 2 * n * (n + 1);
-    for (int k = t; k < off[PIC_MAX_LEVELS]; k += blockDim.x)
-      if (k < f0 || k >= f1) sm[k] = 0.f;
-    coarse_load(F(lc), f_top, n);
-  }
+  // zero every level (corrections start at 0; coarse right-hand sides keep a zero boundary);
+  // the layout is a multiple of 4 floats, 16-byte aligned
+  for (int k = t; k < total / 4; k += T) reinterpret_cast<float4*>(sm)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
-  int l = lc;
-  for (; l < L - 1 && nl[l] > kWarpLevelMax; ++l) {
-    level_sweeps<false, true>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_pre, t, TW);
-    level_restrict<false>(E(l), F(l), nl[l], PT(l), IH2(l), F(l + 1), nl[l + 1], PT(l + 1), t, TW);
+  coarse_load(sm + lv[lc].off + lv[lc].n * (lv[lc].n + 1), f_top, lv[lc].n);
+  __syncthreads();
+  for (int l = lc; l < L - 1; ++l) {
+    level_sweeps<true>(sm, lv[l], omega, nu_pre, t, T);
+    level_restrict(sm, lv[l], lv[l + 1], t, T);
   }
-  if (nl[l] > kWarpLevelMax) {  // a large coarsest level (l == L - 1)
-    level_sweeps<false>(E(l), F(l), nl[l], PT(l), H2(l), omega, nu_coarse, t, TW);
-  } else {
-    if (t < 32) {
-      for (int k = l; k < L - 1; ++k) {
-        level_sweeps<true, true>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_pre, t, 32);
-        level_restrict<true>(E(k), F(k), nl[k], PT(k), IH2(k), F(k + 1), nl[k + 1], PT(k + 1), t, 32);
-      }
-      level_sweeps<true>(E(L - 1), F(L - 1), nl[L - 1], PT(L - 1), H2(L - 1), omega, nu_coarse, t, 32);
-      for (int k = L - 2; k >= l; --k) {
-        level_prolong<true>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, 32);
-        level_sweeps<true>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, 32);
-      }
-    }
-    __syncthreads();
+  level_sweeps(sm, lv[L - 1], omega, nu_coarse, t, T);
+  for (int l = L - 2; l >= lc; --l) {
+    level_prolong(sm, lv[l], lv[l + 1], t, T);
+    level_sweeps(sm, lv[l], omega, nu_post, t, T);
   }
-  for (int k = l - 1; k >= lc; --k) {
-    level_prolong<false>(E(k), nl[k], PT(k), E(k + 1), PT(k + 1), t, TW);
-    level_sweeps<false>(E(k), F(k), nl[k], PT(k), H2(k), omega, nu_post, t, TW);
-  }
-  coarse_store(e_top, E(lc), nl[lc]);
+  coarse_store(e_top, sm + lv[lc].off, lv[lc].n);
   __syncthreads();  // shared memory is free for the CTA's next job
-#undef E
-#undef F
-#undef PT
-#undef H2
-#undef IH2
 }
 
-__global__ void __launch_bounds__(kCoarseThreads) mg_coarse_kernel(const int* __restrict__ job_list, const JobDev* __restrict__ jobs,
-                                                         const JobState* __restrict__ st) {
-  extern __shared__ float sm[];
+__global__ void __launch_bounds__(kCoarseThreads) mg_coarse_kernel(const int* __restrict__ job_list,
+                                                                   const JobDev* __restrict__ jobs,
+                                                                   const JobState* __restrict__ st) {
+  extern __shared__ __align__(16) float sm[];
   coarse_solve(job_list[blockIdx.x], jobs, st, sm);
 }
 
@@ -619,7 +603,7 @@ __device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__
 // mode 2: level 0 update only (e_0 produced by the coarse kernel).
 __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
                                                     JobState* __restrict__ st, int l, int mode, int* running) {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
@@ -1100,7 +1084,7 @@ __device__ bool grid_barrier(unsigned* count, unsigned target) {
 }
 
 __global__ void __launch_bounds__(1024, 1) mg_levels_kernel(const __grid_constant__ MgLevelsArgs a) {
-  extern __shared__ float sm[];
+  extern __shared__ __align__(16) float sm[];
   const QuarterGroup g{(int)(threadIdx.x >> 8)};
   float* qsm = sm + g.q * a.quarter_floats;
   const int slots = gridDim.x * 4, slot = blockIdx.x * 4 + g.q;
