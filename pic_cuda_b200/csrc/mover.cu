@@ -7,17 +7,16 @@
 //   MCC      null-collision Monte Carlo (or the reference's elastic form, mcc.cu:56-85)
 //   drift    update_coordinates (kernels.cu:8-23) on cell-relative FP32 positions
 //   walls    detect_intersections (collisions.cu:7-54) / box absorption; hits are appended
-//            with warp-aggregated atomics (compaction happens in compact.cu)
-//   deposit  updateDensity (kernels.cu:26-69) at the new position: per warp a segmented
-//            reduction over lanes that share a cell (particles are counting-sorted by cell),
-//            then one atomic per node per segment; FP32 or int64 fixed point.
+//            with one atomic per warp item (compaction happens in compact.cu)
+//   deposit  updateDensity (kernels.cu:26-69) at the new position: runs of equal cells are
+//            summed in registers (particles are counting-sorted by cell), then a warp-segmented
+//            reduction and one atomic per node per segment; FP32 or int64 fixed point.
 // The kick + MCC of step k are fused into the pass of step k+1 (the job's kick_pending
 // flag); an explicit flush applies them before any read-back.
 #include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
 #include "particle_ops.cuh"
-#include "tma.cuh"
 
 namespace {
 
@@ -78,57 +77,18 @@ __device__ __forceinline__ void seg_reduce4(T& a, T& b, T& c, T& d, int seg) {
 
 }  // namespace
 
-// Deposit one particle per lane (key = packed cell or CELL_OUT) with a warp-segmented
-// reduction; must be called by all 32 lanes.
-__device__ __forceinline__ void warp_deposit(const JobDev& J, const SlotDev& S, uint32_t key, float fx, float fy) {
-  const int lane = lane_id();
-  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-  const bool head = (lane == 0) || (key != prev);
-  const unsigned heads = __ballot_sync(0xffffffffu, head);
-  const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
-  const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-  const bool valid = key != PIC_CELL_OUT;
-  const int i = cell_i(key), j = cell_j(key);
-  const size_t a = (size_t)j * J.nx + i;
-  if (J.deposit_mode == 0) {
-    const float q = S.qdep;
-    float v0 = valid ? q * w00 : 0.f, v1 = valid ? q * w10 : 0.f, v2 = valid ? q * w01 : 0.f, v3 = valid ? q * w11 : 0.f;
-    seg_reduce4(v0, v1, v2, v3, seg);
-    if (head && valid) {
-      float* rho = J.rho_f;
-      atomicAdd(rho + a, v0);
-      atomicAdd(rho + a + 1, v1);
-      atomicAdd(rho + a + J.nx, v2);
-      atomicAdd(rho + a + J.nx + 1, v3);
-    }
-  } else {
-    const double Q = (double)S.qfix;
-    long long v0 = 0, v1 = 0, v2 = 0, v3 = 0;
-    if (valid) {
-      v0 = __double2ll_rn((double)w00 * Q);
-      v1 = __double2ll_rn((double)w10 * Q);
-      v2 = __double2ll_rn((double)w01 * Q);
-      v3 = S.qfix - v0 - v1 - v2;
-    }
-    seg_reduce4(v0, v1, v2, v3, seg);
-    if (head && valid) {
-      unsigned long long* rho = (unsigned long long*)J.rho_i;
-      atomicAdd(rho + a, (unsigned long long)v0);
-      atomicAdd(rho + a + 1, (unsigned long long)v1);
-      atomicAdd(rho + a + J.nx, (unsigned long long)v2);
-      atomicAdd(rho + a + J.nx + 1, (unsigned long long)v3);
-    }
-  }
-}
-
-// 512-particle chunks and 5 CTAs (40 warps) per SM (47 registers, no spills).  Measured on
-// B200 (1025^2, 2e7 particles): 1024-particle chunks at 2 CTAs per SM take 15% longer than
-// 512 at 4, and 5 CTAs per SM take 3% less than 4 (0.574 against 0.593 ms per pass).
-#ifndef PIC_MOVER_MIN_BLOCKS
-#define PIC_MOVER_MIN_BLOCKS 5
-#endif
-constexpr int kRounds = PIC_CHUNK / PIC_MOVER_THREADS;
+// Particles per lane and per warp work item: lane l of a warp holds particles 4l .. 4l+3 of
+// a 128-particle item in registers, loaded with one 16-byte load per array (512 contiguous
+// bytes per warp and array).  Capacities are multiples of PIC_CHUNK, so every item lies
+// inside the arrays.
+constexpr int kPPL = 4;
+constexpr int kItem = 32 * kPPL;
 constexpr int kWarps = PIC_MOVER_THREADS / 32;
+// CTAs per SM: the pass is limited by how many 16-byte loads are in flight, and 4 particles
+// per lane need ~80 registers, so 3 CTAs (24 warps) per SM.
+#ifndef PIC_MOVER_MIN_BLOCKS
+#define PIC_MOVER_MIN_BLOCKS 3
+#endif
 
 // One real-or-null collision of a null-collision candidate (Vahedi & Surendra 1995): the
 // candidate's process is chosen with u1 * nu_max against the cumulative n sigma_j(E) v.
@@ -210,284 +170,346 @@ __global__ void __launch_bounds__(256) efield32_kernel(const JobDev* __restrict_
   }
 }
 
-// Particle arrays of one chunk staged in shared memory.
-enum { A_CELL = 0, A_FX, A_FY, A_VX, A_VY, A_VZ, A_PID, kNArr };
-constexpr int kChunkBytes = PIC_CHUNK * 4;
-constexpr size_t kMoverDynSmem = 2ull * kNArr * kChunkBytes;
+// The slot and job tables of the slot a warp works on, copied to shared memory when the
+// warp moves to another slot (every parameter read in the per-particle code is then a
+// shared-memory load, and the functions shared with the ionisation kernel take them as is).
+struct WarpTables {
+  SlotDev S;
+  JobDev J;
+};
 
-__device__ __forceinline__ int chunk_slot(const int* __restrict__ chunk_prefix, int nslots, int g) {
-  int lo = 0, hi = nslots - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (chunk_prefix[mid] <= g) lo = mid; else hi = mid - 1;
-  }
-  return lo;
+__device__ __forceinline__ void copy_words(void* dst, const void* src, int bytes, int lane) {
+  int* d = reinterpret_cast<int*>(dst);
+  const int* s = reinterpret_cast<const int*>(src);
+  for (int q = lane; q < bytes / 4; q += 32) d[q] = s[q];
 }
 
-// Issue the bulk copies of chunk g into buffer b (one thread).  vz and pid are staged only
-// for jobs with collisions.
-__device__ __forceinline__ void issue_chunk(const JobDev* __restrict__ jobs, const SlotDev* __restrict__ slots,
-                                            const int* __restrict__ chunk_prefix, int nslots, int g, uint32_t* buf,
-                                            uint64_t* mbar) {
-  const int s = chunk_slot(chunk_prefix, nslots, g);
-  const SlotDev& S = slots[s];
-  const size_t base = (size_t)(g - chunk_prefix[s]) * PIC_CHUNK;
-  const bool mcc = jobs[S.job].mcc_mode != 0 && S.n_proc > 0;
-  tma::mbar_arrive_expect_tx(mbar, (uint32_t)(kChunkBytes * (mcc ? 7 : 5)));
-  tma::bulk_g2s(buf + A_CELL * PIC_CHUNK, S.cell + base, kChunkBytes, mbar);
-  tma::bulk_g2s(buf + A_FX * PIC_CHUNK, S.fx + base, kChunkBytes, mbar);
-  tma::bulk_g2s(buf + A_FY * PIC_CHUNK, S.fy + base, kChunkBytes, mbar);
-  tma::bulk_g2s(buf + A_VX * PIC_CHUNK, S.vx + base, kChunkBytes, mbar);
-  tma::bulk_g2s(buf + A_VY * PIC_CHUNK, S.vy + base, kChunkBytes, mbar);
-  if (mcc) {
-    tma::bulk_g2s(buf + A_VZ * PIC_CHUNK, S.vz + base, kChunkBytes, mbar);
-    tma::bulk_g2s(buf + A_PID * PIC_CHUNK, S.pid + base, kChunkBytes, mbar);
+// Segmented sum of the four corner weights of one run per lane over the warp (runs of equal
+// keys in lane order); the head lane of each segment adds the totals to rho.
+template <typename V>
+__device__ __forceinline__ void warp_runs_deposit(V* rho, int nx, uint32_t key, V v0, V v1, V v2, V v3) {
+  const int lane = lane_id();
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = (lane == 0) || (key != prev);
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
+  const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
+  seg_reduce4(v0, v1, v2, v3, seg);
+  if (head && key != PIC_CELL_OUT) {
+    V* r = rho + (size_t)cell_j(key) * nx + cell_i(key);
+    atomicAdd(r, v0);
+    atomicAdd(r + 1, v1);
+    atomicAdd(r + nx, v2);
+    atomicAdd(r + nx + 1, v3);
   }
 }
 
-// One chunk = PIC_CHUNK particles of one slot; warp w owns the contiguous entries
-// [w * kPerWarp, (w + 1) * kPerWarp), lane l handles w * kPerWarp + r * 32 + l.
-// Chunks reach shared memory through bulk asynchronous copies, double buffered: while the
-// CTA works on chunk k, chunk k+1 is in flight, so HBM latency is covered by the copy engine
-// rather than by resident warps; results return with bulk stores.
-//  pass A  kick and the null-collision candidate test.  E comes from the per-step node field
-//          (float2 loads; particles are cell-sorted, so a warp's loads hit a few cache lines);
-//          candidates (~nu_max dt of the particles) are listed per warp and collided by that
-//          warp's lanes afterwards
-//  pass B  drift, absorption, hit list and CIC deposit
-// Two block barriers per chunk (chunk data ready; results complete before the bulk stores),
-// a third only when the chunk starts a new slot and the slot and job tables are copied to
-// shared memory (every parameter read in the per-particle code is a shared-memory load).
+// CIC weights of one particle (updateDensity, kernels.cu:56-68) in deposit units: FP32, or
+// int64 fixed point whose four parts sum to the particle's quantised charge exactly.
+__device__ __forceinline__ void cic_f32(float q, float fx, float fy, float& a, float& b, float& c, float& d) {
+  a = q * ((1.f - fx) * (1.f - fy)); b = q * (fx * (1.f - fy)); c = q * ((1.f - fx) * fy); d = q * (fx * fy);
+}
+__device__ __forceinline__ void cic_i64(long long qf, float fx, float fy, long long& a, long long& b, long long& c,
+                                        long long& d) {
+  const double Q = (double)qf;
+  a = __double2ll_rn((double)((1.f - fx) * (1.f - fy)) * Q);
+  b = __double2ll_rn((double)(fx * (1.f - fy)) * Q);
+  c = __double2ll_rn((double)((1.f - fx) * fy) * Q);
+  d = qf - a - b - c;
+}
+
+// Deposit of a lane's kPPL particles (keys in lane order): runs of equal keys inside the lane
+// are summed in registers; every finished run but the lane's last goes to rho directly, and
+// the last runs of all lanes go through one warp-segmented reduction.  Called by all lanes.
+template <typename V, typename W>
+__device__ __forceinline__ void lane_deposit(V* rho, int nx, const uint32_t key[kPPL], const float fx[kPPL],
+                                             const float fy[kPPL], W weights) {
+  V a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  uint32_t rk = key[0];
+  if (rk != PIC_CELL_OUT) weights(fx[0], fy[0], a0, a1, a2, a3);
+#pragma unroll
+  for (int k = 1; k < kPPL; ++k) {
+    V b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+    if (key[k] != PIC_CELL_OUT) weights(fx[k], fy[k], b0, b1, b2, b3);
+    if (key[k] == rk) {
+      a0 += b0; a1 += b1; a2 += b2; a3 += b3;
+    } else {
+      if (rk != PIC_CELL_OUT) {
+        V* r = rho + (size_t)cell_j(rk) * nx + cell_i(rk);
+        atomicAdd(r, a0); atomicAdd(r + 1, a1); atomicAdd(r + nx, a2); atomicAdd(r + nx + 1, a3);
+      }
+      rk = key[k]; a0 = b0; a1 = b1; a2 = b2; a3 = b3;
+    }
+  }
+  warp_runs_deposit(rho, nx, rk, a0, a1, a2, a3);
+}
+
+// The fused particle pass.  Warp w of the grid takes items w, w + W, w + 2W, ... (W warps in
+// the grid) over the concatenated items of all active slots; the slot of an item comes from
+// the item prefix, and a warp's items only move forward through the slots.  Per item:
+//   loads    cell, fx, fy, vx, vy (+ vz, pid with collisions): one streaming 16-byte load
+//            per array and lane
+//   pass A   kick (E gathered from the per-step node field; particles are cell-sorted, so a
+//            warp's gathers hit a few cache lines) and the null-collision candidate test;
+//            the item's candidates (~nu_max dt of the particles) are listed in shared memory
+//            by rank and collided warp-cooperatively, 32 per round
+//   pass B   drift, absorption (hits appended with one atomic per item), CIC deposit
+//   stores   streaming 16-byte stores of what changed
+// The particle stream bypasses L2 retention (evict-first loads and stores) so the grids the
+// gathers and deposits touch stay resident.  No block-level synchronisation.
 __global__ void __launch_bounds__(PIC_MOVER_THREADS, PIC_MOVER_MIN_BLOCKS)
 mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
-             const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ chunk_prefix,
+             const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ item_prefix,
              int nslots, int flags, uint32_t explicit_step) {
-  extern __shared__ __align__(128) uint32_t dsm[];
-  constexpr int kPerWarp = PIC_CHUNK / kWarps;
-  __shared__ __align__(8) uint64_t mbar[2];
-  __shared__ int wlist[kWarps][kPerWarp];
-  __shared__ int wcount[kWarps];
-  __shared__ unsigned proc_count[8];
-  __shared__ double ke_sh[kWarps];
-  __shared__ SlotDev sS;
-  __shared__ JobDev sJ;
-  __shared__ int cur_slot;
-  __shared__ int abort_flag;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int wbase = warp * kPerWarp;
-  const int total = chunk_prefix[nslots];
-  if (t == 0) {
-    cur_slot = -1;
-    abort_flag = 0;
-    tma::mbar_init(&mbar[0], 1);
-    tma::mbar_init(&mbar[1], 1);
-    tma::fence_mbar_init();
-  }
-  if (t < 8) proc_count[t] = 0u;
-  __syncthreads();
-  uint32_t parity[2] = {0u, 0u};
-  if (t == 0 && (int)blockIdx.x < total) issue_chunk(jobs, slots, chunk_prefix, nslots, blockIdx.x, dsm, &mbar[0]);
-  int k = 0;
-  for (int g = blockIdx.x; g < total; g += gridDim.x, ++k) {
-    const int b = k & 1;
-    uint32_t* buf = dsm + b * kNArr * PIC_CHUNK;
-    // prefetch the next chunk into the other buffer, once the bulk stores of the chunk that
-    // used it have read their source (every thread finished with that buffer before the
-    // previous iteration's second barrier)
-    if (t == 0 && g + (int)gridDim.x < total) {
-      tma::bulk_wait_read_all();
-      issue_chunk(jobs, slots, chunk_prefix, nslots, g + gridDim.x, dsm + (b ^ 1) * kNArr * PIC_CHUNK, &mbar[b ^ 1]);
+  __shared__ WarpTables tab[kWarps];
+  __shared__ float clist[kWarps][7][32];   // collision candidates of one round: vx vy vz pid cell fx fy
+  __shared__ unsigned pcount[kWarps][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int total = item_prefix[nslots];
+  const SlotDev& S = tab[warp].S;
+  const JobDev& J = tab[warp].J;
+  unsigned* const pc = pcount[warp];
+  if (lane < 8) pc[lane] = 0u;
+  __syncwarp();
+  int cur = -1;
+  double ke = 0.0;
+  bool do_kick = false, do_mcc = false, do_drift = false, do_walls = false, do_dep = false, want_ke = false;
+  uint32_t mcc_step = 0;
+  int n = 0;
+  // kinetic energy and collision counts of the slot a warp leaves go to its job's state
+  auto flush = [&]() {
+    if (cur < 0) return;
+    if (want_ke) {
+      double v = ke;
+#pragma unroll
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0 && v != 0.0) atomicAdd(&st[S.job].ke[S.species], v * S.ke_factor);
     }
-    const int s = chunk_slot(chunk_prefix, nslots, g);
-    if (cur_slot != s) {  // uniform: cur_slot changed before the previous iteration's last barrier
-      __syncthreads();    // thread 0 may still read the old tables for the previous chunk's stores
-      const int* srcS = reinterpret_cast<const int*>(slots + s);
-      const int* srcJ = reinterpret_cast<const int*>(jobs + slots[s].job);
-      int* dS = reinterpret_cast<int*>(&sS);
-      int* dJ = reinterpret_cast<int*>(&sJ);
-      for (int q = t; q < (int)(sizeof(SlotDev) / 4); q += PIC_MOVER_THREADS) dS[q] = srcS[q];
-      for (int q = t; q < (int)(sizeof(JobDev) / 4); q += PIC_MOVER_THREADS) dJ[q] = srcJ[q];
+    ke = 0.0;
+    if (lane < 8) {
+      const unsigned c = pc[lane];
+      if (c) { atomicAdd(&st[S.job].collisions[S.species][lane], (unsigned long long)c); pc[lane] = 0u; }
     }
-    // wait for this chunk's data (bounded)
-    if (!tma::mbar_wait(&mbar[b], parity[b])) atomicOr(&abort_flag, 1);
-    parity[b] ^= 1u;
-    __syncthreads();
-    if (abort_flag) {
-      if (t == 0) atomicOr(&st[slots[s].job].status, PIC_ST_TIMEOUT);
-      break;
+    __syncwarp();
+  };
+  const int nwarps = gridDim.x * kWarps;
+  for (int item = blockIdx.x * kWarps + warp; item < total; item += nwarps) {
+    int s = cur < 0 ? 0 : cur;
+    while (s < nslots - 1 && item_prefix[s + 1] <= item) ++s;
+    if (s != cur) {
+      flush();
+      copy_words(&tab[warp].S, slots + s, sizeof(SlotDev), lane);
+      __syncwarp();
+      copy_words(&tab[warp].J, jobs + S.job, sizeof(JobDev), lane);
+      __syncwarp();
+      cur = s;
+      const JobState& T0 = st[S.job];
+      const bool gated = flags & PIC_PHASE_GATED_I;
+      const bool pending = T0.kick_pending != 0;
+      do_kick = (flags & PIC_PHASE_KICK_I) && (!gated || pending);
+      do_mcc = (flags & PIC_PHASE_MCC_I) && (!gated || pending) && J.mcc_mode != 0 && S.n_proc > 0;
+      do_drift = flags & PIC_PHASE_DRIFT_I;
+      do_walls = (flags & PIC_PHASE_WALLS_I) && J.wall_mode != 0;
+      do_dep = flags & PIC_PHASE_DEPOSIT_I;
+      want_ke = do_kick || do_mcc;
+      mcc_step = gated ? (uint32_t)(T0.step - 1) : explicit_step;
+      n = counts[s];
     }
-    if (t == 0) cur_slot = s;
-    const SlotDev& S = sS;
-    const JobDev& J = sJ;
-    JobState& T = st[S.job];
-    const int n = counts[s];
-    const int base = (g - chunk_prefix[s]) * PIC_CHUNK;
-    const bool gated = flags & PIC_PHASE_GATED_I;
-    const bool pending = T.kick_pending != 0;
-    const bool do_kick = (flags & PIC_PHASE_KICK_I) && (!gated || pending);
-    const bool do_mcc = (flags & PIC_PHASE_MCC_I) && (!gated || pending) && J.mcc_mode != 0 && S.n_proc > 0;
-    const bool do_drift = flags & PIC_PHASE_DRIFT_I;
-    const bool do_walls = (flags & PIC_PHASE_WALLS_I) && J.wall_mode != 0;
-    const bool do_dep = flags & PIC_PHASE_DEPOSIT_I;
-    const uint32_t mcc_step = gated ? (uint32_t)(T.step - 1) : explicit_step;
-    uint32_t* s_cell = buf + A_CELL * PIC_CHUNK;
-    float* s_fx = reinterpret_cast<float*>(buf + A_FX * PIC_CHUNK);
-    float* s_fy = reinterpret_cast<float*>(buf + A_FY * PIC_CHUNK);
-    float* s_vx = reinterpret_cast<float*>(buf + A_VX * PIC_CHUNK);
-    float* s_vy = reinterpret_cast<float*>(buf + A_VY * PIC_CHUNK);
-    float* s_vz = reinterpret_cast<float*>(buf + A_VZ * PIC_CHUNK);
-    const uint32_t* s_pid = buf + A_PID * PIC_CHUNK;
-
+    const int i0 = (item - item_prefix[s]) * kItem + kPPL * lane;
+    // ---- loads
+    uint32_t c[kPPL], pid[kPPL];
+    float fx[kPPL], fy[kPPL], vx[kPPL], vy[kPPL], vz[kPPL];
+    {
+      const uint4 c4 = __ldcs(reinterpret_cast<const uint4*>(S.cell + i0));
+      const float4 x4 = __ldcs(reinterpret_cast<const float4*>(S.fx + i0));
+      const float4 y4 = __ldcs(reinterpret_cast<const float4*>(S.fy + i0));
+      const float4 u4 = __ldcs(reinterpret_cast<const float4*>(S.vx + i0));
+      const float4 w4 = __ldcs(reinterpret_cast<const float4*>(S.vy + i0));
+      c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
+      fx[0] = x4.x; fx[1] = x4.y; fx[2] = x4.z; fx[3] = x4.w;
+      fy[0] = y4.x; fy[1] = y4.y; fy[2] = y4.z; fy[3] = y4.w;
+      vx[0] = u4.x; vx[1] = u4.y; vx[2] = u4.z; vx[3] = u4.w;
+      vy[0] = w4.x; vy[1] = w4.y; vy[2] = w4.z; vy[3] = w4.w;
+      if (do_mcc) {
+        const float4 z4 = __ldcs(reinterpret_cast<const float4*>(S.vz + i0));
+        const uint4 p4 = __ldcs(reinterpret_cast<const uint4*>(S.pid + i0));
+        vz[0] = z4.x; vz[1] = z4.y; vz[2] = z4.z; vz[3] = z4.w;
+        pid[0] = p4.x; pid[1] = p4.y; pid[2] = p4.z; pid[3] = p4.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < kPPL; ++k) { vz[k] = 0.f; pid[k] = 0u; }
+      }
+    }
+    bool valid[kPPL];
+#pragma unroll
+    for (int k = 0; k < kPPL; ++k) valid[k] = i0 + k < n;
     // ---- pass A: kick and collisions
-    if (do_kick || do_mcc) {
+    if (do_kick) {
       const float2* __restrict__ ef = J.efield;
       const int enx = J.nx;
-      if (lane == 0) wcount[warp] = 0;
-      __syncwarp();
+      const float kx = S.kx, ky = S.ky;
 #pragma unroll
-      for (int r = 0; r < kRounds; ++r) {
-        const int q = wbase + r * 32 + lane;
-        const bool valid = base + q < n;
-        bool cand = false;
-        if (valid) {
-          const uint32_t c = s_cell[q];
-          float vx = s_vx[q], vy = s_vy[q];
-          if (do_kick && c != PIC_CELL_OUT) {
-            float gx, gy;
-            const float fx = s_fx[q], fy = s_fy[q];
-            const float2* e0 = ef + cell_j(c) * enx + cell_i(c);
-            const float2 e00 = __ldg(e0), e10 = __ldg(e0 + 1), e01 = __ldg(e0 + enx), e11 = __ldg(e0 + enx + 1);
-            const float w00 = (1.f - fx) * (1.f - fy), w10 = fx * (1.f - fy), w01 = (1.f - fx) * fy, w11 = fx * fy;
-            gx = w00 * e00.x + w10 * e10.x + w01 * e01.x + w11 * e11.x;
-            gy = w00 * e00.y + w10 * e10.y + w01 * e01.y + w11 * e11.y;
-            vx += S.kx * gx;
-            vy += S.ky * gy;
-          }
-          if (do_mcc) {
-            if (J.mcc_mode == 2) {
-              float u[4];
-              draw4(J.seed, s_pid[q], mcc_step, 0u, u);
-              const ProcDev& P = J.procs[S.first_proc];
-              const float v2 = vx * vx + vy * vy;
-              const float sp = sqrtf(v2);
-              const float Pc = 1.f - expf(-J.gas_density * xs_lookup(P, S.half_m_over_e * v2) * sp * J.dt);
-              if (u[0] < Pc) {
-                float sn, cs;
-                sincospif(2.f * u[1], &sn, &cs);
-                vx = sp * cs; vy = sp * sn;
-                atomicAdd(&proc_count[0], 1u);
-              }
-            } else {
-              cand = draw_first(J.seed, s_pid[q], mcc_step, 0u) < S.pnull;
+      for (int k = 0; k < kPPL; ++k)
+        if (valid[k] && c[k] != PIC_CELL_OUT) {
+          const float2* e0 = ef + cell_j(c[k]) * enx + cell_i(c[k]);
+          const float2 e00 = __ldg(e0), e10 = __ldg(e0 + 1), e01 = __ldg(e0 + enx), e11 = __ldg(e0 + enx + 1);
+          const float x = fx[k], y = fy[k];
+          const float w00 = (1.f - x) * (1.f - y), w10 = x * (1.f - y), w01 = (1.f - x) * y, w11 = x * y;
+          const float gx = w00 * e00.x + w10 * e10.x + w01 * e01.x + w11 * e11.x;
+          const float gy = w00 * e00.y + w10 * e10.y + w01 * e01.y + w11 * e11.y;
+          vx[k] += kx * gx;
+          vy[k] += ky * gy;
+        }
+    }
+    if (do_mcc) {
+      if (J.mcc_mode == 2) {
+        const ProcDev& P = J.procs[S.first_proc];
+#pragma unroll
+        for (int k = 0; k < kPPL; ++k)
+          if (valid[k]) {
+            float u[4];
+            draw4(J.seed, pid[k], mcc_step, 0u, u);
+            const float v2 = vx[k] * vx[k] + vy[k] * vy[k];
+            const float sp = sqrtf(v2);
+            const float Pc = 1.f - expf(-J.gas_density * xs_lookup(P, S.half_m_over_e * v2) * sp * J.dt);
+            if (u[0] < Pc) {
+              float sn, cs;
+              sincospif(2.f * u[1], &sn, &cs);
+              vx[k] = sp * cs; vy[k] = sp * sn;
+              atomicAdd(&pc[0], 1u);
             }
           }
-          s_vx[q] = vx;
-          s_vy[q] = vy;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, cand);
-        if (cand) wlist[warp][wcount[warp] + __popc(m & ((1u << lane) - 1u))] = q;
-        __syncwarp();
-        if (lane == 0) wcount[warp] += __popc(m);
-        __syncwarp();
-      }
-      const int ncand = wcount[warp];
-      for (int c = lane; c < ncand; c += 32) {
-        const int q = wlist[warp][c];
-        float u[4];
-        const uint32_t pid = s_pid[q];
-        draw4(J.seed, pid, mcc_step, 0u, u);
-        float vx = s_vx[q], vy = s_vy[q], vz = s_vz[q];
-        collide(J, S, slots, T, pid, s_cell[q], s_fx[q], s_fy[q], vx, vy, vz, u, mcc_step, proc_count);
-        s_vx[q] = vx; s_vy[q] = vy; s_vz[q] = vz;
-      }
-      __syncwarp();
-    }
-
-    // ---- pass B: drift, walls, deposit
-    double ke = 0.0;
-    const bool want_ke = do_kick || do_mcc;
-    if (do_drift || do_dep || want_ke) {
+      } else {
+        bool cand[kPPL];
+        unsigned m[kPPL];
+        int before[kPPL];
+        int ncand = 0;
 #pragma unroll
-      for (int r = 0; r < kRounds; ++r) {
-        const int q = wbase + r * 32 + lane;
-        const bool valid = base + q < n;
-        uint32_t c = PIC_CELL_OUT;
-        float fx = 0.f, fy = 0.f, vx = 0.f, vy = 0.f;
-        if (valid) { c = s_cell[q]; fx = s_fx[q]; fy = s_fy[q]; vx = s_vx[q]; vy = s_vy[q]; }
-        if (valid && want_ke) {
-          const float vz = do_mcc ? s_vz[q] : 0.f;
-          ke += (double)(vx * vx + vy * vy + vz * vz);
+        for (int k = 0; k < kPPL; ++k) {
+          cand[k] = valid[k] && draw_first(J.seed, pid[k], mcc_step, 0u) < S.pnull;
+          m[k] = __ballot_sync(0xffffffffu, cand[k]);
+          before[k] = ncand;
+          ncand += __popc(m[k]);
         }
-        bool absorbed = false;
-        uint32_t nc = c;
-        float nfx = fx, nfy = fy;
-        if (do_drift && valid) {
-          const Drifted d = drift_particle(J, S, c, fx, fy, vx, vy, do_walls);
-          absorbed = d.absorbed; nc = d.cell; nfx = d.fx; nfy = d.fy;
+        // rank of candidate (lane, k): item order k-major, then lane
+        int rank[kPPL];
+#pragma unroll
+        for (int k = 0; k < kPPL; ++k) rank[k] = before[k] + __popc(m[k] & ((1u << lane) - 1u));
+        JobState& T = st[S.job];
+        for (int r0 = 0; r0 < ncand; r0 += 32) {
+#pragma unroll
+          for (int k = 0; k < kPPL; ++k)
+            if (cand[k] && rank[k] >= r0 && rank[k] < r0 + 32) {
+              const int q = rank[k] - r0;
+              clist[warp][0][q] = vx[k]; clist[warp][1][q] = vy[k]; clist[warp][2][q] = vz[k];
+              clist[warp][3][q] = __uint_as_float(pid[k]); clist[warp][4][q] = __uint_as_float(c[k]);
+              clist[warp][5][q] = fx[k]; clist[warp][6][q] = fy[k];
+            }
+          __syncwarp();
+          if (r0 + lane < ncand) {
+            float cvx = clist[warp][0][lane], cvy = clist[warp][1][lane], cvz = clist[warp][2][lane];
+            const uint32_t cpid = __float_as_uint(clist[warp][3][lane]);
+            float u[4];
+            draw4(J.seed, cpid, mcc_step, 0u, u);
+            collide(J, S, slots, T, cpid, __float_as_uint(clist[warp][4][lane]), clist[warp][5][lane],
+                    clist[warp][6][lane], cvx, cvy, cvz, u, mcc_step, pc);
+            clist[warp][0][lane] = cvx; clist[warp][1][lane] = cvy; clist[warp][2][lane] = cvz;
+          }
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < kPPL; ++k)
+            if (cand[k] && rank[k] >= r0 && rank[k] < r0 + 32) {
+              const int q = rank[k] - r0;
+              vx[k] = clist[warp][0][q]; vy[k] = clist[warp][1][q]; vz[k] = clist[warp][2][q];
+            }
+          __syncwarp();
         }
-        if (do_walls) {
-          const int hslot = warp_append(valid && absorbed, hit_counts + s);
-          if (hslot >= 0) S.hits[hslot] = base + q;
-        }
-        if (do_dep) warp_deposit(J, S, (valid && !absorbed) ? nc : PIC_CELL_OUT, nfx, nfy);
-        if (valid && do_drift) { s_cell[q] = nc; s_fx[q] = nfx; s_fy[q] = nfy; }
       }
     }
-    // ---- results back to global memory with bulk stores
-    tma::fence_proxy_async();
     if (want_ke) {
-      for (int o = 16; o; o >>= 1) ke += __shfl_down_sync(0xffffffffu, ke, o);
-      if (lane == 0) ke_sh[warp] = ke;
+#pragma unroll
+      for (int k = 0; k < kPPL; ++k)
+        if (valid[k]) ke += (double)(vx[k] * vx[k] + vy[k] * vy[k] + vz[k] * vz[k]);
     }
-    __syncthreads();
-    if (t == 0) {
-      if (do_drift) {
-        tma::bulk_s2g(S.cell + base, s_cell, kChunkBytes);
-        tma::bulk_s2g(S.fx + base, s_fx, kChunkBytes);
-        tma::bulk_s2g(S.fy + base, s_fy, kChunkBytes);
-      }
-      if (do_kick || do_mcc) {
-        tma::bulk_s2g(S.vx + base, s_vx, kChunkBytes);
-        tma::bulk_s2g(S.vy + base, s_vy, kChunkBytes);
-      }
-      if (do_mcc) tma::bulk_s2g(S.vz + base, s_vz, kChunkBytes);
-      tma::bulk_commit();
-      if (want_ke) {
-        double tk = 0.0;
-        for (int w = 0; w < kWarps; ++w) tk += ke_sh[w];
-        if (tk != 0.0) atomicAdd(&T.ke[S.species], tk * S.ke_factor);
-      }
-      // read and clear the collision counters; the next chunk's collisions start after its
-      // first barrier, which thread 0 reaches only after this
-      for (int p = 0; p < 8; ++p) {
-        const unsigned c = proc_count[p];
-        if (c) {
-          atomicAdd(&T.collisions[S.species][p], (unsigned long long)c);
-          proc_count[p] = 0u;
-        }
+    // ---- pass B: drift, walls, deposit
+    uint32_t key[kPPL];
+    bool absorbed[kPPL];
+#pragma unroll
+    for (int k = 0; k < kPPL; ++k) {
+      absorbed[k] = false;
+      key[k] = valid[k] ? c[k] : PIC_CELL_OUT;
+      if (do_drift && valid[k]) {
+        const Drifted d = drift_particle(J, S, c[k], fx[k], fy[k], vx[k], vy[k], do_walls);
+        absorbed[k] = d.absorbed; c[k] = d.cell; fx[k] = d.fx; fy[k] = d.fy;
+        key[k] = d.absorbed ? PIC_CELL_OUT : d.cell;
       }
     }
+    if (do_walls) {
+      unsigned hm[kPPL];
+      int nh = 0, hb[kPPL];
+#pragma unroll
+      for (int k = 0; k < kPPL; ++k) {
+        hm[k] = __ballot_sync(0xffffffffu, valid[k] && absorbed[k]);
+        hb[k] = nh;
+        nh += __popc(hm[k]);
+      }
+      if (nh) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(hit_counts + s, nh);
+        base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+        for (int k = 0; k < kPPL; ++k)
+          if (valid[k] && absorbed[k]) S.hits[base + hb[k] + __popc(hm[k] & ((1u << lane) - 1u))] = i0 + k;
+      }
+    }
+    if (do_dep) {
+      if (J.deposit_mode == 0) {
+        const float q = S.qdep;
+        lane_deposit<float>(J.rho_f, J.nx, key, fx, fy,
+                            [q](float x, float y, float& a, float& b, float& cc, float& d) { cic_f32(q, x, y, a, b, cc, d); });
+      } else {
+        const long long qf = S.qfix;
+        lane_deposit<unsigned long long>(
+            reinterpret_cast<unsigned long long*>(J.rho_i), J.nx, key, fx, fy,
+            [qf](float x, float y, unsigned long long& a, unsigned long long& b, unsigned long long& cc,
+                 unsigned long long& d) {
+              long long a_, b_, c_, d_;
+              cic_i64(qf, x, y, a_, b_, c_, d_);
+              a = (unsigned long long)a_; b = (unsigned long long)b_; cc = (unsigned long long)c_;
+              d = (unsigned long long)d_;
+            });
+      }
+    }
+    // ---- stores
+    if (do_drift) {
+      __stcs(reinterpret_cast<uint4*>(S.cell + i0), make_uint4(c[0], c[1], c[2], c[3]));
+      __stcs(reinterpret_cast<float4*>(S.fx + i0), make_float4(fx[0], fx[1], fx[2], fx[3]));
+      __stcs(reinterpret_cast<float4*>(S.fy + i0), make_float4(fy[0], fy[1], fy[2], fy[3]));
+    }
+    if (do_kick || do_mcc) {
+      __stcs(reinterpret_cast<float4*>(S.vx + i0), make_float4(vx[0], vx[1], vx[2], vx[3]));
+      __stcs(reinterpret_cast<float4*>(S.vy + i0), make_float4(vy[0], vy[1], vy[2], vy[3]));
+    }
+    if (do_mcc) __stcs(reinterpret_cast<float4*>(S.vz + i0), make_float4(vz[0], vz[1], vz[2], vz[3]));
   }
-  if (t == 0) tma::bulk_wait_all();
+  flush();
 }
 
-// Exclusive prefix of mover chunks per slot (one CTA; slots are few).
+// Exclusive prefix of mover work items (kItem particles) per active slot.
 __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t* __restrict__ active,
                                    int* __restrict__ chunk_prefix, int nslots) {
   if (threadIdx.x == 0) {
     int a = 0;
     for (int s = 0; s < nslots; ++s) {
       chunk_prefix[s] = a;
-      if (!active || active[s]) a += (counts[s] + PIC_CHUNK - 1) / PIC_CHUNK;
+      if (!active || active[s]) a += (counts[s] + kItem - 1) / kItem;
     }
     chunk_prefix[nslots] = a;
   }
 }
 
 int mover_blocks_per_sm() {
-  cudaFuncSetAttribute(mover_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMoverDynSmem);
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, kMoverDynSmem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, 0) != cudaSuccess ||
       b < 1) {
     cudaGetLastError();
     b = 1;
@@ -505,7 +527,7 @@ int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaS
   }
   chunk_table_kernel<<<1, 32, 0, stream>>>(L.counts, L.active, L.chunk_prefix, L.nslots);
   if (L.ev_mover_begin) cudaEventRecord(L.ev_mover_begin, stream);
-  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, kMoverDynSmem, stream>>>(L.jobs, L.st, L.slots, L.counts,
+  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, 0, stream>>>(L.jobs, L.st, L.slots, L.counts,
                                                                           L.hit_counts, L.chunk_prefix, L.nslots, flags,
                                                                           explicit_step);
   if (L.ev_mover_end) cudaEventRecord(L.ev_mover_end, stream);
