@@ -67,7 +67,7 @@ def job_config(spec: JobSpec, sort_every: int = 10) -> L.JobConfig:
     w = N0 * spec.L * spec.L / spec.n_per_species
     return cf.make_config(spec.n, spec.L, 1e-11, [(-cf.QE, cf.ME, w, cap), (cf.QE, cf.M_AR, w, cap)],
                           tol=spec.tol, deposit=spec.deposit, sort_every=sort_every, seed=spec.seed,
-                          mcc=cf.argon_mcc(spec.density), warm_start=1)
+                          mcc=cf.argon_mcc(spec.density), warm_start=1, omega=cf.MG_OMEGA_1E9)
 
 
 def bytes_needed(cfg: L.JobConfig) -> int:
