@@ -243,6 +243,9 @@ struct pic_engine {
   // V-cycle, bound by that one SM's shared-memory bandwidth (7 accesses per node and
   // half-sweep), against about 16 us for 129^2 as two tile launches plus 65^2 .. 3^2 in one CTA.
   int coarse_top = 65;
+  // Programmatic dependent launches between the V-cycle's kernels (PIC_PDL=0 turns them off;
+  // they are also dropped if a step graph with them cannot be built).
+  bool pdl = true;
   int levels_kernel = 0;      // multigrid levels 1..lc as one cooperative launch
   size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
@@ -407,6 +410,7 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   M.coarse_smem = coarse_smem;
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
+  M.pdl = E->pdl ? 1 : 0;
   M.fast_nu_pre = (!ids.empty() && nu_pre_min == nu_pre_max) ? nu_pre_max : -1;
   M.fast_nu_post = (!ids.empty() && nu_post_min == nu_post_max) ? nu_post_max : -1;
   // Levels 1..lc as phases of one cooperative launch (PIC_OPT_MG_LEVELS_KERNEL).  Measured on
@@ -665,8 +669,18 @@ int ensure_graphs(pic_engine* E) {
   if (E->graph_exec) { cudaGraphExecDestroy(E->graph_exec); E->graph_exec = nullptr; }
   if (E->graph_exec_sort) { cudaGraphExecDestroy(E->graph_exec_sort); E->graph_exec_sort = nullptr; }
   int rc = build_step_graph(E, false, &E->graph_exec, &E->graph_fixed_launches[0]);
-  if (rc) return rc;
-  rc = build_step_graph(E, true, &E->graph_exec_sort, &E->graph_fixed_launches[1]);
+  if (rc == PIC_OK) rc = build_step_graph(E, true, &E->graph_exec_sort, &E->graph_fixed_launches[1]);
+  if (rc && E->pdl) {
+    // a graph with programmatic dependencies inside the V-cycle body could not be built:
+    // rebuild the multigrid plan and the graphs with ordinary launches
+    if (E->graph_exec) { cudaGraphExecDestroy(E->graph_exec); E->graph_exec = nullptr; }
+    E->pdl = false;
+    E->mg_dirty = true;
+    for (auto& J : E->jobs) J.mg.valid = false;
+    rc = ensure_mg_all(E);
+    if (rc == PIC_OK) rc = build_step_graph(E, false, &E->graph_exec, &E->graph_fixed_launches[0]);
+    if (rc == PIC_OK) rc = build_step_graph(E, true, &E->graph_exec_sort, &E->graph_fixed_launches[1]);
+  }
   if (rc) return rc;
   E->graph_dirty = false;
   return PIC_OK;
@@ -723,6 +737,7 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
     else if (mg_cluster_supported(8, s8) > 0) { E->cluster_C = 8; E->cluster_smem_max = s8; }
     if (const char* v = std::getenv("PIC_MG_CLUSTER_TOP")) E->cluster_top = std::atoi(v);
     if (const char* v = std::getenv("PIC_MG_COARSE_TOP")) E->coarse_top = std::atoi(v);
+    if (const char* v = std::getenv("PIC_PDL")) E->pdl = std::atoi(v) != 0;
     if (const char* v = std::getenv("PIC_MG_LEVELS_KERNEL")) E->levels_kernel = std::atoi(v) == 1;
   }
   const int nslots = kMaxJobs * kSlotsPerJob;

@@ -69,6 +69,7 @@ struct MgLaunch {
   size_t coarse_smem;
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
   int fast_nu_pre, fast_nu_post;                         // smoothing counts shared by every job, else -1
+  int pdl;                                               // programmatic dependent launches in the V-cycle
   int levels_grid;                                       // >0: levels 1..lc in one cooperative launch
   size_t levels_smem, levels_quarter_floats;
 };

@@ -518,6 +518,7 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   // the layout is a multiple of 4 floats, 16-byte aligned
   for (int k = t; k < total / 4; k += T) reinterpret_cast<float4*>(sm)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
+  tma::pdl_wait();
   coarse_load(sm + lv[lc].off + lv[lc].n * (lv[lc].n + 1), f_top, lv[lc].n);
   __syncthreads();
   for (int l = lc; l < L - 1; ++l) {
@@ -537,6 +538,7 @@ __global__ void __launch_bounds__(kCoarseThreads) mg_coarse_kernel(const int* __
                                                                    const JobDev* __restrict__ jobs,
                                                                    const JobState* __restrict__ st) {
   extern __shared__ __align__(16) float sm[];
+  tma::pdl_trigger();
   coarse_solve(job_list[blockIdx.x], jobs, st, sm);
 }
 
@@ -787,6 +789,8 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
   constexpr int NL = (W * W + NT - 1) / NT;
   __shared__ __align__(16) float e[W * P];
   __shared__ __align__(16) float f[W * P];
+  tma::pdl_trigger();
+  // tile, job and job-state fields: none of them is written by the previous level's launch
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   const JobState& T = st[tr.job];
@@ -801,6 +805,7 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
   float* const fc = J.f[l + 1];
   const float omega = J.omega;
   const int t = threadIdx.x;
+  tma::pdl_wait();
 #pragma unroll
   for (int u = 0; u < NL; ++u) {
     const int q = t + u * NT;
@@ -868,6 +873,9 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   __shared__ __align__(16) float cs[CW * CP];
   __shared__ __align__(16) double P64[MODE ? PW * PW : 1];
   __shared__ __align__(16) double RH[MODE ? kTU * kTU : 1];   // rho of the owned nodes, raw
+  tma::pdl_trigger();
+  // tile, job and job-state fields: within a V-cycle only this kernel's own last CTA (level 0)
+  // writes the state, so they are read before waiting for the previous launch
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
@@ -896,6 +904,7 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   const double tol = J.tol;
   const int max_cycles = J.max_cycles;
   const int t = threadIdx.x;
+  tma::pdl_wait();
   // ---- one batch of asynchronous copies
 #pragma unroll
   for (int u = 0; u < NL; ++u) {
@@ -1018,37 +1027,53 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   }
 }
 
-template <int NU>
-void launch_down_fast(int grid, bool wide, const TileRef* tiles, const JobDev* jobs, const JobState* st, int l,
-                      cudaStream_t s) {
-  if (wide) mg_down_fast_kernel<NU, 1024><<<grid, 1024, 0, s>>>(tiles, jobs, st, l);
-  else mg_down_fast_kernel<NU, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l);
+// Launch with optional programmatic stream serialisation (the kernel may start while the
+// previous launch in the stream finishes; it waits in tma::pdl_wait before reading its output).
+template <typename... KArgs, typename... Args>
+void launch_k(void (*k)(KArgs...), int grid, int block, size_t smem, bool pdl, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k, args...);
 }
 template <int NU>
-void launch_up_fast(int grid, bool wide, const TileRef* tiles, const JobDev* jobs, JobState* st, int l, int mode,
-                    int* running, cudaStream_t s) {
-  if (mode == 1) mg_up_fast_kernel<NU, 1, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l, running);
-  else if (wide) mg_up_fast_kernel<NU, 0, 1024><<<grid, 1024, 0, s>>>(tiles, jobs, st, l, running);
-  else mg_up_fast_kernel<NU, 0, 256><<<grid, 256, 0, s>>>(tiles, jobs, st, l, running);
+void launch_down_fast(int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, const JobState* st,
+                      int l, cudaStream_t s) {
+  if (wide) launch_k(mg_down_fast_kernel<NU, 1024>, grid, 1024, 0, pdl, s, tiles, jobs, st, l);
+  else launch_k(mg_down_fast_kernel<NU, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l);
 }
-void down_fast(int nu, int grid, bool wide, const TileRef* tiles, const JobDev* jobs, const JobState* st, int l,
-               cudaStream_t s) {
+template <int NU>
+void launch_up_fast(int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, JobState* st, int l,
+                    int mode, int* running, cudaStream_t s) {
+  if (mode == 1) launch_k(mg_up_fast_kernel<NU, 1, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l, running);
+  else if (wide) launch_k(mg_up_fast_kernel<NU, 0, 1024>, grid, 1024, 0, pdl, s, tiles, jobs, st, l, running);
+  else launch_k(mg_up_fast_kernel<NU, 0, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l, running);
+}
+void down_fast(int nu, int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, const JobState* st,
+               int l, cudaStream_t s) {
   switch (nu) {
-    case 0: launch_down_fast<0>(grid, wide, tiles, jobs, st, l, s); break;
-    case 1: launch_down_fast<1>(grid, wide, tiles, jobs, st, l, s); break;
-    case 2: launch_down_fast<2>(grid, wide, tiles, jobs, st, l, s); break;
-    case 3: launch_down_fast<3>(grid, wide, tiles, jobs, st, l, s); break;
-    default: launch_down_fast<4>(grid, wide, tiles, jobs, st, l, s); break;
+    case 0: launch_down_fast<0>(grid, wide, pdl, tiles, jobs, st, l, s); break;
+    case 1: launch_down_fast<1>(grid, wide, pdl, tiles, jobs, st, l, s); break;
+    case 2: launch_down_fast<2>(grid, wide, pdl, tiles, jobs, st, l, s); break;
+    case 3: launch_down_fast<3>(grid, wide, pdl, tiles, jobs, st, l, s); break;
+    default: launch_down_fast<4>(grid, wide, pdl, tiles, jobs, st, l, s); break;
   }
 }
-void up_fast(int nu, int grid, bool wide, const TileRef* tiles, const JobDev* jobs, JobState* st, int l, int mode,
-             int* running, cudaStream_t s) {
+void up_fast(int nu, int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, JobState* st, int l,
+             int mode, int* running, cudaStream_t s) {
   switch (nu) {
-    case 0: launch_up_fast<0>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
-    case 1: launch_up_fast<1>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
-    case 2: launch_up_fast<2>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
-    case 3: launch_up_fast<3>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
-    default: launch_up_fast<4>(grid, wide, tiles, jobs, st, l, mode, running, s); break;
+    case 0: launch_up_fast<0>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
+    case 1: launch_up_fast<1>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
+    case 2: launch_up_fast<2>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
+    case 3: launch_up_fast<3>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
+    default: launch_up_fast<4>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
   }
 }
 
@@ -1156,26 +1181,32 @@ int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coa
 
 // Tile launches of one level: the compile-time-shape kernels when every job of the launch
 // has the same smoothing count (<= kMaxFastNu), else the generic ones.
-// 1024-thread CTAs where a level has at most two tiles per SM.
-static void launch_down(const MgLaunch& M, int l, const EngineLaunch& L, cudaStream_t s) {
-  if (M.fast_nu_pre >= 0 && M.fast_nu_pre <= kMaxFastNu)
-    down_fast(M.fast_nu_pre, M.n_down[l], M.n_down[l] <= 2 * L.num_sms, M.down_tiles[l], L.jobs, L.st, l, s);
-  else
-    mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l);
+// 1024-thread CTAs where a level has at most two tiles per SM.  pdl: the launch follows a
+// kernel of the V-cycle that this one's prologue may overlap (programmatic serialisation).
+static bool launch_down(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl, cudaStream_t s) {
+  if (M.fast_nu_pre >= 0 && M.fast_nu_pre <= kMaxFastNu) {
+    down_fast(M.fast_nu_pre, M.n_down[l], M.n_down[l] <= 2 * L.num_sms, pdl && M.pdl, M.down_tiles[l], L.jobs, L.st,
+              l, s);
+    return true;
+  }
+  mg_down_kernel<<<M.n_down[l], 256, down_smem(M.nu_pre_max), s>>>(M.down_tiles[l], L.jobs, L.st, l);
+  return false;
 }
-static void launch_up(const MgLaunch& M, int l, const EngineLaunch& L, cudaStream_t s) {
-  if (M.fast_nu_post >= 0 && M.fast_nu_post <= kMaxFastNu)
-    up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= 2 * L.num_sms, M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
-            L.running, s);
-  else
-    mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
-                                                                L.running);
+static bool launch_up(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl, cudaStream_t s) {
+  if (M.fast_nu_post >= 0 && M.fast_nu_post <= kMaxFastNu) {
+    up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= 2 * L.num_sms, pdl && M.pdl, M.up_tiles[l], L.jobs, L.st, l,
+            l == 0 ? 1 : 0, L.running, s);
+    return true;
+  }
+  mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
+                                                              L.running);
+  return false;
 }
 
 int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   int k = 0;
   if (M.levels_grid > 0 && M.max_depth >= 2 && !M.n_cluster) {
-    if (M.n_down[0]) { launch_down(M, 0, L, s); ++k; }
+    if (M.n_down[0]) { launch_down(M, 0, L, false, s); ++k; }
     MgLevelsArgs a{};
     for (int l = 0; l < PIC_MAX_LEVELS; ++l) {
       a.down_tiles[l] = M.down_tiles[l]; a.n_down[l] = M.n_down[l];
@@ -1198,16 +1229,24 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, mg_levels_kernel, a);
     ++k;
-    if (M.n_up[0]) { launch_up(M, 0, L, s); ++k; }
+    if (M.n_up[0]) { launch_up(M, 0, L, false, s); ++k; }
     if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
     return k;
   }
+  // every launch after the first may overlap its predecessor when both are compile-time-shape
+  // kernels (they wait for the predecessor's output in tma::pdl_wait)
+  bool prev_fast = false;
   for (int l = 0; l < M.max_depth; ++l)
-    if (M.n_down[l]) { launch_down(M, l, L, s); ++k; }
-  if (M.n_coarse) { mg_coarse_kernel<<<M.n_coarse, kCoarseThreads, M.coarse_smem, s>>>(M.coarse_jobs, L.jobs, L.st); ++k; }
-  if (M.n_cluster) k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s);
+    if (M.n_down[l]) { prev_fast = launch_down(M, l, L, prev_fast, s); ++k; }
+  if (M.n_coarse) {
+    launch_k(mg_coarse_kernel, M.n_coarse, kCoarseThreads, M.coarse_smem, prev_fast && M.pdl, s, M.coarse_jobs,
+             L.jobs, L.st);
+    prev_fast = true;
+    ++k;
+  }
+  if (M.n_cluster) { k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s); prev_fast = false; }
   for (int l = M.max_depth - 1; l >= 0; --l)
-    if (M.n_up[l]) { launch_up(M, l, L, s); ++k; }
+    if (M.n_up[l]) { prev_fast = launch_up(M, l, L, prev_fast, s); ++k; }
   if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
   return k;
 }

@@ -83,4 +83,11 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialisation may
+// start while its predecessor in the stream is still running: it must call pdl_wait() before
+// reading anything the predecessor writes.  pdl_trigger() lets the successor launch once every
+// CTA of this kernel has called it (or exited).  Both are no-ops for ordinary launches.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace tma
