@@ -246,6 +246,7 @@ struct pic_engine {
   // Programmatic dependent launches between the V-cycle's kernels (PIC_PDL=0 turns them off;
   // they are also dropped if a step graph with them cannot be built).
   bool pdl = true;
+  int last_solve_cycles = 1;  // V-cycles the last stream-ordered solve ran (speculation depth)
   int levels_kernel = 0;      // multigrid levels 1..lc as one cooperative launch
   size_t cluster_smem_max = 0;
   int64_t pool_bytes = 0, used_bytes = 0;
@@ -445,18 +446,25 @@ int ensure_mg_all(pic_engine* E) {
   return PIC_OK;
 }
 
-// Field solve: init residual, then V-cycles until every job stopped (host read-back).
+// Field solve: init residual, then V-cycles until every job stopped.  The first cycles go
+// out without a host check (one fewer than the last solve needed: a converged job's kernels
+// return at once, so a spare cycle costs launches only); after them the host reads the
+// running-job count back after every cycle.
 int solve(pic_engine* E, const MgBuild& B, const uint8_t* active, cudaStream_t s) {
   if (!B.valid) return PIC_OK;
   EngineLaunch L = make_launch(E, active);
   E->launches += launch_mg_init(L, B.L, s);
-  for (int c = 0; c < B.max_cycles; ++c) {
+  const int unchecked = std::max(1, std::min(E->last_solve_cycles - 1, B.max_cycles));
+  int c = 0;
+  for (; c < B.max_cycles; ++c) {
     E->launches += launch_mg_vcycle(L, B.L, s);
     E->vcycles++;
+    if (c + 1 < unchecked) continue;
     CK(cudaMemcpyAsync(E->h_pinned, E->d_running, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (*E->h_pinned <= 0) break;
   }
+  E->last_solve_cycles = std::min(c + 1, B.max_cycles);
   CK(cudaGetLastError());
   return PIC_OK;
 }

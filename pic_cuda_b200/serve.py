@@ -29,8 +29,13 @@ class Request:
     index: int = 0
 
 
+# Aggregate particle-steps/s of one B200 on the batched mix (measured: 2.1e10), rounded up, so
+# that the default arrival rate keeps the GPU saturated.
+B200_CAPACITY = 2.5e10
+
+
 def served_requests(n_requests: int = 2000, seed: int = 5, ppc_scale: float = 1.0, steps_scale: float = 1.0,
-                    rate: float | None = None, saturation: float = 1.5, capacity: float = 1.2e10,
+                    rate: float | None = None, saturation: float = 1.5, capacity: float = B200_CAPACITY,
                     deposit: int = L.DEPOSIT_F32) -> list[Request]:
     """Seeded request stream.  Without an explicit rate (requests/s), the Poisson rate is
     `saturation` times what a GPU of `capacity` particle-steps/s can serve on average."""
@@ -82,9 +87,11 @@ class Server:
     max_jobs: int = 4096
     device: object = None
     keep_results: bool = False
-    # CUDA-graph steps (rebuilt whenever the job set changes).  Measured on B200 with 32 mixed
-    # requests: 8.3e9 particle-steps/s against 7.5e9 with stream-ordered steps.
-    use_graph: bool = True
+    # Stream-ordered steps by default: the job set changes every quantum or two, and a CUDA
+    # graph would be rebuilt each time.  Measured on B200 (64 requests, ppc x 0.05, steps x 0.1):
+    # graphs on every quantum 7.5e9 particle-steps/s, graphs once the set was stable for a
+    # quantum 7.6e9, stream-ordered always 11.2e9.  With use_graph the stable quanta use graphs.
+    use_graph: bool = False
     clock: object = time.perf_counter
     sleep: object = time.sleep
     log: list = field(default_factory=list)
@@ -108,6 +115,7 @@ class Server:
         t0 = self.clock()
         particle_steps = 0.0
         spent = {"admit": 0.0, "step": 0.0, "complete": 0.0, "idle": 0.0}
+        changed = True   # the job set differs from the last quantum's
         while pending or active:
             now = self.clock() - t0
             while pending and pending[0].arrival <= now and len(active) < self.max_jobs:
@@ -119,6 +127,7 @@ class Server:
                 job = self._admit(req, now)
                 spent["admit"] += self.clock() - ta
                 used += need
+                changed = True
                 active.append([req, job, req.spec.steps, need, self.clock() - t0])
                 self.log.append(("admit", req.index, self.clock() - t0, len(active), used))
             if not active:
@@ -128,8 +137,9 @@ class Server:
                 continue
             k = min(self.quantum, min(a[2] for a in active))
             ts = self.clock()
-            (self.engine.step_graph if self.use_graph else self.engine.step)(k)
+            (self.engine.step_graph if self.use_graph and not changed else self.engine.step)(k)
             self.engine.sync()
+            changed = False
             spent["step"] += self.clock() - ts
             particle_steps += k * sum(2.0 * a[0].spec.n_per_species for a in active)
             tc = self.clock()
@@ -142,6 +152,7 @@ class Server:
                     res = self._result(job)
                     job.destroy()
                     used -= a[3]
+                    changed = True
                     done.append(Completion(req.index, req.arrival, a[4], self.clock() - t0, diag, res))
                     self.log.append(("done", req.index, self.clock() - t0, len(active) - 1, used))
                 else:

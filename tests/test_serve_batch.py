@@ -36,7 +36,7 @@ def test_request_stream():
     assert d.min() >= 20 and d.max() <= 22
     # offered load is about 1.5x the assumed capacity
     work = sum(r.spec.particle_steps for r in reqs)
-    assert 0.8 < work / t[-1] / (1.5 * 1.2e10) < 1.25
+    assert 0.8 < work / t[-1] / (1.5 * serve.B200_CAPACITY) < 1.25
 
 
 def test_fifo_replay():
