@@ -366,10 +366,20 @@ __device__ __forceinline__ ColMap col_map(int t, int T, int m, float rm) {
   return c;
 }
 
+// Barrier of the threads working on a level: the whole CTA, or (SMALL) the first
+// kCoarseSmallThreads threads on hardware barrier 1 while the rest wait further on.
+constexpr int kCoarseSmallThreads = 128;
+constexpr int kCoarseSmallSide = 17;   // levels this small run on kCoarseSmallThreads threads
+template <bool SMALL>
+__device__ __forceinline__ void level_sync() {
+  if (SMALL) asm volatile("bar.sync 1, %0;" ::"n"(kCoarseSmallThreads) : "memory");
+  else __syncthreads();
+}
+
 // nu red-black SOR sweeps (colour (i+j) odd first, Multigrid.cu:246-265) on the interior of
-// level L (row pitch n + 1) by the CTA's T threads.  ZERO: e enters as +0 everywhere
-// (pre-smoothing), so the first half-sweep reads no neighbours.
-template <bool ZERO = false>
+// level L (row pitch n + 1) by T threads.  ZERO: e enters as +0 everywhere (pre-smoothing),
+// so the first half-sweep reads no neighbours.
+template <bool SMALL, bool ZERO = false>
 __device__ void level_sweeps(float* sm, const CoarseLevel& L, float omega, int nu, int t, int T) {
   const int n = L.n, P = n + 1;
   float* const e = sm + L.off;
@@ -397,12 +407,13 @@ __device__ void level_sweeps(float* sm, const CoarseLevel& L, float omega, int n
           }
         }
       }
-      __syncthreads();
+      level_sync<SMALL>();
     }
 }
 
 // Residual of level A and its full weighting (Multigrid.cu:299-349) to the interior of the
 // next level's right-hand side (its boundary stays 0).
+template <bool SMALL>
 __device__ void level_restrict(float* sm, const CoarseLevel& A, const CoarseLevel& B, int t, int T) {
   const int n = A.n, P = n + 1, nc = B.n, Pc = nc + 1;
   const float* const e = sm + A.off;
@@ -425,11 +436,12 @@ __device__ void level_restrict(float* sm, const CoarseLevel& A, const CoarseLeve
       fn[jc * Pc + ic] = (4.f * r[1][1] + 2.f * r[1][0] + 2.f * r[1][2] + 2.f * r[0][1] + 2.f * r[2][1] + r[0][0] +
                           r[0][2] + r[2][0] + r[2][2]) * 0.0625f;
     }
-  __syncthreads();
+  level_sync<SMALL>();
 }
 
 // Bilinear prolongation (Multigrid.cu:351-407) of level B's correction added to the interior
 // of level A's.
+template <bool SMALL>
 __device__ void level_prolong(float* sm, const CoarseLevel& A, const CoarseLevel& B, int t, int T) {
   const int n = A.n, P = n + 1, Pc = B.n + 1;
   float* const e = sm + A.off;
@@ -439,7 +451,7 @@ __device__ void level_prolong(float* sm, const CoarseLevel& A, const CoarseLevel
   if (g < G)
     for (int j = 1 + g; j <= n - 2; j += G)
       e[j * P + i] += prolong_value(c + (j >> 1) * Pc + (i >> 1), Pc, i & 1, j & 1);
-  __syncthreads();
+  level_sync<SMALL>();
 }
 
 // Shared-memory bytes of levels lc .. levels-1 in the coarse solver's layout.
@@ -521,14 +533,32 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   tma::pdl_wait();
   coarse_load(sm + lv[lc].off + lv[lc].n * (lv[lc].n + 1), f_top, lv[lc].n);
   __syncthreads();
-  for (int l = lc; l < L - 1; ++l) {
-    level_sweeps<true>(sm, lv[l], omega, nu_pre, t, T);
-    level_restrict(sm, lv[l], lv[l + 1], t, T);
+  int l = lc;
+  for (; l < L - 1 && lv[l].n > kCoarseSmallSide; ++l) {
+    level_sweeps<false, true>(sm, lv[l], omega, nu_pre, t, T);
+    level_restrict<false>(sm, lv[l], lv[l + 1], t, T);
   }
-  level_sweeps(sm, lv[L - 1], omega, nu_coarse, t, T);
-  for (int l = L - 2; l >= lc; --l) {
-    level_prolong(sm, lv[l], lv[l + 1], t, T);
-    level_sweeps(sm, lv[l], omega, nu_post, t, T);
+  if (lv[l].n > kCoarseSmallSide) {  // a large coarsest level (l == L - 1)
+    level_sweeps<false>(sm, lv[l], omega, nu_coarse, t, T);
+  } else {
+    // the small levels: a few nodes per phase, so few threads and a cheap barrier
+    constexpr int TS = kCoarseSmallThreads;
+    if (t < TS) {
+      for (int k = l; k < L - 1; ++k) {
+        level_sweeps<true, true>(sm, lv[k], omega, nu_pre, t, TS);
+        level_restrict<true>(sm, lv[k], lv[k + 1], t, TS);
+      }
+      level_sweeps<true>(sm, lv[L - 1], omega, nu_coarse, t, TS);
+      for (int k = L - 2; k >= l; --k) {
+        level_prolong<true>(sm, lv[k], lv[k + 1], t, TS);
+        level_sweeps<true>(sm, lv[k], omega, nu_post, t, TS);
+      }
+    }
+    __syncthreads();
+  }
+  for (int k = l - 1; k >= lc; --k) {
+    level_prolong<false>(sm, lv[k], lv[k + 1], t, T);
+    level_sweeps<false>(sm, lv[k], omega, nu_post, t, T);
   }
   coarse_store(e_top, sm + lv[lc].off, lv[lc].n);
   __syncthreads();  // shared memory is free for the CTA's next job
