@@ -243,6 +243,12 @@ __device__ __forceinline__ void lane_deposit(V* rho, int nx, const uint32_t key[
   warp_runs_deposit(rho, nx, rk, a0, a1, a2, a3);
 }
 
+// Deferred collision candidates of a warp: cell fx fy vx vy vz pid index, up to one round of
+// 32 left over plus one item's worth.
+constexpr int kQueue = 32 + kItem;
+constexpr int kQFields = 8;
+constexpr size_t kMoverSmem = (size_t)kWarps * kQFields * kQueue * sizeof(uint32_t);
+
 // The fused particle pass.  Warp w of the grid takes items w, w + W, w + 2W, ... (W warps in
 // the grid) over the concatenated items of all active slots; the slot of an item comes from
 // the item prefix, and a warp's items only move forward through the slots.  Per item:
@@ -250,8 +256,10 @@ __device__ __forceinline__ void lane_deposit(V* rho, int nx, const uint32_t key[
 //            per array and lane
 //   pass A   kick (E gathered from the per-step node field; particles are cell-sorted, so a
 //            warp's gathers hit a few cache lines) and the null-collision candidate test;
-//            the item's candidates (~nu_max dt of the particles) are listed in shared memory
-//            by rank and collided warp-cooperatively, 32 per round
+//            candidates (~nu_max dt of the particles) leave the item for the warp's queue in
+//            shared memory.  Whenever 32 are queued (and when the warp leaves a slot), one
+//            round collides, drifts, deposits and stores them, one candidate per lane, after
+//            their owners have stored the rest of their items.
 //   pass B   drift, absorption (hits appended with one atomic per item), CIC deposit
 //   stores   streaming 16-byte stores of what changed
 // The particle stream bypasses L2 retention (evict-first loads and stores) so the grids the
@@ -260,14 +268,16 @@ __global__ void __launch_bounds__(PIC_MOVER_THREADS, PIC_MOVER_MIN_BLOCKS)
 mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
              const int* __restrict__ counts, int* __restrict__ hit_counts, const int* __restrict__ item_prefix,
              int nslots, int flags, uint32_t explicit_step) {
+  extern __shared__ __align__(16) uint32_t qbuf[];
   __shared__ WarpTables tab[kWarps];
-  __shared__ float clist[kWarps][7][32];   // collision candidates of one round: vx vy vz pid cell fx fy
   __shared__ unsigned pcount[kWarps][8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int total = item_prefix[nslots];
   const SlotDev& S = tab[warp].S;
   const JobDev& J = tab[warp].J;
   unsigned* const pc = pcount[warp];
+  uint32_t* const cq = qbuf + (size_t)warp * kQFields * kQueue;   // field f of entry e: cq[f * kQueue + e]
+  int qn = 0;                                                      // queued candidates (warp-uniform)
   if (lane < 8) pc[lane] = 0u;
   __syncwarp();
   int cur = -1;
@@ -275,9 +285,49 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
   bool do_kick = false, do_mcc = false, do_drift = false, do_walls = false, do_dep = false, want_ke = false;
   uint32_t mcc_step = 0;
   int n = 0;
+  // One round over the first cnt queued candidates (one per lane): collide (Philox stream
+  // (seed, pid, step) as for the candidate test), drift, absorb, deposit, store at the
+  // particle's index; then the queue moves down by cnt.  The owners' stores of these
+  // particles were issued before (the barrier orders them first).
+  auto round = [&](int cnt) {
+    __syncwarp();
+    const int s = cur;
+    bool absorbed = false;
+    int idx = 0;
+    if (lane < cnt) {
+      uint32_t qc = cq[0 * kQueue + lane];
+      float qfx = __uint_as_float(cq[1 * kQueue + lane]), qfy = __uint_as_float(cq[2 * kQueue + lane]);
+      float qvx = __uint_as_float(cq[3 * kQueue + lane]), qvy = __uint_as_float(cq[4 * kQueue + lane]);
+      float qvz = __uint_as_float(cq[5 * kQueue + lane]);
+      const uint32_t qpid = cq[6 * kQueue + lane];
+      idx = (int)cq[7 * kQueue + lane];
+      float u[4];
+      draw4(J.seed, qpid, mcc_step, 0u, u);
+      collide(J, S, slots, st[S.job], qpid, qc, qfx, qfy, qvx, qvy, qvz, u, mcc_step, pc);
+      if (want_ke) ke += (double)(qvx * qvx + qvy * qvy + qvz * qvz);
+      if (do_drift) {
+        const Drifted d = drift_particle(J, S, qc, qfx, qfy, qvx, qvy, do_walls);
+        absorbed = d.absorbed; qc = d.cell; qfx = d.fx; qfy = d.fy;
+        S.cell[idx] = qc; S.fx[idx] = qfx; S.fy[idx] = qfy;
+      }
+      if (do_dep && !absorbed) deposit_one(J, S, qc, qfx, qfy);
+      S.vx[idx] = qvx; S.vy[idx] = qvy; S.vz[idx] = qvz;
+    }
+    if (do_walls) {
+      const int h = warp_append(lane < cnt && absorbed, hit_counts + s);
+      if (h >= 0) S.hits[h] = idx;
+    }
+    __syncwarp();
+    for (int q = lane; q < qn - cnt; q += 32)
+#pragma unroll
+      for (int f = 0; f < kQFields; ++f) cq[f * kQueue + q] = cq[f * kQueue + q + cnt];
+    __syncwarp();
+    qn -= cnt;
+  };
   // kinetic energy and collision counts of the slot a warp leaves go to its job's state
   auto flush = [&]() {
     if (cur < 0) return;
+    if (qn > 0) round(qn);
     if (want_ke) {
       double v = ke;
 #pragma unroll
@@ -394,35 +444,19 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
         int rank[kPPL];
 #pragma unroll
         for (int k = 0; k < kPPL; ++k) rank[k] = before[k] + __popc(m[k] & ((1u << lane) - 1u));
-        JobState& T = st[S.job];
-        for (int r0 = 0; r0 < ncand; r0 += 32) {
+        // candidates leave the item for the warp's queue
 #pragma unroll
-          for (int k = 0; k < kPPL; ++k)
-            if (cand[k] && rank[k] >= r0 && rank[k] < r0 + 32) {
-              const int q = rank[k] - r0;
-              clist[warp][0][q] = vx[k]; clist[warp][1][q] = vy[k]; clist[warp][2][q] = vz[k];
-              clist[warp][3][q] = __uint_as_float(pid[k]); clist[warp][4][q] = __uint_as_float(c[k]);
-              clist[warp][5][q] = fx[k]; clist[warp][6][q] = fy[k];
-            }
-          __syncwarp();
-          if (r0 + lane < ncand) {
-            float cvx = clist[warp][0][lane], cvy = clist[warp][1][lane], cvz = clist[warp][2][lane];
-            const uint32_t cpid = __float_as_uint(clist[warp][3][lane]);
-            float u[4];
-            draw4(J.seed, cpid, mcc_step, 0u, u);
-            collide(J, S, slots, T, cpid, __float_as_uint(clist[warp][4][lane]), clist[warp][5][lane],
-                    clist[warp][6][lane], cvx, cvy, cvz, u, mcc_step, pc);
-            clist[warp][0][lane] = cvx; clist[warp][1][lane] = cvy; clist[warp][2][lane] = cvz;
+        for (int k = 0; k < kPPL; ++k)
+          if (cand[k]) {
+            const int q = qn + rank[k];
+            cq[0 * kQueue + q] = c[k];
+            cq[1 * kQueue + q] = __float_as_uint(fx[k]); cq[2 * kQueue + q] = __float_as_uint(fy[k]);
+            cq[3 * kQueue + q] = __float_as_uint(vx[k]); cq[4 * kQueue + q] = __float_as_uint(vy[k]);
+            cq[5 * kQueue + q] = __float_as_uint(vz[k]); cq[6 * kQueue + q] = pid[k];
+            cq[7 * kQueue + q] = (uint32_t)(i0 + k);
+            valid[k] = false;   // the queue round finishes this particle
           }
-          __syncwarp();
-#pragma unroll
-          for (int k = 0; k < kPPL; ++k)
-            if (cand[k] && rank[k] >= r0 && rank[k] < r0 + 32) {
-              const int q = rank[k] - r0;
-              vx[k] = clist[warp][0][q]; vy[k] = clist[warp][1][q]; vz[k] = clist[warp][2][q];
-            }
-          __syncwarp();
-        }
+        qn += ncand;
       }
     }
     if (want_ke) {
@@ -490,6 +524,8 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
       __stcs(reinterpret_cast<float4*>(S.vy + i0), make_float4(vy[0], vy[1], vy[2], vy[3]));
     }
     if (do_mcc) __stcs(reinterpret_cast<float4*>(S.vz + i0), make_float4(vz[0], vz[1], vz[2], vz[3]));
+    // full rounds of queued candidates, after this item's stores
+    while (qn >= 32) round(32);
   }
   flush();
 }
@@ -508,8 +544,9 @@ __global__ void chunk_table_kernel(const int* __restrict__ counts, const uint8_t
 }
 
 int mover_blocks_per_sm() {
+  cudaFuncSetAttribute(mover_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMoverSmem);
   int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, mover_kernel, PIC_MOVER_THREADS, kMoverSmem) != cudaSuccess ||
       b < 1) {
     cudaGetLastError();
     b = 1;
@@ -527,7 +564,7 @@ int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaS
   }
   chunk_table_kernel<<<1, 32, 0, stream>>>(L.counts, L.active, L.chunk_prefix, L.nslots);
   if (L.ev_mover_begin) cudaEventRecord(L.ev_mover_begin, stream);
-  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, 0, stream>>>(L.jobs, L.st, L.slots, L.counts,
+  mover_kernel<<<L.mover_grid, PIC_MOVER_THREADS, kMoverSmem, stream>>>(L.jobs, L.st, L.slots, L.counts,
                                                                           L.hit_counts, L.chunk_prefix, L.nslots, flags,
                                                                           explicit_step);
   if (L.ev_mover_end) cudaEventRecord(L.ev_mover_end, stream);
