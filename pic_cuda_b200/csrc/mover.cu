@@ -77,17 +77,46 @@ __device__ __forceinline__ void seg_reduce4(T& a, T& b, T& c, T& d, int seg) {
 
 }  // namespace
 
-// Particles per lane and per warp work item: lane l of a warp holds particles 4l .. 4l+3 of
-// a 128-particle item in registers, loaded with one 16-byte load per array (512 contiguous
-// bytes per warp and array).  Capacities are multiples of PIC_CHUNK, so every item lies
-// inside the arrays.
-constexpr int kPPL = 4;
+// Particles per lane and per warp work item: lane l of a warp holds particles kPPL l ..
+// kPPL l + kPPL - 1 of a (32 kPPL)-particle item in registers, loaded with one vector load per
+// array (contiguous per warp and array).  Capacities are multiples of PIC_CHUNK, so every item
+// lies inside the arrays.  With the CTAs per SM below, measured on B200 (1025^2, 2e7
+// particles, ms per pass): 2 per lane at 4 CTAs per SM 0.441; 2 at 3 CTAs 0.466, at 5 CTAs
+// 0.476; 4 per lane at 3 CTAs 0.467, at 4 CTAs 0.510 (register spills).
+#ifndef PIC_MOVER_PPL
+#define PIC_MOVER_PPL 2
+#endif
+constexpr int kPPL = PIC_MOVER_PPL;
 constexpr int kItem = 32 * kPPL;
+
+// kPPL consecutive 4-byte values of one lane as one evict-first vector load / store.
+__device__ __forceinline__ void ld_lane(const float* p, float (&a)[4]) {
+  const float4 v = __ldcs(reinterpret_cast<const float4*>(p)); a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+__device__ __forceinline__ void ld_lane(const float* p, float (&a)[2]) {
+  const float2 v = __ldcs(reinterpret_cast<const float2*>(p)); a[0] = v.x; a[1] = v.y;
+}
+__device__ __forceinline__ void ld_lane(const uint32_t* p, uint32_t (&a)[4]) {
+  const uint4 v = __ldcs(reinterpret_cast<const uint4*>(p)); a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+__device__ __forceinline__ void ld_lane(const uint32_t* p, uint32_t (&a)[2]) {
+  const uint2 v = __ldcs(reinterpret_cast<const uint2*>(p)); a[0] = v.x; a[1] = v.y;
+}
+__device__ __forceinline__ void st_lane(float* p, const float (&a)[4]) {
+  __stcs(reinterpret_cast<float4*>(p), make_float4(a[0], a[1], a[2], a[3]));
+}
+__device__ __forceinline__ void st_lane(float* p, const float (&a)[2]) {
+  __stcs(reinterpret_cast<float2*>(p), make_float2(a[0], a[1]));
+}
+__device__ __forceinline__ void st_lane(uint32_t* p, const uint32_t (&a)[4]) {
+  __stcs(reinterpret_cast<uint4*>(p), make_uint4(a[0], a[1], a[2], a[3]));
+}
+__device__ __forceinline__ void st_lane(uint32_t* p, const uint32_t (&a)[2]) {
+  __stcs(reinterpret_cast<uint2*>(p), make_uint2(a[0], a[1]));
+}
 constexpr int kWarps = PIC_MOVER_THREADS / 32;
-// CTAs per SM: the pass is limited by how many 16-byte loads are in flight, and 4 particles
-// per lane need ~80 registers, so 3 CTAs (24 warps) per SM.
 #ifndef PIC_MOVER_MIN_BLOCKS
-#define PIC_MOVER_MIN_BLOCKS 3
+#define PIC_MOVER_MIN_BLOCKS 4
 #endif
 
 // One real-or-null collision of a null-collision candidate (Vahedi & Surendra 1995): the
@@ -252,7 +281,7 @@ constexpr size_t kMoverSmem = (size_t)kWarps * kQFields * kQueue * sizeof(uint32
 // The fused particle pass.  Warp w of the grid takes items w, w + W, w + 2W, ... (W warps in
 // the grid) over the concatenated items of all active slots; the slot of an item comes from
 // the item prefix, and a warp's items only move forward through the slots.  Per item:
-//   loads    cell, fx, fy, vx, vy (+ vz, pid with collisions): one streaming 16-byte load
+//   loads    cell, fx, fy, vx, vy (+ vz, pid with collisions): one evict-first vector load
 //            per array and lane
 //   pass A   kick (E gathered from the per-step node field; particles are cell-sorted, so a
 //            warp's gathers hit a few cache lines) and the null-collision candidate test;
@@ -261,7 +290,7 @@ constexpr size_t kMoverSmem = (size_t)kWarps * kQFields * kQueue * sizeof(uint32
 //            round collides, drifts, deposits and stores them, one candidate per lane, after
 //            their owners have stored the rest of their items.
 //   pass B   drift, absorption (hits appended with one atomic per item), CIC deposit
-//   stores   streaming 16-byte stores of what changed
+//   stores   evict-first vector stores of what changed
 // The particle stream bypasses L2 retention (evict-first loads and stores) so the grids the
 // gathers and deposits touch stay resident.  No block-level synchronisation.
 __global__ void __launch_bounds__(PIC_MOVER_THREADS, PIC_MOVER_MIN_BLOCKS)
@@ -369,21 +398,14 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     uint32_t c[kPPL], pid[kPPL];
     float fx[kPPL], fy[kPPL], vx[kPPL], vy[kPPL], vz[kPPL];
     {
-      const uint4 c4 = __ldcs(reinterpret_cast<const uint4*>(S.cell + i0));
-      const float4 x4 = __ldcs(reinterpret_cast<const float4*>(S.fx + i0));
-      const float4 y4 = __ldcs(reinterpret_cast<const float4*>(S.fy + i0));
-      const float4 u4 = __ldcs(reinterpret_cast<const float4*>(S.vx + i0));
-      const float4 w4 = __ldcs(reinterpret_cast<const float4*>(S.vy + i0));
-      c[0] = c4.x; c[1] = c4.y; c[2] = c4.z; c[3] = c4.w;
-      fx[0] = x4.x; fx[1] = x4.y; fx[2] = x4.z; fx[3] = x4.w;
-      fy[0] = y4.x; fy[1] = y4.y; fy[2] = y4.z; fy[3] = y4.w;
-      vx[0] = u4.x; vx[1] = u4.y; vx[2] = u4.z; vx[3] = u4.w;
-      vy[0] = w4.x; vy[1] = w4.y; vy[2] = w4.z; vy[3] = w4.w;
+      ld_lane(S.cell + i0, c);
+      ld_lane(S.fx + i0, fx);
+      ld_lane(S.fy + i0, fy);
+      ld_lane(S.vx + i0, vx);
+      ld_lane(S.vy + i0, vy);
       if (do_mcc) {
-        const float4 z4 = __ldcs(reinterpret_cast<const float4*>(S.vz + i0));
-        const uint4 p4 = __ldcs(reinterpret_cast<const uint4*>(S.pid + i0));
-        vz[0] = z4.x; vz[1] = z4.y; vz[2] = z4.z; vz[3] = z4.w;
-        pid[0] = p4.x; pid[1] = p4.y; pid[2] = p4.z; pid[3] = p4.w;
+        ld_lane(S.vz + i0, vz);
+        ld_lane(S.pid + i0, pid);
       } else {
 #pragma unroll
         for (int k = 0; k < kPPL; ++k) { vz[k] = 0.f; pid[k] = 0u; }
@@ -515,15 +537,15 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     }
     // ---- stores
     if (do_drift) {
-      __stcs(reinterpret_cast<uint4*>(S.cell + i0), make_uint4(c[0], c[1], c[2], c[3]));
-      __stcs(reinterpret_cast<float4*>(S.fx + i0), make_float4(fx[0], fx[1], fx[2], fx[3]));
-      __stcs(reinterpret_cast<float4*>(S.fy + i0), make_float4(fy[0], fy[1], fy[2], fy[3]));
+      st_lane(S.cell + i0, c);
+      st_lane(S.fx + i0, fx);
+      st_lane(S.fy + i0, fy);
     }
     if (do_kick || do_mcc) {
-      __stcs(reinterpret_cast<float4*>(S.vx + i0), make_float4(vx[0], vx[1], vx[2], vx[3]));
-      __stcs(reinterpret_cast<float4*>(S.vy + i0), make_float4(vy[0], vy[1], vy[2], vy[3]));
+      st_lane(S.vx + i0, vx);
+      st_lane(S.vy + i0, vy);
     }
-    if (do_mcc) __stcs(reinterpret_cast<float4*>(S.vz + i0), make_float4(vz[0], vz[1], vz[2], vz[3]));
+    if (do_mcc) st_lane(S.vz + i0, vz);
     // full rounds of queued candidates, after this item's stores
     while (qn >= 32) round(32);
   }
