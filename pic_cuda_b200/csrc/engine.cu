@@ -70,6 +70,9 @@ struct JobHost {
   int64_t bytes = 0;
   int64_t steps = 0;
   bool pending = false;
+  // JobState::total_charge holds the sum of the present rho: the level-0 residual kernel
+  // of every field solve computes it; entry points that change rho otherwise clear this
+  bool charge_fresh = false;
   MgBuild mg;
 };
 
@@ -206,7 +209,7 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
   for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
   b += 4 * N;                                                         // second level-0 rhs
-  b += 16ll * L.ntiles0;
+  b += 24ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
   for (int s = 0; s < c.n_species; ++s) {
     const int64_t cap = round_up(std::max<int64_t>(c.species[s].capacity, 1), PIC_CHUNK);
@@ -902,7 +905,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     if (l > 0) ALLOC(D.eu[l], 4ll * lay.nl[l] * lay.nl[l]);
   }
   ALLOC(D.f0b, N * 4);
-  ALLOC(D.partials, 16ll * lay.ntiles0);
+  ALLOC(D.partials, 24ll * lay.ntiles0);   // per level-0 tile: r^2, F^2 (pairs), then charge
   if (c.n_walls > 0) {
     std::vector<double> w(4 * c.n_walls);
     for (int k = 0; k < c.n_walls; ++k) {
@@ -1180,6 +1183,9 @@ int pic_step(pic_engine* E, int nsteps, void* stream) {
     rc = step_once(E, s);
     if (rc) return rc;
   }
+  if (nsteps > 0)
+    for (int j = 0; j < E->njobs_hw; ++j)
+      if (E->jobs[j].alive) E->jobs[j].charge_fresh = true;
   return PIC_OK;
 }
 
@@ -1204,7 +1210,7 @@ int pic_step_graph(pic_engine* E, int nsteps, void* stream) {
     E->graph_steps++;
     E->steps_taken++;
     for (int j = 0; j < E->njobs_hw; ++j)
-      if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; }
+      if (E->jobs[j].alive) { E->jobs[j].steps++; E->jobs[j].pending = true; E->jobs[j].charge_fresh = true; }
   }
   return PIC_OK;
 }
@@ -1268,7 +1274,9 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
   CK(cudaSetDevice(E->device));
   cudaStream_t s = E->stream;
   CK(cudaDeviceSynchronize());
-  launch_rho_sum(E->d_jobs + job, E->d_st + job, E->d_diag, std::min(1024, 2 * E->num_sms), s);
+  // the last field solve summed rho already unless rho changed since
+  if (!E->jobs[job].charge_fresh)
+    launch_rho_sum(E->d_jobs + job, E->d_st + job, E->d_diag, std::min(1024, 2 * E->num_sms), s);
   JobState T;
   int cnt[kSlotsPerJob], ab[kSlotsPerJob];
   CK(cudaMemcpyAsync(&T, E->d_st + job, sizeof(JobState), cudaMemcpyDeviceToHost, s));
@@ -1297,6 +1305,7 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
 int pic_job_run_phases(pic_engine* E, int job, int flags, int64_t step_index, void* stream) {
   int rc = check_job(E, job);
   if (rc) return rc;
+  E->jobs[job].charge_fresh = false;
   CK(cudaSetDevice(E->device));
   cudaStream_t s = pick(E, stream);
   rc = flush(E, s);
@@ -1329,6 +1338,7 @@ int pic_job_compact(pic_engine* E, int job, void* stream) {
 int pic_job_zero_rho(pic_engine* E, int job, void* stream) {
   int rc = check_job(E, job);
   if (rc) return rc;
+  E->jobs[job].charge_fresh = false;
   CK(cudaSetDevice(E->device));
   JobDev& D = E->jobs[job].dev;
   launch_zero_rho(nullptr, (int64_t)D.nx * D.ny, D.deposit_mode, D.deposit_mode == 0 ? (void*)D.rho_f : (void*)D.rho_i,
@@ -1359,6 +1369,7 @@ int pic_job_solve_field(pic_engine* E, int job, void* stream) {
   if (rc) return rc;
   CK(cudaSetDevice(E->device));
   JobHost& J = E->jobs[job];
+  J.charge_fresh = true;
   if (!J.mg.valid) {
     rc = build_mg(E, std::vector<int>{job}, J.mg);
     if (rc) return rc;
@@ -1395,6 +1406,7 @@ int pic_job_get_grid(pic_engine* E, int job, int which, double* out, int memory)
 int pic_job_set_grid(pic_engine* E, int job, int which, const double* in, int memory) {
   int rc = check_job(E, job);
   if (rc) return rc;
+  if (which == PIC_GRID_RHO) E->jobs[job].charge_fresh = false;
   if ((which != PIC_GRID_RHO && which != PIC_GRID_PHI) || !in) return fail(PIC_ERR_ARG, "only RHO and PHI can be set");
   CK(cudaSetDevice(E->device));
   JobHost& J = E->jobs[job];

@@ -87,7 +87,8 @@ __device__ bool last_of_job(JobState& T, int nlocal) {
 // ---------------------------------------------------------------- mg_init
 // Level-0 defect of the initial guess on a 32 x 32 tile: the potential (and with the
 // extrapolated warm start the previous solution) with a one-node halo and rho arrive in one
-// batch of asynchronous copies; the guess is formed once per node in shared memory.
+// batch of asynchronous copies; the guess is formed once per node in shared memory.  The
+// same pass sums the deposited charge (deterministic per-tile partials, like the norms).
 __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
                                                       JobState* __restrict__ st, int* running) {
   constexpr int PW = kTI + 2, NT = 256;
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   const double rhs_scale = J.rhs_scale;
   const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
   double* const partials = J.partials;
+  const double qref = J.qref;
   const int i0 = tr.ti * kTI, j0 = tr.tj * kTI;
   const int t = threadIdx.x;
 #pragma unroll
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     }
     __syncthreads();
   }
-  double ar = 0.0, af = 0.0;
+  double ar = 0.0, af = 0.0, aq = 0.0;
 #pragma unroll
   for (int u = 0; u < NO; ++u) {
     const int k = t + u * NT;
@@ -174,20 +176,25 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     f0[c] = (float)r;
     ar += r * r;
     af += F * F;
+    aq += rv;
   }
   const double sr = block_sum(ar);
   const double sf = block_sum(af);
+  const double sq = block_sum(aq);
   if (t == 0) {
     partials[2 * (tr.pbase + tr.local)] = sr;
     partials[2 * (tr.pbase + tr.local) + 1] = sf;
+    partials[2 * tr.nlocal + tr.pbase + tr.local] = sq;   // deposited charge (third block)
   }
   if (last_of_job(T, tr.nlocal)) {
     __threadfence();
     const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
     const double f2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 1);
+    const double q = ordered_sum(partials + 2 * tr.nlocal + tr.pbase, tr.nlocal, 1, 0);
     if (t != 0) return;
     T.rnorm2 = r2;
     T.fnorm2 = f2;
+    T.total_charge = q * qref;
     T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
     T.cycles = 0;
     T.converged = 0;
