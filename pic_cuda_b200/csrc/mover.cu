@@ -61,11 +61,12 @@ __device__ __forceinline__ void neutral_velocity(uint64_t seed, uint32_t pid, ui
   v[0] = sig * r0 * c; v[1] = sig * r0 * s; v[2] = sig * r1 * c2;
 }
 
+// Segmented sums towards each segment's first lane; maxlen (warp-uniform) bounds the segment
+// lengths, so only ceil(log2(maxlen)) shuffle levels run.
 template <typename T>
-__device__ __forceinline__ void seg_reduce4(T& a, T& b, T& c, T& d, int seg) {
+__device__ __forceinline__ void seg_reduce4(T& a, T& b, T& c, T& d, int seg, int maxlen) {
   const int lane = lane_id();
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
+  for (int o = 1; o < maxlen; o <<= 1) {
     const T ta = __shfl_down_sync(0xffffffffu, a, o);
     const T tb = __shfl_down_sync(0xffffffffu, b, o);
     const T tc = __shfl_down_sync(0xffffffffu, c, o);
@@ -222,7 +223,12 @@ __device__ __forceinline__ void warp_runs_deposit(V* rho, int nx, uint32_t key, 
   const bool head = (lane == 0) || (key != prev);
   const unsigned heads = __ballot_sync(0xffffffffu, head);
   const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
-  seg_reduce4(v0, v1, v2, v3, seg);
+  // longest segment: each lane measures its own from its head to the next head
+  const unsigned after = lane == 31 ? 0u : heads & (0xfffffffeu << lane);
+  const int first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+  const int next = after ? __ffs(after) - 1 : 32;
+  const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)(next - first));
+  seg_reduce4(v0, v1, v2, v3, seg, maxlen);
   if (head && key != PIC_CELL_OUT) {
     V* r = rho + (size_t)cell_j(key) * nx + cell_i(key);
     atomicAdd(r, v0);
@@ -290,7 +296,8 @@ constexpr size_t kMoverSmem = (size_t)kWarps * kQFields * kQueue * sizeof(uint32
 //            round collides, drifts, deposits and stores them, one candidate per lane, after
 //            their owners have stored the rest of their items.
 //   pass B   drift, absorption (hits appended with one atomic per item), CIC deposit
-//   stores   evict-first vector stores of what changed
+//   stores   evict-first vector stores of what changed (vz only in the queue rounds; the
+//            cell word only when some particle of the warp crossed a cell edge)
 // The particle stream bypasses L2 retention (evict-first loads and stores) so the grids the
 // gathers and deposits touch stay resident.  No block-level synchronisation.
 __global__ void __launch_bounds__(PIC_MOVER_THREADS, PIC_MOVER_MIN_BLOCKS)
@@ -487,6 +494,9 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
         if (valid[k]) ke += (double)(vx[k] * vx[k] + vy[k] * vy[k] + vz[k] * vz[k]);
     }
     // ---- pass B: drift, walls, deposit
+    uint32_t c_in[kPPL];
+#pragma unroll
+    for (int k = 0; k < kPPL; ++k) c_in[k] = c[k];
     uint32_t key[kPPL];
     bool absorbed[kPPL];
 #pragma unroll
@@ -537,7 +547,12 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
     }
     // ---- stores
     if (do_drift) {
-      st_lane(S.cell + i0, c);
+      // the cell word changes only when a particle crosses a cell edge (rare for ions): a warp
+      // whose cells all stayed leaves them in place
+      bool moved = false;
+#pragma unroll
+      for (int k = 0; k < kPPL; ++k) moved |= c[k] != c_in[k];
+      if (__any_sync(0xffffffffu, moved)) st_lane(S.cell + i0, c);
       st_lane(S.fx + i0, fx);
       st_lane(S.fy + i0, fy);
     }
@@ -545,7 +560,7 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
       st_lane(S.vx + i0, vx);
       st_lane(S.vy + i0, vy);
     }
-    if (do_mcc) st_lane(S.vz + i0, vz);
+    // vz changes only in a collision, and the queue round stores the collided particles
     // full rounds of queued candidates, after this item's stores
     while (qn >= 32) round(32);
   }
