@@ -273,6 +273,10 @@ struct pic_engine {
   cudaGraphExec_t graph_exec_sort = nullptr;
   bool graph_dirty = true;
   cudaStream_t cap_stream = nullptr, body_stream = nullptr;
+  // The counting sort due before a job's next step runs on side_stream, concurrently with the
+  // field solve of this step (the solve touches only grids, the sort only particle arrays).
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int* d_loop = nullptr;                    // [0] iterations of the current solve
   unsigned long long* d_loop_total = nullptr;  // V-cycle iterations run by graph launches
   int64_t graph_fixed_launches[2] = {0, 0};
@@ -536,16 +540,16 @@ int check_job(pic_engine* E, int job) {
 }
 
 // One full step of every live job.
-int step_once(pic_engine* E, cudaStream_t s) {
-  EngineLaunch L = make_launch(E, nullptr);
-  // counting sort of the jobs that are due
+// Counting sort (stream-ordered on s) of the jobs for which `due` holds.
+template <typename Due>
+int sort_jobs(pic_engine* E, const EngineLaunch& L, Due due, cudaStream_t s, bool* launched) {
   std::vector<uint8_t> mask(L.nslots, 0);
   bool any = false;
   int max_cells = 0;
   int64_t max_p = 0;
   for (int j = 0; j < E->njobs_hw; ++j) {
     JobHost& J = E->jobs[j];
-    if (!J.alive || J.cfg.sort_every <= 0 || J.steps % J.cfg.sort_every != 0) continue;
+    if (!J.alive || J.cfg.sort_every <= 0 || !due(J)) continue;
     for (int k = 0; k < J.cfg.n_species; ++k) {
       mask[j * kSlotsPerJob + k] = 1;
       max_p = std::max<int64_t>(max_p, J.cfg.species[k].capacity);
@@ -553,12 +557,25 @@ int step_once(pic_engine* E, cudaStream_t s) {
     max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
     any = true;
   }
-  if (any) {
-    CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
-    phase_mark(E, 0, true, s);
-    E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
-    phase_mark(E, 0, false, s);
-  }
+  *launched = any;
+  if (!any) return PIC_OK;
+  CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
+  phase_mark(E, 0, true, s);
+  E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+  phase_mark(E, 0, false, s);
+  return PIC_OK;
+}
+// A job's first step sorts its (freshly loaded) particles before the particle pass; later
+// sorts run at the end of the step before the one that is due (step + 1 a multiple of
+// sort_every), concurrently with that step's field solve.
+bool sort_before_first(const JobHost& J) { return J.steps == 0; }
+bool sort_after(const JobHost& J) { return (J.steps + 1) % J.cfg.sort_every == 0; }
+
+int step_once(pic_engine* E, cudaStream_t s) {
+  EngineLaunch L = make_launch(E, nullptr);
+  bool sorted = false;
+  int rc = sort_jobs(E, L, sort_before_first, s, &sorted);
+  if (rc) return rc;
   E->launches += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
   int max_nodes = 0;
   for (int j = 0; j < E->njobs_hw; ++j)
@@ -582,10 +599,18 @@ int step_once(pic_engine* E, cudaStream_t s) {
   E->launches += launch_compact(L, s);
   E->launches += launch_ionize(L, true, s);
   phase_mark(E, 2, false, s);
+  // the sort due before the next step, on the side stream while the field is solved
+  CK(cudaEventRecord(E->ev_fork, s));
+  CK(cudaStreamWaitEvent(E->side_stream, E->ev_fork, 0));
+  bool side = false;
+  rc = sort_jobs(E, L, sort_after, E->side_stream, &side);
+  if (rc) return rc;
+  CK(cudaEventRecord(E->ev_join, E->side_stream));
   phase_mark(E, 3, true, s);
-  int rc = solve(E, E->mg_all, nullptr, s);
+  rc = solve(E, E->mg_all, nullptr, s);
   if (rc) return rc;
   phase_mark(E, 3, false, s);
+  CK(cudaStreamWaitEvent(s, E->ev_join, 0));
   E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
   E->steps_taken++;
   for (int j = 0; j < E->njobs_hw; ++j)
@@ -609,7 +634,14 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
     if (E->jobs[j].alive) max_nodes = std::max(max_nodes, E->jobs[j].dev.nx * E->jobs[j].dev.ny);
   cudaError_t err = cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (err != cudaSuccess) { cudaGraphDestroy(g); return fail(PIC_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(err)); }
+  n += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
+  n += launch_zero_rho_all(L, max_nodes, s);
+  n += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
+                           PIC_PHASE_GATED_I, 0, s);
+  n += launch_compact(L, s);
+  n += launch_ionize(L, true, s);
   if (with_sort) {
+    // the sort due before the next step, on a parallel branch of the graph beside the solve
     int max_cells = 0;
     int64_t max_p = 0;
     for (int j = 0; j < E->njobs_hw; ++j) {
@@ -618,15 +650,12 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
       for (int k = 0; k < J.cfg.n_species; ++k) max_p = std::max<int64_t>(max_p, J.cfg.species[k].capacity);
       max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
     }
-    n += launch_sort_mask(L, E->d_mask, s);
-    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+    if (err == cudaSuccess) err = cudaEventRecord(E->ev_fork, s);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(E->side_stream, E->ev_fork, 0);
+    n += launch_sort_mask(L, E->d_mask, 1, E->side_stream);
+    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), E->side_stream);
+    if (err == cudaSuccess) err = cudaEventRecord(E->ev_join, E->side_stream);
   }
-  n += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
-  n += launch_zero_rho_all(L, max_nodes, s);
-  n += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
-                           PIC_PHASE_GATED_I, 0, s);
-  n += launch_compact(L, s);
-  n += launch_ionize(L, true, s);
   n += launch_mg_init(L, E->mg_all.L, s);
   cudaMemsetAsync(E->d_loop, 0, sizeof(int), s);
   // conditional WHILE node for the V-cycles
@@ -660,6 +689,7 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
     }
   }
   if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+  if (err == cudaSuccess && with_sort) err = cudaStreamWaitEvent(s, E->ev_join, 0);
   if (err == cudaSuccess) n += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
   cudaGraph_t done = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(s, &done);
@@ -778,6 +808,9 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
   if (e == cudaSuccess) e = cudaMalloc(&E->d_diag, sizeof(double) * 1024);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->cap_stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->body_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&E->side_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&E->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_loop, sizeof(int) * 4);
   if (e == cudaSuccess) e = cudaMalloc(&E->d_loop_total, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(E->d_loop_total, 0, sizeof(unsigned long long));
@@ -810,6 +843,9 @@ int pic_engine_destroy(pic_engine* E) {
   if (E->graph_exec_sort) cudaGraphExecDestroy(E->graph_exec_sort);
   if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
   if (E->body_stream) cudaStreamDestroy(E->body_stream);
+  if (E->side_stream) cudaStreamDestroy(E->side_stream);
+  if (E->ev_fork) cudaEventDestroy(E->ev_fork);
+  if (E->ev_join) cudaEventDestroy(E->ev_join);
   if (E->d_loop) cudaFree(E->d_loop);
   if (E->d_loop_total) cudaFree(E->d_loop_total);
   cudaFree(E->d_jobs); cudaFree(E->d_st); cudaFree(E->d_slots); cudaFree(E->d_counts); cudaFree(E->d_hits);
@@ -1200,10 +1236,13 @@ int pic_step_graph(pic_engine* E, int nsteps, void* stream) {
   if (rc) return rc;
   cudaStream_t s = pick(E, stream);
   for (int k = 0; k < nsteps; ++k) {
+    bool sorted = false;
+    rc = sort_jobs(E, make_launch(E, nullptr), sort_before_first, s, &sorted);
+    if (rc) return rc;
     bool sort_due = false;
     for (int j = 0; j < E->njobs_hw; ++j) {
       const JobHost& J = E->jobs[j];
-      if (J.alive && J.cfg.sort_every > 0 && J.steps % J.cfg.sort_every == 0) sort_due = true;
+      if (J.alive && J.cfg.sort_every > 0 && sort_after(J)) sort_due = true;
     }
     CK(cudaGraphLaunch(sort_due ? E->graph_exec_sort : E->graph_exec, s));
     E->launches += E->graph_fixed_launches[sort_due ? 1 : 0];

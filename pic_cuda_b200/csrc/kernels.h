@@ -50,7 +50,7 @@ int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t
 int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);
 void launch_pid_max(const SlotDev* slot_dev, int64_t n, JobState* st, cudaStream_t s);
 int launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s);
-int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, cudaStream_t s);
+int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, int offset, cudaStream_t s);
 int launch_vcycle_condition(cudaGraphConditionalHandle h, const int* running, int* iterations, int max_iterations,
                             unsigned long long* total, cudaStream_t s);
 void launch_rho_sum(const JobDev* jd, JobState* st, double* scratch, int nparts, cudaStream_t s);

@@ -178,21 +178,23 @@ __global__ void sort_swap(SlotDev* slots, const uint8_t* mask, int nslots) {
   swp(S.vx, S.vx_b); swp(S.vy, S.vy_b); swp(S.vz, S.vz_b); swp(S.pid, S.pid_b);
 }
 
-// Slots whose job is due for a counting sort this step (sort_every > 0 and step % sort_every == 0).
-__global__ void sort_mask_kernel(const JobDev* jobs, const JobState* st, const uint8_t* active, uint8_t* mask, int nslots) {
+// Slots whose job is due for a counting sort: sort_every > 0 and (step + offset) % sort_every
+// == 0 (offset 1: the sort at the end of a step, before the step counter advances).
+__global__ void sort_mask_kernel(const JobDev* jobs, const JobState* st, const uint8_t* active, uint8_t* mask, int nslots,
+                                 int offset) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots) return;
   const int j = s / PIC_MAX_SPECIES;
   const JobDev& J = jobs[j];
-  const bool due = active[s] && J.sort_every > 0 && (st[j].step % J.sort_every) == 0;
+  const bool due = active[s] && J.sort_every > 0 && ((st[j].step + offset) % J.sort_every) == 0;
   mask[s] = due ? 1 : 0;
 }
 
 }  // namespace
 
-int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, cudaStream_t st) {
+int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, int offset, cudaStream_t st) {
   if (L.nslots == 0) return 0;
-  sort_mask_kernel<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.jobs, L.st, L.active, mask, L.nslots);
+  sort_mask_kernel<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.jobs, L.st, L.active, mask, L.nslots, offset);
   return 1;
 }
 
