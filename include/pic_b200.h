@@ -23,7 +23,11 @@
  *   pic_solve_multigrid_f64   solve_multigrid (Multigrid.hpp:3-11, Multigrid.cu:573-642)
  *                             on caller-owned FP64 device arrays
  *   pic_efield_f64            computeElectricField (kernels.cu:134-191) on FP64 arrays
+ *   pic_solve_embedded_f64    Multigrid::vcycle of Multigrid_embedded.cu:110-188 (masked
+ *                             nodes, interior electrodes) driven to a tolerance
  *   pic_job_export_species    Particles2D::debugParticles read-back (particles.cu:200)
+ *   pic_job_snapshot_positions  convertPositionsToFloat into the viewer's vertex buffer
+ *                             (kernels.cu:268-274, render.h:384-405), headless
  *   pic_job_get_grid          Grid2D::debugGrid read-back (grid.cu:30)
  */
 #ifndef PIC_B200_H
@@ -191,6 +195,12 @@ int pic_job_load_species(pic_engine* e, int job, int species, int64_t n,
 int pic_job_export_species(pic_engine* e, int job, int species, int64_t capacity,
                            double* x, double* y, double* vx, double* vy, double* vz,
                            uint32_t* pid, int64_t* n_out, int memory);
+/* Headless snapshot for a viewer: interleaved FP32 (x, y) of every particle of a species, 8 bytes
+ * per particle, into a device buffer (memory = PIC_MEM_DEVICE, e.g. a mapped vertex buffer) or
+ * host memory; what convertPositionsToFloat (kernels.cu:268-274) writes into the reference's
+ * OpenGL vertex buffer.  Each value is the FP64 export's position rounded once to FP32. */
+int pic_job_snapshot_positions(pic_engine* e, int job, int species, int64_t capacity, float* xy,
+                               int64_t* n_out, int memory);
 /* Same, in the engine's FP32 cell-relative layout (device pointers, no conversion). */
 int pic_job_export_species_raw(pic_engine* e, int job, int species, int64_t capacity,
                                uint32_t* cell, float* fx, float* fy, float* vx, float* vy,
@@ -246,6 +256,33 @@ int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int 
  * edges; E is interleaved (Ex, Ey) per node like the reference's double2 array. */
 int pic_efield_f64(const double* phi, double* E_xy, int nx, int ny, double dx, double dy,
                    void* stream);
+
+/* Embedded-boundary multigrid, Multigrid_embedded.cu:1-190 (the reference's Multigrid class
+ * and its vcycle, :110-188, driven to a tolerance).  Solves lap(phi) = rhs (FP64) on the FLUID
+ * nodes of `mask` (nx*ny bytes, row-major like phi): PIC_NODE_DIRICHLET nodes are interior
+ * electrodes held at phi_bc (phi_bc NULL: they keep the value phi holds), PIC_NODE_SOLID
+ * nodes and the grid boundary keep theirs.  V-cycle of Multigrid::vcycle over `levels` levels
+ * (nx_{l+1} = (nx_l - 1)/2 + 1): nu_pre red-black Gauss-Seidel sweeps ((i+j) even first;
+ * the reference's colour test at :22 updates every node on its second colour, a precedence
+ * slip, and this follows the intended test), residual, full weighting, coarse phi = 0,
+ * recursion (the coarsest level runs the pre-sweeps only), prolongation, nu_post sweeps.
+ * options 0 = the reference's transfer operators (coarse node kind injected from fine node
+ * (2i, 2j), piecewise-constant prolongation from coarse (i/2, j/2)); they do not converge for
+ * every geometry (an electrode edge on an odd node index makes the coarse electrode smaller
+ * than the fine one).  PIC_EMB_COARSEN_ANY takes the coarse kind from the 3x3 fine nodes as
+ * the reference's comment at :73 states; PIC_EMB_PROLONG_BILINEAR prolongates bilinearly.
+ * Stops when ||r|| / ||rhs|| over the FLUID nodes (||r|| / ||r_0|| if rhs is 0 there) is below
+ * tol or after max_cycles V-cycles (PIC_ERR_NOT_CONVERGED); reading the norm synchronises
+ * `stream` once per cycle.  tol == 0 runs exactly max_cycles V-cycles without reading it in
+ * between (once at the end with relres_out) and, like pic_solve_multigrid_f64, returns
+ * PIC_ERR_NOT_CONVERGED.  Working arrays come from a
+ * per-device cache keyed by (nx, ny, levels); calls on one device share it, so issue them on
+ * one stream or one after another. */
+enum { PIC_NODE_FLUID = 0, PIC_NODE_DIRICHLET = 1, PIC_NODE_SOLID = 2 };
+enum { PIC_EMB_COARSEN_ANY = 1, PIC_EMB_PROLONG_BILINEAR = 2 };
+int pic_solve_embedded_f64(double* phi, const double* rhs, const uint8_t* mask, const double* phi_bc,
+                           int nx, int ny, int levels, double h, int nu_pre, int nu_post, int options,
+                           double tol, int max_cycles, void* stream, int* cycles_out, double* relres_out);
 
 /* No counterpart in the reference.  pic_solve_multigrid_f64 with the same arguments,
  * arithmetic and return codes, for callers that must not allocate device memory: all

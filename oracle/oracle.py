@@ -70,6 +70,15 @@ def lib():
             "orc_sim_step": (None, [C.c_void_p, C.c_int]),
             "orc_sim_total_charge": (C.c_double, [C.c_void_p]),
             "orc_num_threads": (C.c_int, []),
+            "orc_emb_half_sweep": (None, [_D, _D, _U8, _D, C.c_int, C.c_int, C.c_double, C.c_int]),
+            "orc_emb_residual": (None, [_D, _D, _D, _U8, C.c_int, C.c_int, C.c_double]),
+            "orc_emb_restrict": (None, [_D, _D, _U8, _U8, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "orc_emb_prolong": (None, [_D, _D, _U8, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "orc_emb_vcycles": (None, [_D, _D, _U8, _D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                       C.c_int, C.c_int]),
+            "orc_emb_solve": (C.c_int, [_D, _D, _U8, _D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                        C.c_int, C.c_double, C.c_int, _D]),
+            "orc_emb_norms": (None, [_D, _D, _U8, C.c_int, C.c_int, C.c_double, _D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -184,6 +193,87 @@ def residual(phi, f, h):
     r = np.empty_like(phi)
     lib().orc_residual(_d(r), _d(phi), _d(f), nx, ny, h)
     return r
+
+
+# ---- embedded-boundary multigrid (Multigrid_embedded.cu): mask 0 FLUID, 1 DIRICHLET, 2 SOLID
+def _u8(a):
+    return a.ctypes.data_as(_U8)
+
+
+def _mask(m):
+    return np.ascontiguousarray(m, np.uint8)
+
+
+def emb_coarse_shape(nx, ny):
+    return (nx - 1) // 2 + 1, (ny - 1) // 2 + 1
+
+
+def emb_half_sweep(phi, rhs, mask, bc, h2, colour):
+    """One colour of smooth_redblack (Multigrid_embedded.cu:15-33), intended colour test."""
+    phi = f64(phi).copy()
+    rhs, mask = f64(rhs), _mask(mask)
+    bcp = _d(f64(bc)) if bc is not None else None
+    ny, nx = phi.shape
+    lib().orc_emb_half_sweep(_d(phi), _d(rhs), _u8(mask), bcp, nx, ny, h2, colour)
+    return phi
+
+
+def emb_residual(phi, rhs, mask, h2i):
+    """residual_kernel (Multigrid_embedded.cu:35-55) into a zeroed array."""
+    phi, rhs, mask = f64(phi), f64(rhs), _mask(mask)
+    ny, nx = phi.shape
+    res = np.zeros_like(phi)
+    lib().orc_emb_residual(_d(res), _d(phi), _d(rhs), _u8(mask), nx, ny, h2i)
+    return res
+
+
+def emb_restrict(res, mask, options=0):
+    """restrict_kernel (Multigrid_embedded.cu:57-86): coarse rhs and coarse mask (zeroed
+    boundary, like the reference's cudaMemset arrays)."""
+    res, mask = f64(res), _mask(mask)
+    nyf, nxf = res.shape
+    nxc, nyc = emb_coarse_shape(nxf, nyf)
+    coarse = np.zeros((nyc, nxc))
+    mc = np.zeros((nyc, nxc), np.uint8)
+    lib().orc_emb_restrict(_d(res), _d(coarse), _u8(mask), _u8(mc), nxf, nyf, nxc, nyc, options)
+    return coarse, mc
+
+
+def emb_prolong(coarse, fine, mask, options=0):
+    """prolongate_add_kernel (Multigrid_embedded.cu:88-104)."""
+    coarse, fine, mask = f64(coarse), f64(fine).copy(), _mask(mask)
+    nyf, nxf = fine.shape
+    nyc, nxc = coarse.shape
+    lib().orc_emb_prolong(_d(coarse), _d(fine), _u8(mask), nxf, nyf, nxc, nyc, options)
+    return fine
+
+
+def emb_vcycles(phi, rhs, mask, bc, h, levels, cycles, nu1=2, nu2=2, options=0):
+    phi = f64(phi).copy()
+    rhs, mask = f64(rhs), _mask(mask)
+    bcp = _d(f64(bc)) if bc is not None else None
+    ny, nx = phi.shape
+    lib().orc_emb_vcycles(_d(phi), _d(rhs), _u8(mask), bcp, nx, ny, levels, h, nu1, nu2, options, cycles)
+    return phi
+
+
+def emb_solve(phi, rhs, mask, bc, h, levels, nu1=2, nu2=2, tol=1e-10, max_cycles=100, options=0):
+    phi = f64(phi).copy()
+    rhs, mask = f64(rhs), _mask(mask)
+    bcp = _d(f64(bc)) if bc is not None else None
+    ny, nx = phi.shape
+    rel = C.c_double()
+    cyc = lib().orc_emb_solve(_d(phi), _d(rhs), _u8(mask), bcp, nx, ny, levels, h, nu1, nu2, options, tol,
+                              max_cycles, C.byref(rel))
+    return phi, cyc, rel.value
+
+
+def emb_norms(phi, rhs, mask, h):
+    phi, rhs, mask = f64(phi), f64(rhs), _mask(mask)
+    ny, nx = phi.shape
+    out = np.zeros(2)
+    lib().orc_emb_norms(_d(phi), _d(rhs), _u8(mask), nx, ny, h, _d(out))
+    return out
 
 
 class Sim:

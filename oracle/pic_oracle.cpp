@@ -393,6 +393,229 @@ ORC_API void orc_residual(double* r, const double* phi, const double* f, int nx,
   residual(r, phi, f, nx, ny, h);
 }
 
+// ------------------------------------------------------------------ embedded-boundary multigrid (FP64)
+// Multigrid_embedded.cu:1-190: a per-node mask marks FLUID (0) nodes, where lap(phi) = rhs
+// is solved, DIRICHLET (1) nodes (interior electrodes: phi = phi_bc) and SOLID (2) nodes
+// (left as they are).  V-cycle of Multigrid::vcycle (:159-188): nu1 red-black Gauss-Seidel
+// sweeps (colour 0 = (i+j) even first), residual, full weighting with the coarse mask
+// injected from the fine node (2i, 2j), coarse phi zeroed, recursion, piecewise-constant
+// prolongation (fine FLUID node += coarse (i/2, j/2)), nu2 sweeps; the coarsest level only
+// runs the nu1 pre-sweeps.  Level l has spacing h 2^l.  DIRICHLET nodes take phi_bc; without a
+// phi_bc array they keep the value phi holds, which below level 0 is the zeroed coarse phi:
+// what the reference's coarse phi_bc arrays, left at their cudaMemset zero (:124-137), give.
+// The reference's colour test `(i + j) & 1 != redblack` (:22) parses as
+// (i + j) & (1 != redblack): colour 0 updates the even nodes as intended, colour 1 updates
+// every interior node concurrently (a data race).  This restatement applies the intended
+// test, (i + j) & 1 == colour, to both colours.
+static const uint8_t kFluid = 0, kDirichlet = 1;
+
+// smooth_redblack (Multigrid_embedded.cu:15-33), one colour.
+static void emb_half_sweep(double* phi, const double* rhs, const uint8_t* mask, const double* bc, int nx, int ny,
+                           double h2, int colour) {
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j < ny - 1; ++j)
+    for (int i = 1 + ((1 + j + colour) & 1); i < nx - 1; i += 2) {
+      const int64_t id = (int64_t)j * nx + i;
+      if (mask[id] == kFluid) {
+        const double sum = phi[id - nx] + phi[id + nx] + phi[id - 1] + phi[id + 1];
+        phi[id] = 0.25 * (sum - h2 * rhs[id]);
+      } else if (mask[id] == kDirichlet && bc) {
+        phi[id] = bc[id];   // without phi_bc the node keeps the value phi holds
+      }
+    }
+}
+// residual_kernel (Multigrid_embedded.cu:35-55): r = rhs - lap(phi) / h^2 on interior FLUID
+// nodes, 0 on other interior nodes; boundary entries are left as they are (the reference's
+// res arrays are zeroed once and their boundary is never written).
+static void emb_residual(double* res, const double* phi, const double* rhs, const uint8_t* mask, int nx, int ny,
+                         double h2i) {
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j < ny - 1; ++j)
+    for (int i = 1; i < nx - 1; ++i) {
+      const int64_t id = (int64_t)j * nx + i;
+      if (mask[id] == kFluid) {
+        const double lap = phi[id - nx] + phi[id + nx] + phi[id - 1] + phi[id + 1] - 4.0 * phi[id];
+        res[id] = rhs[id] - h2i * lap;
+      } else {
+        res[id] = 0.0;
+      }
+    }
+}
+// restrict_kernel (Multigrid_embedded.cu:57-86) on interior coarse nodes: the coarse mask is
+// the fine node (2ic, 2jc)'s; FLUID coarse nodes get the full-weighted fine residual.
+// any: the coarse kind from the 3x3 fine nodes instead, the rule the reference's comment at
+// :73 states: DIRICHLET if any of them is, else SOLID if any is not FLUID, else FLUID.
+static uint8_t emb_coarse_kind(const uint8_t* mf, int64_t idf, int nxf, bool any) {
+  if (!any) return mf[idf];
+  bool dir = false, other = false;
+  for (int dj = -1; dj <= 1; ++dj)
+    for (int di = -1; di <= 1; ++di) {
+      const uint8_t m = mf[idf + (int64_t)dj * nxf + di];
+      dir |= m == kDirichlet;
+      other |= m != kFluid && m != kDirichlet;
+    }
+  return dir ? kDirichlet : other ? 2 : kFluid;
+}
+static void emb_restrict(const double* fine, double* coarse, const uint8_t* mf, uint8_t* mc, int nxf, int nxc,
+                         int nyc, bool any) {
+#pragma omp parallel for schedule(static)
+  for (int jc = 1; jc < nyc - 1; ++jc)
+    for (int ic = 1; ic < nxc - 1; ++ic) {
+      const int64_t idc = (int64_t)jc * nxc + ic, idf = (int64_t)(2 * jc) * nxf + 2 * ic;
+      const uint8_t m = emb_coarse_kind(mf, idf, nxf, any);
+      mc[idc] = m;
+      if (m == kFluid) {
+        double sum = 0.0;
+        sum += fine[idf];
+        sum += 0.5 * (fine[idf - 1] + fine[idf + 1] + fine[idf - nxf] + fine[idf + nxf]);
+        sum += 0.25 * (fine[idf - nxf - 1] + fine[idf - nxf + 1] + fine[idf + nxf - 1] + fine[idf + nxf + 1]);
+        coarse[idc] = sum / 4.0;
+      } else {
+        coarse[idc] = 0.0;
+      }
+    }
+}
+// prolongate_add_kernel (Multigrid_embedded.cu:88-104): interior FLUID fine nodes add the
+// coarse value at (i/2, j/2); bilinear: the bilinear interpolant of the coarse values instead.
+static void emb_prolong(const double* coarse, double* fine, const uint8_t* mf, int nxf, int nyf, int nxc,
+                        bool bilinear) {
+#pragma omp parallel for schedule(static)
+  for (int j = 1; j < nyf - 1; ++j)
+    for (int i = 1; i < nxf - 1; ++i) {
+      const int64_t idf = (int64_t)j * nxf + i;
+      if (mf[idf] != kFluid) continue;
+      const int64_t a = (int64_t)(j / 2) * nxc + i / 2;
+      const bool io = i & 1, jo = j & 1;
+      double v;
+      if (!bilinear || (!io && !jo)) v = coarse[a];
+      else if (io && !jo) v = 0.5 * (coarse[a] + coarse[a + 1]);
+      else if (!io && jo) v = 0.5 * (coarse[a] + coarse[a + nxc]);
+      else v = 0.25 * (coarse[a] + coarse[a + 1] + coarse[a + nxc] + coarse[a + nxc + 1]);
+      fine[idf] += v;
+    }
+}
+
+struct EmbWork {
+  int nx = 0, ny = 0, levels = 0;
+  std::vector<std::vector<double>> phi, rhs, res;
+  std::vector<std::vector<uint8_t>> mask;
+  std::vector<int> nxl, nyl;
+  void ensure(int nx_, int ny_, int levels_) {
+    if (nx_ == nx && ny_ == ny && levels_ == levels) return;
+    nx = nx_; ny = ny_; levels = levels_;
+    phi.assign(levels, {}); rhs.assign(levels, {}); res.assign(levels, {}); mask.assign(levels, {});
+    nxl.assign(levels, 0); nyl.assign(levels, 0);
+    int a = nx, b = ny;
+    for (int l = 0; l < levels; ++l) {
+      nxl[l] = a; nyl[l] = b;
+      phi[l].assign((size_t)a * b, 0.0); rhs[l].assign((size_t)a * b, 0.0);
+      res[l].assign((size_t)a * b, 0.0); mask[l].assign((size_t)a * b, 0);
+      a = (a - 1) / 2 + 1; b = (b - 1) / 2 + 1;   // Multigrid_embedded.cu:140-141
+    }
+  }
+};
+static EmbWork g_emb;
+
+// Multigrid::vcycle(l) (Multigrid_embedded.cu:159-188); level 0 works on the caller's arrays.
+static void emb_vcycle(EmbWork& w, int l, double* phi0, const double* rhs0, const uint8_t* mask0,
+                       const double* bc0, double h, int nu1, int nu2, int options) {
+  double* phi = l ? w.phi[l].data() : phi0;
+  const double* rhs = l ? w.rhs[l].data() : rhs0;
+  const uint8_t* mask = l ? w.mask[l].data() : mask0;
+  const double* bc = l ? nullptr : bc0;
+  const int nx = w.nxl[l], ny = w.nyl[l];
+  const double h2 = h * h * std::ldexp(1.0, 2 * l), h2i = 1.0 / h2;
+  for (int k = 0; k < nu1; ++k) {
+    emb_half_sweep(phi, rhs, mask, bc, nx, ny, h2, 0);
+    emb_half_sweep(phi, rhs, mask, bc, nx, ny, h2, 1);
+  }
+  if (l == w.levels - 1) return;
+  emb_residual(w.res[l].data(), phi, rhs, mask, nx, ny, h2i);
+  emb_restrict(w.res[l].data(), w.rhs[l + 1].data(), mask, w.mask[l + 1].data(), nx, w.nxl[l + 1], w.nyl[l + 1],
+               options & PIC_EMB_COARSEN_ANY);
+  std::fill(w.phi[l + 1].begin(), w.phi[l + 1].end(), 0.0);
+  emb_vcycle(w, l + 1, phi0, rhs0, mask0, bc0, h, nu1, nu2, options);
+  emb_prolong(w.phi[l + 1].data(), phi, mask, nx, ny, w.nxl[l + 1], options & PIC_EMB_PROLONG_BILINEAR);
+  for (int k = 0; k < nu2; ++k) {
+    emb_half_sweep(phi, rhs, mask, bc, nx, ny, h2, 0);
+    emb_half_sweep(phi, rhs, mask, bc, nx, ny, h2, 1);
+  }
+}
+// Squared norms over the interior FLUID nodes of level 0: [0] residual, [1] rhs.
+static void emb_norms(const double* phi, const double* rhs, const uint8_t* mask, int nx, int ny, double h,
+                      double out[2]) {
+  const double h2i = 1.0 / (h * h);
+  double r2 = 0.0, f2 = 0.0;
+#pragma omp parallel for reduction(+ : r2, f2) schedule(static)
+  for (int j = 1; j < ny - 1; ++j)
+    for (int i = 1; i < nx - 1; ++i) {
+      const int64_t id = (int64_t)j * nx + i;
+      if (mask[id] != kFluid) continue;
+      const double lap = phi[id - nx] + phi[id + nx] + phi[id - 1] + phi[id + 1] - 4.0 * phi[id];
+      const double r = rhs[id] - h2i * lap;
+      r2 += r * r;
+      f2 += rhs[id] * rhs[id];
+    }
+  out[0] = r2; out[1] = f2;
+}
+
+ORC_API void orc_emb_half_sweep(double* phi, const double* rhs, const uint8_t* mask, const double* bc, int nx, int ny,
+                                double h2, int colour) {
+  emb_half_sweep(phi, rhs, mask, bc, nx, ny, h2, colour);
+}
+ORC_API void orc_emb_residual(double* res, const double* phi, const double* rhs, const uint8_t* mask, int nx, int ny,
+                              double h2i) {
+  emb_residual(res, phi, rhs, mask, nx, ny, h2i);
+}
+ORC_API void orc_emb_restrict(const double* fine, double* coarse, const uint8_t* mf, uint8_t* mc, int nxf, int nyf,
+                              int nxc, int nyc, int options) {
+  (void)nyf;
+  emb_restrict(fine, coarse, mf, mc, nxf, nxc, nyc, options & PIC_EMB_COARSEN_ANY);
+}
+ORC_API void orc_emb_prolong(const double* coarse, double* fine, const uint8_t* mf, int nxf, int nyf, int nxc,
+                             int nyc, int options) {
+  (void)nyc;
+  emb_prolong(coarse, fine, mf, nxf, nyf, nxc, options & PIC_EMB_PROLONG_BILINEAR);
+}
+ORC_API void orc_emb_vcycles(double* phi, const double* rhs, const uint8_t* mask, const double* bc, int nx, int ny,
+                             int levels, double h, int nu1, int nu2, int options, int cycles) {
+  g_emb.ensure(nx, ny, levels);
+  for (int c = 0; c < cycles; ++c) emb_vcycle(g_emb, 0, phi, rhs, mask, bc, h, nu1, nu2, options);
+}
+// Relative residual of the embedded problem: ||r|| / ||rhs|| over the interior FLUID nodes,
+// or ||r|| / ||r_0|| (the residual of the initial guess) when rhs is zero there (a Laplace
+// problem driven by the electrodes alone); 0 when both are zero.
+static double emb_rel(const double n[2], double r0) {
+  if (n[1] > 0.0) return std::sqrt(n[0] / n[1]);
+  if (r0 > 0.0) return std::sqrt(n[0] / r0);
+  return std::sqrt(n[0]);
+}
+// V-cycles until the relative residual drops below tol or max_cycles ran (checked after every
+// cycle).  Returns the number of cycles; relres_out gets the final relative residual.
+ORC_API int orc_emb_solve(double* phi, const double* rhs, const uint8_t* mask, const double* bc, int nx, int ny,
+                          int levels, double h, int nu1, int nu2, int options, double tol, int max_cycles,
+                          double* relres_out) {
+  g_emb.ensure(nx, ny, levels);
+  double n[2];
+  emb_norms(phi, rhs, mask, nx, ny, h, n);
+  const double r0 = n[0];
+  int cyc = 0;
+  double rel = emb_rel(n, r0);
+  while (cyc < max_cycles) {
+    emb_vcycle(g_emb, 0, phi, rhs, mask, bc, h, nu1, nu2, options);
+    ++cyc;
+    emb_norms(phi, rhs, mask, nx, ny, h, n);
+    rel = emb_rel(n, r0);
+    if (rel < tol) break;
+  }
+  if (relres_out) *relres_out = rel;
+  return cyc;
+}
+ORC_API void orc_emb_norms(const double* phi, const double* rhs, const uint8_t* mask, int nx, int ny, double h,
+                           double out[2]) {
+  emb_norms(phi, rhs, mask, nx, ny, h, out);
+}
+
 // ------------------------------------------------------------------ cross sections
 struct Table {
   std::vector<double> e, s;

@@ -2,7 +2,8 @@
 //
 // TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile together with the reference's
 // sources where they lie (kernels.cu, collisions.cu, particles.cu, Multigrid.cu, grid.cu,
-// boundaries.cu, mcc.cu of dimad285/PIC_CUDA) into oracle/_ref/libpicref.so.  main.cu
+// boundaries.cu, mcc.cu, Multigrid_embedded.cu of dimad285/PIC_CUDA) into
+// oracle/_ref/libpicref.so.  main.cu
 // cannot be compiled (it needs GL/glew.h, render.h:4), so the step sequence of
 // updateSimulationCUDA (main.cu:60-135) is re-sequenced here without the viewer.
 // Every entry point takes and returns host arrays; it is used only to pin the FP64
@@ -81,6 +82,60 @@ RH_API int refh_efield(const double* phi, int m, int n, double dx, double dy, do
   int bad = ck(cudaDeviceSynchronize());
   cudaMemcpy(exy, dE, sizeof(double2) * m * n, cudaMemcpyDeviceToHost);
   cudaFree(dphi); cudaFree(dE);
+  return bad;
+}
+
+// The kernels of Multigrid_embedded.cu (compiled from the reference's file with -rdc; it has
+// no header), launched with the reference's 8x8 blocks (Multigrid_embedded.cu:162-163).
+__global__ void smooth_redblack(double* phi, const double* rhs, const unsigned char* mask, const double* phi_bc,
+                                int nx, int ny, double h2, int redblack);
+__global__ void residual_kernel(const double* phi, const double* rhs, const unsigned char* mask,
+                                const double* phi_bc, double* res, int nx, int ny, double h2i);
+__global__ void restrict_kernel(const double* fine, double* coarse, const unsigned char* mask_fine,
+                                unsigned char* mask_coarse, int nxf, int nyf, int nxc, int nyc);
+__global__ void prolongate_add_kernel(const double* coarse, double* fine, const unsigned char* mask_fine, int nxf,
+                                      int nyf, int nxc, int nyc);
+
+// On host arrays of an nx*ny level and its (nx-1)/2+1 x (ny-1)/2+1 coarse level:
+//   phi_sweep0    phi after smooth_redblack with redblack = 0 (the colour whose test the
+//                 reference evaluates as intended; redblack = 1 updates every node at once)
+//   res           residual_kernel of phi into a zeroed array
+//   rhs_c, mask_c restrict_kernel of res into zeroed arrays
+//   phi_prol      phi after prolongate_add_kernel of phi_c
+RH_API int refh_emb_kernels(int nx, int ny, const double* phi, const double* rhs, const unsigned char* mask,
+                            const double* bc, double h2, const double* phi_c, double* phi_sweep0, double* res,
+                            double* rhs_c, unsigned char* mask_c, double* phi_prol) {
+  const int nxc = (nx - 1) / 2 + 1, nyc = (ny - 1) / 2 + 1;
+  const size_t N = (size_t)nx * ny, Nc = (size_t)nxc * nyc;
+  double *dphi = nullptr, *drhs = nullptr, *dbc = nullptr, *dres = nullptr, *drc = nullptr, *dpc = nullptr;
+  unsigned char *dm = nullptr, *dmc = nullptr;
+  int bad = ck(cudaMalloc(&dphi, 8 * N)) | ck(cudaMalloc(&drhs, 8 * N)) | ck(cudaMalloc(&dbc, 8 * N)) |
+            ck(cudaMalloc(&dres, 8 * N)) | ck(cudaMalloc(&drc, 8 * Nc)) | ck(cudaMalloc(&dpc, 8 * Nc)) |
+            ck(cudaMalloc(&dm, N)) | ck(cudaMalloc(&dmc, Nc));
+  if (bad) return 1;
+  cudaMemcpy(drhs, rhs, 8 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dbc, bc, 8 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dm, mask, N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dpc, phi_c, 8 * Nc, cudaMemcpyHostToDevice);
+  cudaMemset(dres, 0, 8 * N);
+  cudaMemset(drc, 0, 8 * Nc);
+  cudaMemset(dmc, 0, Nc);
+  const dim3 t(8, 8), b((nx + 7) / 8, (ny + 7) / 8), bc2((nxc + 7) / 8, (nyc + 7) / 8);
+  cudaMemcpy(dphi, phi, 8 * N, cudaMemcpyHostToDevice);
+  smooth_redblack<<<b, t>>>(dphi, drhs, dm, dbc, nx, ny, h2, 0);
+  bad |= ck(cudaDeviceSynchronize());
+  cudaMemcpy(phi_sweep0, dphi, 8 * N, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dphi, phi, 8 * N, cudaMemcpyHostToDevice);
+  residual_kernel<<<b, t>>>(dphi, drhs, dm, dbc, dres, nx, ny, 1.0 / h2);
+  restrict_kernel<<<bc2, t>>>(dres, drc, dm, dmc, nx, ny, nxc, nyc);
+  prolongate_add_kernel<<<b, t>>>(dpc, dphi, dm, nx, ny, nxc, nyc);
+  bad |= ck(cudaDeviceSynchronize());
+  cudaMemcpy(res, dres, 8 * N, cudaMemcpyDeviceToHost);
+  cudaMemcpy(rhs_c, drc, 8 * Nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(mask_c, dmc, Nc, cudaMemcpyDeviceToHost);
+  cudaMemcpy(phi_prol, dphi, 8 * N, cudaMemcpyDeviceToHost);
+  cudaFree(dphi); cudaFree(drhs); cudaFree(dbc); cudaFree(dres); cudaFree(drc); cudaFree(dpc);
+  cudaFree(dm); cudaFree(dmc);
   return bad;
 }
 

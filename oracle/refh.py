@@ -29,6 +29,8 @@ def lib():
                                  C.c_double, _D, C.c_int, C.c_double, _D, _D, _D, _I, _I, _I,
                                  C.POINTER(C.c_float)]
         L.refh_elastic.argtypes = [C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, _D, _D, C.c_int]
+        _U8 = C.POINTER(C.c_uint8)
+        L.refh_emb_kernels.argtypes = [C.c_int, C.c_int, _D, _D, _U8, _D, C.c_double, _D, _D, _D, _D, _U8, _D]
         _lib = L
     return _lib
 
@@ -101,3 +103,22 @@ def elastic(vx, vy, mass, density, dt, xs_e, xs_s):
     e, s = np.ascontiguousarray(xs_e, np.float64), np.ascontiguousarray(xs_s, np.float64)
     assert lib().refh_elastic(len(vx), _d(vx), _d(vy), mass, density, dt, _d(e), _d(s), len(e)) == 0
     return vx, vy
+
+
+def emb_kernels(phi, rhs, mask, bc, h2, phi_c):
+    """The kernels of Multigrid_embedded.cu on one level: smooth_redblack(redblack=0),
+    residual_kernel, restrict_kernel of that residual, prolongate_add_kernel of phi_c."""
+    phi, rhs, bc = (np.ascontiguousarray(a, np.float64) for a in (phi, rhs, bc))
+    mask = np.ascontiguousarray(mask, np.uint8)
+    phi_c = np.ascontiguousarray(phi_c, np.float64)
+    ny, nx = phi.shape
+    nyc, nxc = phi_c.shape
+    assert (nxc, nyc) == ((nx - 1) // 2 + 1, (ny - 1) // 2 + 1)
+    u8 = C.POINTER(C.c_uint8)
+    out = {"phi_sweep0": np.empty_like(phi), "res": np.empty_like(phi), "rhs_c": np.empty((nyc, nxc)),
+           "mask_c": np.empty((nyc, nxc), np.uint8), "phi_prol": np.empty_like(phi)}
+    rc = lib().refh_emb_kernels(nx, ny, _d(phi), _d(rhs), mask.ctypes.data_as(u8), _d(bc), h2, _d(phi_c),
+                                _d(out["phi_sweep0"]), _d(out["res"]), _d(out["rhs_c"]),
+                                out["mask_c"].ctypes.data_as(u8), _d(out["phi_prol"]))
+    assert rc == 0
+    return out

@@ -23,6 +23,8 @@ PHASE_KICK, PHASE_MCC, PHASE_DRIFT, PHASE_WALLS, PHASE_DEPOSIT = 1, 2, 4, 8, 16
 GRID_RHO, GRID_PHI, GRID_EX, GRID_EY = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 OPT_MG_LEVELS_KERNEL, OPT_MG_CLUSTER_TOP, OPT_MG_COARSE_TOP = 1, 2, 3
+NODE_FLUID, NODE_DIRICHLET, NODE_SOLID = 0, 1, 2
+EMB_COARSEN_ANY, EMB_PROLONG_BILINEAR = 1, 2
 
 
 class SpeciesConfig(C.Structure):
@@ -100,6 +102,9 @@ _SIGS = {
     "pic_solve_multigrid_f64": (_I, [_VP, _VP, _I, _I, _I, C.c_double, C.c_double, _I, _I, _I, C.c_double, _I,
                                      _VP, C.POINTER(_I), _D]),
     "pic_efield_f64": (_I, [_VP, _VP, _I, _I, C.c_double, C.c_double, _VP]),
+    "pic_job_snapshot_positions": (_I, [_VP, _I, _I, _I64, _VP, C.POINTER(_I64), _I]),
+    "pic_solve_embedded_f64": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, C.c_double, _I, _I, _I, C.c_double, _I, _VP,
+                                    C.POINTER(_I), _D]),
     "pic_engine_set_option": (_I, [_VP, _I, _I64]),
     "pic_engine_get_option": (_I, [_VP, _I, C.POINTER(_I64)]),
     "pic_job_set_sort_every": (_I, [_VP, _I, _I]),

@@ -53,6 +53,21 @@ __global__ void export_kernel(const SlotDev* __restrict__ sd, int64_t n, double*
   }
 }
 
+// Interleaved FP32 (x, y) of every particle: what convertPositionsToFloat (kernels.cu:268-274)
+// writes into the reference's OpenGL vertex buffer, here into a plain buffer.  Rounded once from
+// the FP64 position the FP64 export returns.
+__global__ void snapshot_kernel(const SlotDev* __restrict__ sd, int64_t n, float2* __restrict__ xy, double dx,
+                                double dy) {
+  const SlotDev S = *sd;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = S.cell[p];
+    double gx, gy;
+    if (c != PIC_CELL_OUT) { gx = (double)cell_i(c) + (double)S.fx[p]; gy = (double)cell_j(c) + (double)S.fy[p]; }
+    else { gx = (double)S.fx[p]; gy = (double)S.fy[p]; }
+    xy[p] = make_float2((float)(gx * dx), (float)(gy * dy));
+  }
+}
+
 __global__ void export_raw_kernel(const SlotDev* __restrict__ sd, int64_t n, uint32_t* cell, float* fx, float* fy,
                                   float* vx, float* vy, float* vz, uint32_t* pid) {
   const SlotDev S = *sd;
@@ -210,6 +225,10 @@ void launch_export_species(const SlotDev* slot_dev, int64_t n, double* x, double
                            uint32_t* pid, double dx, double dy, cudaStream_t s) {
   if (n <= 0) return;
   export_kernel<<<grid_for(n), 256, 0, s>>>(slot_dev, n, x, y, vx, vy, vz, pid, dx, dy);
+}
+void launch_snapshot(const SlotDev* slot_dev, int64_t n, float* xy, double dx, double dy, cudaStream_t s) {
+  if (n <= 0) return;
+  snapshot_kernel<<<grid_for(n), 256, 0, s>>>(slot_dev, n, reinterpret_cast<float2*>(xy), dx, dy);
 }
 void launch_export_raw(const SlotDev* slot_dev, int64_t n, uint32_t* cell, float* fx, float* fy, float* vx, float* vy,
                        float* vz, uint32_t* pid, cudaStream_t s) {

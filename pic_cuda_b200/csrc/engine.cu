@@ -209,6 +209,7 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
   for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
   b += 4 * N;                                                         // second level-0 rhs
+  if (c.deposit_mode != PIC_DEPOSIT_I64) b += 16;                      // rho padding
   b += 24ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
   for (int s = 0; s < c.n_species; ++s) {
@@ -929,7 +930,13 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     int r_ = A((void**)&(ptr), (size_t)(bytes));           \
     if (r_) { free_job(E, J); return r_; }                 \
   } while (0)
-  if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, N * 4); else ALLOC(D.rho_i, N * 8);
+  // FP32 rho: 16-byte aligned and padded to whole 16-byte blocks (the deposit's vector
+  // reductions address the aligned block around a row's two nodes)
+  if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, round_up(N * 4, 16)); else ALLOC(D.rho_i, N * 8);
+  if (D.rho_f && (reinterpret_cast<uintptr_t>(D.rho_f) & 15)) {
+    free_job(E, J);
+    return fail(PIC_ERR_CUDA, "device pool returned a rho allocation that is not 16-byte aligned");
+  }
   ALLOC(D.efield, N * 8);
   ALLOC(D.phi64[0], N * 8);
   ALLOC(D.phi64[1], N * 8);
@@ -1182,6 +1189,35 @@ int pic_job_export_species(pic_engine* E, int job, int species, int64_t capacity
     for (int k = 0; k < 5; ++k)
       if (dst[k]) CK(cudaMemcpyAsync(dst[k], b[k], nb, cudaMemcpyDeviceToHost, s));
     if (pid) CK(cudaMemcpyAsync(pid, pb, (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return PIC_OK;
+}
+
+int pic_job_snapshot_positions(pic_engine* E, int job, int species, int64_t capacity, float* xy, int64_t* n_out,
+                               int memory) {
+  int rc = check_job(E, job);
+  if (rc) return rc;
+  JobHost& J = E->jobs[job];
+  if (species < 0 || species >= J.cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
+  if (!xy && capacity > 0) return fail(PIC_ERR_ARG, "null output buffer");
+  CK(cudaSetDevice(E->device));
+  cudaStream_t s = E->stream;
+  int n = 0;
+  rc = read_count(E, job, species, &n);   // positions do not depend on a pending kick: no flush
+  if (rc) return rc;
+  if (n_out) *n_out = n;
+  if (n > capacity) return fail(PIC_ERR_CAPACITY, "output buffer too small");
+  const double dxv = J.cfg.Lx / (J.cfg.nx - 1), dyv = J.cfg.Ly / (J.cfg.ny - 1);
+  const SlotDev* sd = E->d_slots + job * kSlotsPerJob + species;
+  if (memory == PIC_MEM_DEVICE) {
+    launch_snapshot(sd, n, xy, dxv, dyv, s);
+  } else if (n > 0) {
+    rc = ensure_stage(E, (size_t)n * 8);
+    if (rc) return rc;
+    launch_snapshot(sd, n, (float*)E->d_stage, dxv, dyv, s);
+    CK(cudaMemcpyAsync(xy, E->d_stage, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());

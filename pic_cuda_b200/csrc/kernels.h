@@ -104,6 +104,7 @@ void launch_load_species(const SlotDev* slot_dev, const JobDev* job_dev, int64_t
                          int ncy, cudaStream_t s);
 void launch_export_species(const SlotDev* slot_dev, int64_t n, double* x, double* y, double* vx, double* vy,
                            double* vz, uint32_t* pid, double dx, double dy, cudaStream_t s);
+void launch_snapshot(const SlotDev* slot_dev, int64_t n, float* xy, double dx, double dy, cudaStream_t s);
 void launch_export_raw(const SlotDev* slot_dev, int64_t n, uint32_t* cell, float* fx, float* fy, float* vx,
                        float* vy, float* vz, uint32_t* pid, cudaStream_t s);
 void launch_grid_export(const JobDev* job_dev, const JobState* st_dev, int which, double* out, int nx, int ny,
@@ -112,3 +113,22 @@ void launch_grid_import(const JobDev* job_dev, const JobState* st_dev, int which
                         int ny, cudaStream_t s);
 void launch_zero_rho(const JobDev* job_dev, int64_t nodes, int deposit_mode, void* rho, cudaStream_t s);
 void launch_efield_f64(const double* phi, double* exy, int nx, int ny, double dx, double dy, cudaStream_t s);
+
+// ---- embedded-boundary multigrid (mg_embedded.cu)
+// Level arrays of one embedded solve.  phi[l] is where level l's result ends up; alt[l] is the
+// second buffer the tile kernels write into (levels above the one-CTA ones); bc[l] may be
+// null (DIRICHLET nodes then keep their phi).
+struct EmbLevels {
+  int L = 0, lc = 0;
+  int nx[PIC_MAX_LEVELS] = {}, ny[PIC_MAX_LEVELS] = {};
+  double* phi[PIC_MAX_LEVELS] = {};
+  double* alt[PIC_MAX_LEVELS] = {};
+  double* rhs[PIC_MAX_LEVELS] = {};
+  uint8_t* mask[PIC_MAX_LEVELS] = {};
+  const double* bc[PIC_MAX_LEVELS] = {};
+  double h = 0.0;
+};
+// Level sizes and the first level the one-CTA kernel solves.
+void emb_layout(EmbLevels& P, int nx, int ny, int levels);
+// One V-cycle of Multigrid::vcycle(l0) (Multigrid_embedded.cu:159-188) on P's arrays.
+int emb_vcycle(const EmbLevels& P, int l0, int nu1, int nu2, int options, cudaStream_t s);

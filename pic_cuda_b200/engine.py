@@ -88,6 +88,32 @@ class Job:
                                                    p(out["pid"]), C.byref(n)), "pic_job_export_species_raw")
         return {k: v[: n.value] for k, v in out.items()}
 
+    def snapshot_positions(self, species: int, device: bool = False):
+        """Interleaved FP32 (x, y) of every particle, shape (n, 2): the headless counterpart of
+        the reference's vertex-buffer fill (kernels.cu:268-274).  device=True returns a CUDA
+        torch tensor filled on the device, else a numpy array."""
+        cap = int(self.cfg.species[species].capacity)
+        n = C.c_int64()
+        if device:
+            import torch
+            out = torch.empty((cap, 2), dtype=torch.float32, device=torch.device("cuda", self.engine.device))
+            ptr, mem = C.c_void_p(out.data_ptr()), L.MEM_DEVICE
+        else:
+            out = np.empty((cap, 2), np.float32)
+            ptr, mem = out.ctypes.data_as(C.c_void_p), L.MEM_HOST
+        L.check(L.lib().pic_job_snapshot_positions(self.engine.h, self.id, species, cap, ptr, C.byref(n), mem),
+                "pic_job_snapshot_positions")
+        return out[: n.value]
+
+    def write_snapshot(self, path) -> None:
+        """Positions of every species and the job's diagnostics to one .npz file (the headless
+        replacement of the reference's viewer frame)."""
+        data = {f"xy{s}": self.snapshot_positions(s) for s in range(int(self.cfg.n_species))}
+        d = self.diagnostics()
+        for k, v in d.items():
+            data[f"diag_{k}"] = np.asarray(v)
+        np.savez_compressed(path, **data)
+
     def hits(self, species: int) -> np.ndarray:
         cap = int(self.cfg.species[species].capacity)
         buf = np.empty(max(cap, 1), np.int64)
@@ -211,4 +237,21 @@ def solve_multigrid_f64(phi, rho, nx: int, ny: int, levels: int, h: float, omega
                                          C.byref(rel))
     if rc not in (L.PIC_OK, L.PIC_ERR_NOT_CONVERGED):
         L.check(rc, "pic_solve_multigrid_f64")
+    return cyc.value, rel.value, rc == L.PIC_OK
+
+
+def solve_embedded_f64(phi, rhs, mask, phi_bc, levels: int, h: float, nu_pre: int = 2, nu_post: int = 2,
+                       options: int = 0, tol: float = 1e-10, max_cycles: int = 100):
+    """Embedded-boundary multigrid (Multigrid_embedded.cu:110-188) on CUDA torch tensors:
+    phi, rhs, phi_bc FP64 and mask uint8 (PIC_NODE_*), all (ny, nx); phi in place; phi_bc may
+    be None.  Returns (cycles, relative residual, converged)."""
+    ny, nx = phi.shape
+    cyc = C.c_int()
+    rel = C.c_double()
+    bc = C.c_void_p(phi_bc.data_ptr()) if phi_bc is not None else None
+    rc = L.lib().pic_solve_embedded_f64(C.c_void_p(phi.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                        C.c_void_p(mask.data_ptr()), bc, nx, ny, levels, h, nu_pre, nu_post, options,
+                                        tol, max_cycles, None, C.byref(cyc), C.byref(rel))
+    if rc not in (L.PIC_OK, L.PIC_ERR_NOT_CONVERGED):
+        L.check(rc, "pic_solve_embedded_f64")
     return cyc.value, rel.value, rc == L.PIC_OK

@@ -18,6 +18,8 @@
 //           out: f64 v[2N], v_abs[N], energy[N], crs[N], f64 table energies, sigmas
 //   solve   in: i32[n, levels], f64[h, omega], f64 phi0[n*n], rho[n*n]
 //           out: f64 phi[n*n]
+//   embedded in: i32[nx, ny, levels, cycles], f64[h], f64 phi0, rhs, phi_bc [nx*ny], u8 mask
+//           out: f64 phi[nx*ny] after `cycles` vcycle(0) calls, level 1's f64 rhs and u8 mask
 //   kernels in: i32[m], f64[dx, dt], f64 q[S], m[S], walls[4W], r[2N], v[2N], i32 type[N],
 //               f64 phi[m*m], f64 table energies, sigmas
 //           (the reference's kernel sequence main.cu:64-127 plus kernels.cu:196-274, one
@@ -36,6 +38,7 @@
 #include <vector>
 
 #include "compat/Multigrid.hpp"
+#include "compat/Multigrid_embedded.hpp"
 #include "compat/boundaries.h"
 #include "compat/collisions.cuh"
 #include "compat/diagnostics.h"
@@ -215,6 +218,27 @@ void run_solve(In& in, Out& out) {
   cudaFree(rho_d);
 }
 
+// The reference's embedded-boundary class (Multigrid_embedded.cu:106-190) used as its
+// vcycle is written to be used: fill level 0, call vcycle(0) repeatedly.
+void run_embedded(In& in, Out& out) {
+  const auto hi = in.rec<int32_t>();
+  const double h = in.rec<double>()[0];
+  const auto phi0 = in.rec<double>(), rhs = in.rec<double>(), bc = in.rec<double>();
+  const auto mask = in.rec<uint8_t>();
+  const int nx = hi[0], ny = hi[1], levels = hi[2], cycles = hi[3];
+  Multigrid mg(nx, ny, levels, h);
+  h2d(mg.levels[0].phi, phi0);
+  h2d(mg.levels[0].rhs, rhs);
+  h2d(mg.levels[0].phi_bc, bc);
+  h2d(mg.levels[0].mask, mask);
+  for (int c = 0; c < cycles; ++c) mg.vcycle(0);
+  ck(cudaDeviceSynchronize());
+  const MGLevel& L1 = mg.levels[levels > 1 ? 1 : 0];
+  out.rec(d2h(mg.levels[0].phi, (size_t)nx * ny));
+  out.rec(d2h(L1.rhs, (size_t)L1.nx * L1.ny));
+  out.rec(d2h(L1.mask, (size_t)L1.nx * L1.ny));
+}
+
 void run_kernels(In& in, Out& out) {
   const int gm = in.rec<int32_t>()[0];
   const auto hd = in.rec<double>();
@@ -292,6 +316,7 @@ int main(int argc, char** argv) {
     else if (mode == "elastic") run_elastic(in, out, argc > 4 ? argv[4] : "");
     else if (mode == "solve") run_solve(in, out);
     else if (mode == "kernels") run_kernels(in, out);
+    else if (mode == "embedded") run_embedded(in, out);
     else throw std::runtime_error("unknown mode");
   } catch (const std::exception& e) {
     fprintf(stderr, "compat_driver: %s\n", e.what());

@@ -1,7 +1,7 @@
 """Generates tests/golden/*.npz from the reference's own CUDA kernels.
 
 Runs where a GPU and oracle/_ref/libpicref.so (built by `make -C oracle ref` from the
-reference's sources) are available:  python tests/golden/make_golden.py [outdir]
+reference's sources) are available:  python tests/golden/make_golden.py [outdir] [--only embedded]
 Every fixture stores its seeded inputs and the reference's outputs; tests/test_golden.py
 checks that the FP64 oracle reproduces them (CPU only).
 """
@@ -19,9 +19,13 @@ Q, M = [0.1, -1.0], [1.0, 1.0]
 WALLS = [[0, 0, 1, 0], [1, 0, 1, 1], [1, 1, 0, 1], [0, 1, 0, 0], [0.25, 0.25, 0.25, 0.75], [0.75, 0.25, 0.75, 0.75]]
 
 
-def main(out: Path):
+def main(out: Path, only: str | None = None):
     out.mkdir(parents=True, exist_ok=True)
     assert refh.available(), "needs a GPU and oracle/_ref/libpicref.so"
+    if only in (None, "embedded"):
+        embedded(out)
+    if only == "embedded":
+        return
     rng = np.random.default_rng(20240601)
     # updateDensity (kernels.cu:26)
     n = 4000
@@ -57,5 +61,28 @@ def main(out: Path):
     print("wrote", sorted(p.name for p in out.glob("*.npz")))
 
 
+def embedded(out: Path):
+    """The kernels of Multigrid_embedded.cu on a rectangular level with an electrode whose
+    edges sit on odd and even node indices and a solid block (own seed)."""
+    rng = np.random.default_rng(20241203)
+    nx, ny = 65, 49
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[12:25, 16:31] = 1
+    mask[30:41, 40:52] = 2
+    bc = np.zeros((ny, nx))
+    bc[mask == 1] = 2.5
+    phi = rng.standard_normal((ny, nx))
+    rhs = rng.standard_normal((ny, nx))
+    h2 = (1.0 / 64) ** 2
+    phi_c = rng.standard_normal(((ny - 1) // 2 + 1, (nx - 1) // 2 + 1))
+    r = refh.emb_kernels(phi, rhs, mask, bc, h2, phi_c)
+    np.savez_compressed(out / "ref_embedded.npz", phi=phi, rhs=rhs, mask=mask, bc=bc, h2=h2, phi_c=phi_c, **r)
+
+
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("outdir", nargs="?", default=str(Path(__file__).resolve().parent))
+    ap.add_argument("--only", choices=["embedded"], default=None, help="write only this fixture")
+    a = ap.parse_args()
+    main(Path(a.outdir), a.only)

@@ -235,3 +235,60 @@ def test_oracle_extrapolated_warm_start(orc):
         res[ws] = (cyc, s.grid(L.GRID_PHI))
     assert sum(res[1][0][2:]) < sum(res[0][0][2:])
     assert np.linalg.norm(res[1][1] - res[0][1]) <= 1e-6 * np.linalg.norm(res[0][1])
+
+
+# ---- embedded-boundary multigrid (Multigrid_embedded.cu), oracle known answers
+def _emb_problem(n, seed=0):
+    rng = np.random.default_rng(seed)
+    mask = np.zeros((n, n), np.uint8)
+    mask[n // 4: n // 2, n // 4: n // 2 + 1] = 1        # electrode, edges on odd and even nodes
+    mask[3 * n // 5: 3 * n // 4, 3 * n // 5: 4 * n // 5] = 2
+    bc = np.where(mask == 1, 2.5, 0.0)
+    return 0.1 * rng.standard_normal((n, n)), rng.standard_normal((n, n)), mask, bc
+
+
+def test_embedded_half_sweep_colours_and_kinds(orc):
+    """Colour 0 updates only interior nodes with (i + j) even, colour 1 only odd ones (the
+    intended test of Multigrid_embedded.cu:22); DIRICHLET nodes take phi_bc, SOLID ones and the
+    boundary keep phi."""
+    n = 33
+    phi, rhs, mask, bc = _emb_problem(n, 1)
+    j, i = np.mgrid[0:n, 0:n]
+    interior = (i > 0) & (j > 0) & (i < n - 1) & (j < n - 1)
+    for colour in (0, 1):
+        out = orc.emb_half_sweep(phi, rhs, mask, bc, (1.0 / (n - 1)) ** 2, colour)
+        changed = out != phi
+        this = interior & (((i + j) & 1) == colour)
+        assert not np.any(changed & ~this)
+        assert np.all(changed[this & (mask == 0)])
+        assert np.all(out[this & (mask == 1)] == 2.5)
+        assert np.array_equal(out[mask == 2], phi[mask == 2])
+
+
+def test_embedded_all_fluid_is_textbook_multigrid(orc):
+    """With every node FLUID and bilinear prolongation the V(2,2) cycle contracts the residual
+    like the standard Poisson multigrid (below 0.1 per cycle)."""
+    n = 129
+    h = 1.0 / (n - 1)
+    rng = np.random.default_rng(2)
+    rhs = rng.standard_normal((n, n))
+    mask = np.zeros((n, n), np.uint8)
+    phi = np.zeros((n, n))
+    r = [np.sqrt(orc.emb_norms(phi, rhs, mask, h)[0])]
+    for _ in range(4):
+        phi = orc.emb_vcycles(phi, rhs, mask, None, h, 7, 1, options=2)
+        r.append(np.sqrt(orc.emb_norms(phi, rhs, mask, h)[0]))
+    assert all(r[k + 1] < 0.1 * r[k] for k in range(1, 4))
+
+
+def test_embedded_reference_operators_diverge_coarsen_any_converges(orc):
+    """The reference's injected coarse kinds shrink an electrode whose edge sits on an odd node,
+    and its V-cycle diverges at 257^2; the coarsening its comment states (:73) converges."""
+    n = 257
+    h = 1.0 / (n - 1)
+    phi, rhs, mask, bc = _emb_problem(n, 5)
+    _, cyc, rel = orc.emb_solve(phi, rhs, mask, bc, h, 8, tol=1e-10, max_cycles=30, options=0)
+    assert cyc == 30 and rel > 1.0
+    out, cyc, rel = orc.emb_solve(phi, rhs, mask, bc, h, 8, tol=1e-10, max_cycles=100, options=1)
+    assert rel < 1e-10 and cyc < 100
+    assert np.all(out[mask == 1] == 2.5)
