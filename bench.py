@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="mcc_mixed", choices=["plain_small", "mcc_mixed", "large", "batched", "served"])
+    ap.add_argument("--workload", default="mcc_mixed",
+                    choices=["plain_small", "mcc_mixed", "large", "batched", "served", "embedded"])
     ap.add_argument("--jobs", type=int, default=None, help="batched: jobs; served: requests")
     ap.add_argument("--ppc-scale", type=float, default=None, help="batched/served: particles-per-cell factor")
     ap.add_argument("--steps-scale", type=float, default=None, help="served: request step-count factor")
@@ -450,9 +451,134 @@ def run_served_bench(args):
     print(json.dumps(line), flush=True)
 
 
+# Embedded-boundary multigrid (Multigrid_embedded.cu) on its own: 4097^2 nodes (the large
+# configuration's grid; ~0.55 GB of level arrays, larger than L2), an electrode at 2.5 whose
+# edges sit on odd and even nodes and a solid block, random charge, V(2,2) cycles over 10
+# levels with the coarsening the reference's comment states and bilinear prolongation.
+EMB_N, EMB_LEVELS = 4097, 10
+
+
+def embedded_problem(n):
+    import numpy as np
+    rng = np.random.default_rng(4242)
+    mask = np.zeros((n, n), np.uint8)
+    mask[n // 4: n // 2, n // 4: n // 2 + 1] = 1
+    mask[3 * n // 5: 3 * n // 4, 3 * n // 5: 4 * n // 5] = 2
+    bc = np.where(mask == 1, 2.5, 0.0)
+    return np.zeros((n, n)), rng.standard_normal((n, n)), mask, bc
+
+
+def embedded_bytes_per_cycle(n, levels):
+    """Algorithmic HBM bytes of one V-cycle: per level above the one-CTA ones, pre-smoothing
+    (phi, rhs read and phi written: 24 B/node, kinds 1 B), restriction (phi, rhs, kinds read:
+    17 B/node; coarse rhs, kinds, phi written: 17 B per coarse node) and prolongation +
+    post-smoothing (24 + 1 B/node, coarse phi 8 B per coarse node); the one-CTA levels read and
+    write their arrays once (25 B/node)."""
+    b, a = 0, n
+    for l in range(levels):
+        N, Nc = a * a, ((a - 1) // 2 + 1) ** 2
+        if N <= 65 * 65:
+            b += 25 * N
+        else:
+            b += 25 * N + 17 * N + 17 * Nc + 25 * N + 8 * Nc
+        a = (a - 1) // 2 + 1
+    return b
+
+
+def run_embedded_bench(args):
+    import numpy as np
+    import torch
+    from oracle import oracle as orc
+    from pic_cuda_b200 import _lib as L
+    from pic_cuda_b200.engine import solve_embedded_f64
+    unit = "V-cycles/s"
+    n, levels = EMB_N, EMB_LEVELS
+    h = 1.0 / (n - 1)
+    phi, rhs, mask, bc = embedded_problem(n)
+    opts = L.EMB_COARSEN_ANY | L.EMB_PROLONG_BILINEAR
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        cyc = max(1, min(args.steps, args.cpu_steps))
+        orc.emb_vcycles(phi, rhs, mask, bc, h, levels, 1, options=opts)
+        t0 = time.perf_counter()
+        orc.emb_vcycles(phi, rhs, mask, bc, h, levels, cyc, options=opts)
+        v = cyc / (time.perf_counter() - t0)
+        print(json.dumps({"metric": f"embedded-boundary multigrid {unit}", "value": v, "unit": unit, "impl": "reference",
+                          "n_gpus": args.gpus, "steps": cyc, "warmup": 1, "higher_is_better": True,
+                          "dtype": "f64", "data": "synthetic", "config": {"workload": "embedded", "grid": f"{n}x{n}"},
+                          "cpu_baseline": {"value": v, "unit": unit, "cores": orc.num_threads(), "kind": "port",
+                                           "sample": f"{cyc} oracle V-cycles"},
+                          "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+              flush=True)
+        return
+    dev = torch.device("cuda", 0)
+    d = {k: torch.tensor(a, device=dev) for k, a in (("phi", phi), ("rhs", rhs), ("mask", mask), ("bc", bc))}
+    stream = torch.cuda.current_stream(dev)
+    solve_embedded_f64(d["phi"], d["rhs"], d["mask"], d["bc"], levels, h, 2, 2, opts, tol=0.0,
+                       max_cycles=max(args.warmup, 3))
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        solve_embedded_f64(d["phi"], d["rhs"], d["mask"], d["bc"], levels, h, 2, 2, opts, tol=0.0,
+                           max_cycles=args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    peak, peak_kind = peaks()
+    bpc = embedded_bytes_per_cycle(n, levels)
+    # end to end: pinned host arrays in, a solve to 1e-8 (at most 200 V-cycles) through the C ABI,
+    # phi back to the host
+    hp = {k: torch.from_numpy(a).pin_memory() for k, a in (("phi", phi), ("rhs", rhs), ("mask", mask), ("bc", bc))}
+    out = torch.empty_like(hp["phi"]).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dd = {k: v.to(dev, non_blocking=True) for k, v in hp.items()}
+    cyc, rel, ok = solve_embedded_f64(dd["phi"], dd["rhs"], dd["mask"], dd["bc"], levels, h, 2, 2, opts, tol=1e-8,
+                                      max_cycles=200)
+    out.copy_(dd["phi"])
+    e2e_s = time.perf_counter() - t0
+    # the reference's own kernels in its V-cycle sequence on the same B200 and problem
+    ref = None
+    try:
+        from oracle import refh
+        if refh.available():
+            _, ref_ms = refh.emb_vcycles_timed(phi, rhs, mask, bc, h, levels, 20, warmup=3)
+            ref = {"ms_per_vcycle": ref_ms, "vcycles_per_s": 1000.0 / ref_ms, "speedup": ref_ms / ms,
+                   "path": "Multigrid::vcycle (Multigrid_embedded.cu:159-188) re-sequenced on the reference's "
+                           "kernels, 8x8 blocks, legacy stream; its colour test races (:22)"}
+    except (OSError, AssertionError) as e:
+        ref = {"unavailable": str(e)}
+    line = {"metric": f"embedded-boundary multigrid {unit}", "value": 1000.0 / ms, "unit": unit, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "embedded", "grid": f"{n}x{n}", "levels": levels, "sweeps": "2+2",
+                       "options": "coarsen any + bilinear prolongation",
+                       "l2": "level arrays larger than L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "achieved": bpc / (ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bpc / (ms / 1000.0) / 1e9 / peak, "traffic": None, "kernel": "whole V-cycle",
+                         "bytes_per_vcycle": bpc, "peak_source": f"{peak_kind} hbm_gbs"},
+            "clocks": clk.summary(),
+            "e2e": {"value": cyc / e2e_s, "unit": unit, "h2d_bytes_per_step": 25 * n * n / cyc,
+                    "d2h_bytes_per_step": 8 * n * n / cyc, "cycles": cyc, "relres": rel, "converged": ok,
+                    "seconds": e2e_s},
+            "reference_cuda": ref}
+    if not args.no_cpu_baseline:
+        cyc_cpu = max(1, args.cpu_steps)
+        orc.emb_vcycles(phi, rhs, mask, bc, h, levels, 1, options=opts)
+        t0 = time.perf_counter()
+        orc.emb_vcycles(phi, rhs, mask, bc, h, levels, cyc_cpu, options=opts)
+        line["cpu_baseline"] = {"value": cyc_cpu / (time.perf_counter() - t0), "unit": unit,
+                                "cores": orc.num_threads(), "kind": "port", "sample": f"{cyc_cpu} oracle V-cycles"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "embedded":
+        run_embedded_bench(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":
         run_batched_bench(args)

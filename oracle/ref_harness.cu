@@ -8,6 +8,7 @@
 // updateSimulationCUDA (main.cu:60-135) is re-sequenced here without the viewer.
 // Every entry point takes and returns host arrays; it is used only to pin the FP64
 // oracle (tests/golden/make_golden.py) and to time the reference's CUDA step.
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -136,6 +137,74 @@ RH_API int refh_emb_kernels(int nx, int ny, const double* phi, const double* rhs
   cudaMemcpy(phi_prol, dphi, 8 * N, cudaMemcpyDeviceToHost);
   cudaFree(dphi); cudaFree(drhs); cudaFree(dbc); cudaFree(dres); cudaFree(drc); cudaFree(dpc);
   cudaFree(dm); cudaFree(dmc);
+  return bad;
+}
+
+// Multigrid::vcycle (Multigrid_embedded.cu:159-188) re-sequenced on the reference's kernels:
+// the class itself cannot be linked (its members are defined inside the class body of a .cu
+// file with no header).  Level arrays as its constructor makes them (:119-146).  Runs `cycles`
+// V-cycles from level 0 after `warmup` untimed ones and returns phi and the mean time per
+// V-cycle (CUDA events on the legacy stream, as the class launches).  The second colour of
+// its smoother updates every node at once (:22), so phi is what the reference computes, races
+// included; only the time is meant to be compared.
+namespace {
+struct RefEmbLevel { int nx, ny; double *phi, *rhs, *res, *bc; unsigned char* mask; };
+void ref_emb_vcycle(std::vector<RefEmbLevel>& Ls, int l, double h) {
+  RefEmbLevel& L = Ls[l];
+  const dim3 t(8, 8), b((L.nx + 7) / 8, (L.ny + 7) / 8);
+  const double h2 = h * h * std::pow(2.0, l) * std::pow(2.0, l), h2i = 1.0 / h2;
+  for (int k = 0; k < 2; ++k) {
+    smooth_redblack<<<b, t>>>(L.phi, L.rhs, L.mask, L.bc, L.nx, L.ny, h2, 0);
+    smooth_redblack<<<b, t>>>(L.phi, L.rhs, L.mask, L.bc, L.nx, L.ny, h2, 1);
+  }
+  if (l == (int)Ls.size() - 1) return;
+  residual_kernel<<<b, t>>>(L.phi, L.rhs, L.mask, L.bc, L.res, L.nx, L.ny, h2i);
+  RefEmbLevel& C = Ls[l + 1];
+  const dim3 bc((C.nx + 7) / 8, (C.ny + 7) / 8);
+  restrict_kernel<<<bc, t>>>(L.res, C.rhs, L.mask, C.mask, L.nx, L.ny, C.nx, C.ny);
+  cudaMemset(C.phi, 0, sizeof(double) * C.nx * C.ny);
+  ref_emb_vcycle(Ls, l + 1, h);
+  prolongate_add_kernel<<<b, t>>>(C.phi, L.phi, L.mask, L.nx, L.ny, C.nx, C.ny);
+  for (int k = 0; k < 2; ++k) {
+    smooth_redblack<<<b, t>>>(L.phi, L.rhs, L.mask, L.bc, L.nx, L.ny, h2, 0);
+    smooth_redblack<<<b, t>>>(L.phi, L.rhs, L.mask, L.bc, L.nx, L.ny, h2, 1);
+  }
+}
+}  // namespace
+
+RH_API int refh_emb_vcycles(int nx, int ny, int levels, double h, int warmup, int cycles, double* phi,
+                            const double* rhs, const unsigned char* mask, const double* bc, float* ms_per_cycle) {
+  std::vector<RefEmbLevel> Ls;
+  int bad = 0;
+  for (int l = 0, a = nx, b = ny; l < levels; ++l, a = (a - 1) / 2 + 1, b = (b - 1) / 2 + 1) {
+    RefEmbLevel L{a, b, nullptr, nullptr, nullptr, nullptr, nullptr};
+    const size_t N = (size_t)a * b;
+    bad |= ck(cudaMalloc(&L.phi, 8 * N)) | ck(cudaMalloc(&L.rhs, 8 * N)) | ck(cudaMalloc(&L.res, 8 * N)) |
+           ck(cudaMalloc(&L.bc, 8 * N)) | ck(cudaMalloc(&L.mask, N));
+    if (bad) return 1;
+    cudaMemset(L.phi, 0, 8 * N); cudaMemset(L.rhs, 0, 8 * N); cudaMemset(L.res, 0, 8 * N);
+    cudaMemset(L.bc, 0, 8 * N); cudaMemset(L.mask, 0, N);
+    Ls.push_back(L);
+  }
+  const size_t N = (size_t)nx * ny;
+  cudaMemcpy(Ls[0].phi, phi, 8 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(Ls[0].rhs, rhs, 8 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(Ls[0].mask, mask, N, cudaMemcpyHostToDevice);
+  cudaMemcpy(Ls[0].bc, bc, 8 * N, cudaMemcpyHostToDevice);
+  for (int c = 0; c < warmup; ++c) ref_emb_vcycle(Ls, 0, h);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0); cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  for (int c = 0; c < cycles; ++c) ref_emb_vcycle(Ls, 0, h);
+  cudaEventRecord(e1);
+  bad |= ck(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (ms_per_cycle) *ms_per_cycle = cycles > 0 ? ms / cycles : 0.f;
+  cudaMemcpy(phi, Ls[0].phi, 8 * N, cudaMemcpyDeviceToHost);
+  bad |= ck(cudaGetLastError());
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  for (auto& L : Ls) { cudaFree(L.phi); cudaFree(L.rhs); cudaFree(L.res); cudaFree(L.bc); cudaFree(L.mask); }
   return bad;
 }
 

@@ -31,6 +31,8 @@ def lib():
         L.refh_elastic.argtypes = [C.c_int, _D, _D, C.c_double, C.c_double, C.c_double, _D, _D, C.c_int]
         _U8 = C.POINTER(C.c_uint8)
         L.refh_emb_kernels.argtypes = [C.c_int, C.c_int, _D, _D, _U8, _D, C.c_double, _D, _D, _D, _D, _U8, _D]
+        L.refh_emb_vcycles.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D, _D, _U8, _D,
+                                       C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -122,3 +124,16 @@ def emb_kernels(phi, rhs, mask, bc, h2, phi_c):
                                 out["mask_c"].ctypes.data_as(u8), _d(out["phi_prol"]))
     assert rc == 0
     return out
+
+
+def emb_vcycles_timed(phi, rhs, mask, bc, h, levels, cycles, warmup=2):
+    """Multigrid::vcycle re-sequenced on the reference's kernels; returns (phi, ms per V-cycle)."""
+    phi = np.ascontiguousarray(phi, np.float64).copy()
+    rhs, bc = np.ascontiguousarray(rhs, np.float64), np.ascontiguousarray(bc, np.float64)
+    mask = np.ascontiguousarray(mask, np.uint8)
+    ny, nx = phi.shape
+    ms = C.c_float(0)
+    rc = lib().refh_emb_vcycles(nx, ny, levels, h, warmup, cycles, _d(phi), _d(rhs),
+                                mask.ctypes.data_as(C.POINTER(C.c_uint8)), _d(bc), C.byref(ms))
+    assert rc == 0
+    return phi, ms.value

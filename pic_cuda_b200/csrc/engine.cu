@@ -209,7 +209,6 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
   for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
   b += 4 * N;                                                         // second level-0 rhs
-  if (c.deposit_mode != PIC_DEPOSIT_I64) b += 16;                      // rho padding
   b += 24ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
   for (int s = 0; s < c.n_species; ++s) {
@@ -930,13 +929,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     int r_ = A((void**)&(ptr), (size_t)(bytes));           \
     if (r_) { free_job(E, J); return r_; }                 \
   } while (0)
-  // FP32 rho: 16-byte aligned and padded to whole 16-byte blocks (the deposit's vector
-  // reductions address the aligned block around a row's two nodes)
-  if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, round_up(N * 4, 16)); else ALLOC(D.rho_i, N * 8);
-  if (D.rho_f && (reinterpret_cast<uintptr_t>(D.rho_f) & 15)) {
-    free_job(E, J);
-    return fail(PIC_ERR_CUDA, "device pool returned a rho allocation that is not 16-byte aligned");
-  }
+  if (c.deposit_mode == PIC_DEPOSIT_F32) ALLOC(D.rho_f, N * 4); else ALLOC(D.rho_i, N * 8);
   ALLOC(D.efield, N * 8);
   ALLOC(D.phi64[0], N * 8);
   ALLOC(D.phi64[1], N * 8);

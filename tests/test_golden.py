@@ -75,3 +75,20 @@ def test_golden_full_step(orc):
         np.testing.assert_allclose(o["x"][b], d["x1"][sel][a], rtol=0, atol=1e-14)
         np.testing.assert_allclose(o["vx"][b], d["vx1"][sel][a], rtol=1e-10, atol=1e-14)
         np.testing.assert_allclose(o["vy"][b], d["vy1"][sel][a], rtol=1e-10, atol=1e-14)
+
+
+def test_golden_embedded_kernels(orc):
+    """The kernels of Multigrid_embedded.cu on one seeded rectangular level (65 x 49, an
+    electrode with edges on odd and even nodes, a solid block): smooth_redblack with
+    redblack = 0 (the colour whose test evaluates as intended), residual_kernel,
+    restrict_kernel (coarse rhs and injected coarse kinds) and prolongate_add_kernel."""
+    d = load("ref_embedded.npz")
+    h2 = float(d["h2"])
+    s0 = orc.emb_half_sweep(d["phi"], d["rhs"], d["mask"], d["bc"], h2, 0)
+    assert rel_l2(s0, d["phi_sweep0"]) < 1e-14
+    res = orc.emb_residual(d["phi"], d["rhs"], d["mask"], 1.0 / h2)
+    assert rel_l2(res, d["res"]) < 1e-13
+    rc, mc = orc.emb_restrict(d["res"], d["mask"])
+    assert np.array_equal(mc, d["mask_c"])
+    assert rel_l2(rc, d["rhs_c"]) < 1e-14
+    assert np.array_equal(orc.emb_prolong(d["phi_c"], d["phi"], d["mask"]), d["phi_prol"])
