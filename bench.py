@@ -286,14 +286,8 @@ def run_ours(args):
     pst = eng.stats(reset=True)
     eng.profile(False)
     particles = 0.5 * (n0 + n1)
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = torch.tensor([particles], device=dev, dtype=torch.float64)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-        ms_max, particles_all = float(t.item()), float(tot.item())
-    else:
-        ms_max, particles_all = ms, particles
+    from pic_cuda_b200 import shard
+    ms_max, particles_all = shard.reduce_timing(ms, particles, dist, dev)
     value = particles_all * args.steps / (ms_max / 1000.0)
 
     # roofline of the fused particle pass
@@ -393,28 +387,51 @@ def run_e2e(args, cfg, n, Te, Ti, Ld, steps_job, local, rank):
 
 def run_batched_bench(args):
     """Batched mix in HBM-budgeted waves (one set of launches per step for a wave's jobs,
-    autotuned) against the same jobs one after another with the plain step."""
+    autotuned) against the same jobs one after another with the plain step.  Under torchrun
+    the jobs are split over the ranks by work (shard.shard_jobs), each rank runs its share,
+    and the line reports the whole mix: work summed, time the slowest rank's."""
     import torch
-    from pic_cuda_b200 import autotune, batch
+    from pic_cuda_b200 import autotune, batch, shard
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     n_jobs = args.jobs or 256
     scale = args.ppc_scale if args.ppc_scale is not None else 0.02
-    specs = batch.batched_specs(n_jobs, seed=4, ppc_scale=scale, steps=300)
+    all_specs = batch.batched_specs(n_jobs, seed=4, ppc_scale=scale, steps=300)
+    mine = shard.shard_jobs([sp.particle_steps for sp in all_specs], world)[rank]
+    specs = [all_specs[j] for j in mine]
     budget = int((args.budget_gb or 120.0) * 1e9)
     torch.cuda.synchronize()
     tuner = autotune.Tuner()
-    with ClockSampler(0) as clk:
-        b = batch.run_batched(specs, budget, tuner=tuner)
-        seq = batch.run_sequential(specs)
-    line = {"metric": METRIC, "value": b.rate, "unit": UNIT, "n_gpus": 1, "steps": 300, "warmup": 0,
-            "ms_per_step": 1000.0 * b.seconds / 300, "higher_is_better": True, "scaling": "weak",
+    with ClockSampler(local) as clk:
+        b = batch.run_batched(specs, budget, device=local, tuner=tuner)
+        seq = batch.run_sequential(specs, device=local)
+    dev = torch.device("cuda", local)
+    sec, work = shard.reduce_timing(b.seconds, b.particle_steps, dist, dev)
+    seq_sec, seq_work = shard.reduce_timing(seq.seconds, seq.particle_steps, dist, dev)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    rate, seq_rate = work / sec, seq_work / seq_sec
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": 300, "warmup": 0,
+            "ms_per_step": 1000.0 * sec / 300, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "mode": "batched",
             "config": {"workload": "batched", "jobs": n_jobs, "ppc_scale": scale,
                        "grids": "uniform over {65,129,257,513}^2", "ppc": "U[50,400] x ppc_scale per species",
                        "waves": b.waves, "budget_gb": budget / 1e9, "tuned": tuner.chosen,
-                       "particle_steps": b.particle_steps},
-            "sequential": {"value": seq.rate, "seconds": seq.seconds, "particle_steps": seq.particle_steps},
-            "speedup_vs_sequential": b.rate / seq.rate if seq.rate > 0 else None,
-            "seconds": b.seconds, "wall_seconds": b.wall_seconds, "clocks": clk.summary()}
+                       "particle_steps": work, "parallelism": f"jobs sharded over {world} ranks by work"
+                       if world > 1 else "single GPU"},
+            "sequential": {"value": seq_rate, "seconds": seq_sec, "particle_steps": seq_work},
+            "speedup_vs_sequential": rate / seq_rate if seq_rate > 0 else None,
+            "seconds": sec, "wall_seconds": b.wall_seconds, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -469,18 +486,18 @@ def embedded_problem(n):
 
 
 def embedded_bytes_per_cycle(n, levels):
-    """Algorithmic HBM bytes of one V-cycle: per level above the one-CTA ones, pre-smoothing
-    (phi, rhs read and phi written: 24 B/node, kinds 1 B), restriction (phi, rhs, kinds read:
-    17 B/node; coarse rhs, kinds, phi written: 17 B per coarse node) and prolongation +
-    post-smoothing (24 + 1 B/node, coarse phi 8 B per coarse node); the one-CTA levels read and
-    write their arrays once (25 B/node)."""
+    """Algorithmic HBM bytes of one V-cycle, counted once: per level above the one-CTA ones,
+    pre-smoothing with the restriction (phi, rhs, kinds read: 17 B/node; phi written: 8 B/node;
+    coarse rhs, kinds and phi written: 17 B per coarse node) and prolongation + post-smoothing
+    (phi, rhs, kinds read and phi written: 25 B/node; coarse phi read: 8 B per coarse node);
+    the one-CTA levels read and write their arrays once (25 B/node)."""
     b, a = 0, n
     for l in range(levels):
         N, Nc = a * a, ((a - 1) // 2 + 1) ** 2
         if N <= 65 * 65:
             b += 25 * N
         else:
-            b += 25 * N + 17 * N + 17 * Nc + 25 * N + 8 * Nc
+            b += 25 * N + 17 * Nc + 25 * N + 8 * Nc
         a = (a - 1) // 2 + 1
     return b
 
@@ -530,26 +547,33 @@ def run_embedded_bench(args):
     bpc = embedded_bytes_per_cycle(n, levels)
     # end to end: pinned host arrays in, a solve to 1e-8 (at most 200 V-cycles) through the C ABI,
     # phi back to the host
-    hp = {k: torch.from_numpy(a).pin_memory() for k, a in (("phi", phi), ("rhs", rhs), ("mask", mask), ("bc", bc))}
-    out = torch.empty_like(hp["phi"]).pin_memory()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    dd = {k: v.to(dev, non_blocking=True) for k, v in hp.items()}
-    cyc, rel, ok = solve_embedded_f64(dd["phi"], dd["rhs"], dd["mask"], dd["bc"], levels, h, 2, 2, opts, tol=1e-8,
-                                      max_cycles=200)
-    out.copy_(dd["phi"])
-    e2e_s = time.perf_counter() - t0
+    e2e = None
+    if not args.no_e2e:
+        hp = {k: torch.from_numpy(a).pin_memory() for k, a in (("phi", phi), ("rhs", rhs), ("mask", mask),
+                                                                ("bc", bc))}
+        out = torch.empty_like(hp["phi"]).pin_memory()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dd = {k: v.to(dev, non_blocking=True) for k, v in hp.items()}
+        cyc, rel, ok = solve_embedded_f64(dd["phi"], dd["rhs"], dd["mask"], dd["bc"], levels, h, 2, 2, opts,
+                                          tol=1e-8, max_cycles=200)
+        out.copy_(dd["phi"])
+        e2e_s = time.perf_counter() - t0
+        e2e = {"value": cyc / e2e_s, "unit": unit, "h2d_bytes_per_step": 25 * n * n / cyc,
+               "d2h_bytes_per_step": 8 * n * n / cyc, "cycles": cyc, "relres": rel, "converged": ok,
+               "seconds": e2e_s}
     # the reference's own kernels in its V-cycle sequence on the same B200 and problem
     ref = None
-    try:
-        from oracle import refh
-        if refh.available():
-            _, ref_ms = refh.emb_vcycles_timed(phi, rhs, mask, bc, h, levels, 20, warmup=3)
-            ref = {"ms_per_vcycle": ref_ms, "vcycles_per_s": 1000.0 / ref_ms, "speedup": ref_ms / ms,
-                   "path": "Multigrid::vcycle (Multigrid_embedded.cu:159-188) re-sequenced on the reference's "
-                           "kernels, 8x8 blocks, legacy stream; its colour test races (:22)"}
-    except (OSError, AssertionError) as e:
-        ref = {"unavailable": str(e)}
+    if not args.no_ref_cuda:
+        try:
+            from oracle import refh
+            if refh.available():
+                _, ref_ms = refh.emb_vcycles_timed(phi, rhs, mask, bc, h, levels, 20, warmup=3)
+                ref = {"ms_per_vcycle": ref_ms, "vcycles_per_s": 1000.0 / ref_ms, "speedup": ref_ms / ms,
+                       "path": "Multigrid::vcycle (Multigrid_embedded.cu:159-188) re-sequenced on the reference's "
+                               "kernels, 8x8 blocks, legacy stream; its colour test races (:22)"}
+        except (OSError, AssertionError) as e:
+            ref = {"unavailable": str(e)}
     line = {"metric": f"embedded-boundary multigrid {unit}", "value": 1000.0 / ms, "unit": unit, "n_gpus": 1,
             "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -560,9 +584,7 @@ def run_embedded_bench(args):
                          "frac": bpc / (ms / 1000.0) / 1e9 / peak, "traffic": None, "kernel": "whole V-cycle",
                          "bytes_per_vcycle": bpc, "peak_source": f"{peak_kind} hbm_gbs"},
             "clocks": clk.summary(),
-            "e2e": {"value": cyc / e2e_s, "unit": unit, "h2d_bytes_per_step": 25 * n * n / cyc,
-                    "d2h_bytes_per_step": 8 * n * n / cyc, "cycles": cyc, "relres": rel, "converged": ok,
-                    "seconds": e2e_s},
+            "e2e": e2e,
             "reference_cuda": ref}
     if not args.no_cpu_baseline:
         cyc_cpu = max(1, args.cpu_steps)
