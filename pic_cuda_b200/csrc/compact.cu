@@ -14,7 +14,8 @@
 
 namespace {
 
-// aux[4*s + 0] = holes found, aux[4*s + 1] = tail survivors found.
+// aux[4*s + 0] = holes found, aux[4*s + 1] = tail survivors found, aux[4*s + 2] = ionisation
+// newborns absorbed since the last compaction.
 __global__ void compact_mark(const SlotDev* __restrict__ slots, const int* __restrict__ counts,
                              const int* __restrict__ hit_counts, int* __restrict__ aux, const uint8_t* active) {
   const int s = blockIdx.y;
@@ -69,12 +70,16 @@ __global__ void compact_move(const SlotDev* __restrict__ slots, int* __restrict_
   }
 }
 
+// absorbed_out[s] = this pass's hits plus the ionisation newborns lost since the last
+// compaction (aux[4 s + 2], which the ionisation kernel accumulates).
 __global__ void compact_finish(int* __restrict__ counts, int* __restrict__ hit_counts, int nslots,
-                               const uint8_t* active, int* absorbed_out) {
+                               const uint8_t* active, int* aux, int* absorbed_out) {
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslots; s += gridDim.x * blockDim.x) {
     if (active && !active[s]) continue;
     const int k = hit_counts[s];
-    if (absorbed_out) absorbed_out[s] = k;
+    const int lost = aux[4 * s + 2];
+    aux[4 * s + 2] = 0;
+    if (absorbed_out) absorbed_out[s] = k + lost;
     if (k == 0) continue;
     counts[s] -= k;
     hit_counts[s] = 0;
@@ -89,6 +94,7 @@ int launch_compact(const EngineLaunch& L, cudaStream_t st) {
   compact_mark<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
   compact_lists<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
   compact_move<<<grid, 256, 0, st>>>(L.slots, L.counts, L.hit_counts, L.aux, L.active);
-  compact_finish<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.counts, L.hit_counts, L.nslots, L.active, L.absorbed);
+  compact_finish<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.counts, L.hit_counts, L.nslots, L.active, L.aux,
+                                                         L.absorbed);
   return 4;
 }

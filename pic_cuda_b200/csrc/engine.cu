@@ -595,13 +595,16 @@ int step_once(pic_engine* E, cudaStream_t s) {
   E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I |
                                      PIC_PHASE_DEPOSIT_I | PIC_PHASE_GATED_I, 0, s);
   L.ev_mover_begin = L.ev_mover_end = nullptr;
-  phase_mark(E, 2, true, s);
-  E->launches += launch_compact(L, s);
+  // the pairs of this step's ionisations (appended after the live particles, drifted and
+  // deposited) before the field solve, which needs their charge
   E->launches += launch_ionize(L, true, s);
-  phase_mark(E, 2, false, s);
-  // the sort due before the next step, on the side stream while the field is solved
+  // removal of the absorbed particles, then the sort due before the next step, on the side
+  // stream while the field is solved (they touch only particle arrays, the solve only grids)
   CK(cudaEventRecord(E->ev_fork, s));
   CK(cudaStreamWaitEvent(E->side_stream, E->ev_fork, 0));
+  phase_mark(E, 2, true, E->side_stream);
+  E->launches += launch_compact(L, E->side_stream);
+  phase_mark(E, 2, false, E->side_stream);
   bool side = false;
   rc = sort_jobs(E, L, sort_after, E->side_stream, &side);
   if (rc) return rc;
@@ -638,10 +641,13 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
   n += launch_zero_rho_all(L, max_nodes, s);
   n += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_DRIFT_I | PIC_PHASE_WALLS_I | PIC_PHASE_DEPOSIT_I |
                            PIC_PHASE_GATED_I, 0, s);
-  n += launch_compact(L, s);
   n += launch_ionize(L, true, s);
+  // removal of the absorbed particles and the sort due before the next step, on a parallel
+  // branch of the graph beside the solve
+  if (err == cudaSuccess) err = cudaEventRecord(E->ev_fork, s);
+  if (err == cudaSuccess) err = cudaStreamWaitEvent(E->side_stream, E->ev_fork, 0);
+  n += launch_compact(L, E->side_stream);
   if (with_sort) {
-    // the sort due before the next step, on a parallel branch of the graph beside the solve
     int max_cells = 0;
     int64_t max_p = 0;
     for (int j = 0; j < E->njobs_hw; ++j) {
@@ -650,12 +656,10 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
       for (int k = 0; k < J.cfg.n_species; ++k) max_p = std::max<int64_t>(max_p, J.cfg.species[k].capacity);
       max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
     }
-    if (err == cudaSuccess) err = cudaEventRecord(E->ev_fork, s);
-    if (err == cudaSuccess) err = cudaStreamWaitEvent(E->side_stream, E->ev_fork, 0);
     n += launch_sort_mask(L, E->d_mask, 1, E->side_stream);
     n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), E->side_stream);
-    if (err == cudaSuccess) err = cudaEventRecord(E->ev_join, E->side_stream);
   }
+  if (err == cudaSuccess) err = cudaEventRecord(E->ev_join, E->side_stream);
   n += launch_mg_init(L, E->mg_all.L, s);
   cudaMemsetAsync(E->d_loop, 0, sizeof(int), s);
   // conditional WHILE node for the V-cycles
@@ -689,7 +693,7 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
     }
   }
   if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
-  if (err == cudaSuccess && with_sort) err = cudaStreamWaitEvent(s, E->ev_join, 0);
+  if (err == cudaSuccess) err = cudaStreamWaitEvent(s, E->ev_join, 0);
   if (err == cudaSuccess) n += launch_step_end(E->d_st, E->njobs_hw, nullptr, 1, 1, s);
   cudaGraph_t done = nullptr;
   const cudaError_t e2 = cudaStreamEndCapture(s, &done);
@@ -1056,6 +1060,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   CK(cudaMemset(E->d_st + id, 0, sizeof(JobState)));
   CK(cudaMemset(E->d_counts + id * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob));
   CK(cudaMemset(E->d_hits + id * kSlotsPerJob, 0, sizeof(int) * kSlotsPerJob));
+  CK(cudaMemset(E->d_aux + 4 * id * kSlotsPerJob, 0, sizeof(int) * 4 * kSlotsPerJob));
   for (int s = 0; s < kSlotsPerJob; ++s) E->h_active[id * kSlotsPerJob + s] = s < c.n_species ? 1 : 0;
   E->njobs_hw = std::max(E->njobs_hw, id + 1);
   rc = upload_active(E);

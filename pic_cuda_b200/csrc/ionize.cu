@@ -51,7 +51,7 @@ __device__ int block_scan01(int v, int* total) {
 
 __global__ void __launch_bounds__(256)
 ionize_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const SlotDev* __restrict__ slots,
-              int* __restrict__ counts, int* __restrict__ absorbed, int drift_dep) {
+              int* __restrict__ counts, int* __restrict__ aux, int drift_dep) {
   const int job = blockIdx.x;
   const JobDev& J = jobs[job];
   JobState& T = st[job];
@@ -131,7 +131,9 @@ ionize_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const 
   if (threadIdx.x == 0) {
     counts[se] = min(ce, (int)SE.capacity);
     counts[si] = min(ci, (int)SI.capacity);
-    if (absorbed) { absorbed[se] += lost_e; absorbed[si] += lost_i; }
+    // newborns absorbed in their first drift: added to the slots' absorbed counts by the
+    // next compaction (aux[4 s + 2])
+    if (aux) { aux[4 * se + 2] += lost_e; aux[4 * si + 2] += lost_i; }
     T.next_pid = pid0 + 2u * (uint32_t)ne;
     T.ionizations = ne;
     T.event_count = 0;
@@ -142,7 +144,6 @@ ionize_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const 
 
 int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s) {
   if (L.njobs == 0) return 0;
-  ionize_kernel<<<L.njobs, 256, 0, s>>>(L.jobs, L.st, L.slots, L.counts, L.absorbed,
-                                         drift_and_deposit ? 1 : 0);
+  ionize_kernel<<<L.njobs, 256, 0, s>>>(L.jobs, L.st, L.slots, L.counts, L.aux, drift_and_deposit ? 1 : 0);
   return 1;
 }

@@ -20,14 +20,16 @@
 // the reference's zeroed coarse phi_bc arrays give).
 //
 // Kernels of one V-cycle:
-//   emb_smooth_kernel<NU, PRO>  a 32 x 32 output tile with a halo of 2 NU nodes: phi, the
-//       node kinds and the right-hand side (DIRICHLET nodes: phi_bc in the same slot) are
-//       staged in shared memory once, the NU sweeps run there (after k half-sweeps every node
-//       at least k nodes inside the tile edge is exact), and with PRO the coarse correction
-//       is prolongated while staging.  Tiles read halos that neighbouring CTAs own, so the
-//       result goes to the level's other phi buffer.
-//   emb_restrict_kernel  one thread per coarse node: the nine fine residuals on the fly,
-//       full weighting, the coarse node kind, and the coarse phi zeroed (no residual array).
+//   emb_down_kernel<NU>  pre-smoothing fused with the restriction: a 32 x 32 output tile with
+//       a halo of 2 NU + 2 nodes (phi, node kinds and the right-hand side, DIRICHLET nodes'
+//       phi_bc in the same slot, staged in shared memory with every load of a thread issued
+//       at once); the NU sweeps run there (after k half-sweeps every node at least k nodes
+//       inside the tile edge is exact); the smoothed output region is written back, and the
+//       16 x 16 coarse nodes of the tile get the full-weighted residual of their nine fine
+//       nodes (from shared memory), their kind, and phi = 0.  No residual array.
+//   emb_smooth_kernel<NU, PRO>  the same tile scheme with a halo of 2 NU for the
+//       post-smoothing: the coarse correction is prolongated while staging (PRO).  Tiles read
+//       halos that neighbouring CTAs own, so results go to the level's other phi buffer.
 //   emb_coarse_kernel  every level from the first one with at most 65 x 65 nodes down, in one
 //       CTA's shared memory (one launch for the whole lower V-cycle).
 //   emb_norm_kernel / emb_norm_final_kernel  ||r||^2 and ||rhs||^2 over the FLUID nodes in a
@@ -72,111 +74,186 @@ __device__ __forceinline__ uint8_t smoother_kind(uint8_t m, bool has_bc) {
   return kSolid;
 }
 
-// One colour of smooth_redblack on interior tile nodes (tile row pitch W, W even): thread k
-// takes row 1 + k / ((W-2)/2) and the k-th interior column of the wanted parity, so no thread
-// skips nodes of the other colour.  (x0, y0) = grid coordinates of tile node (0, 0).
+// Shared-memory tile of W x W nodes (W even) whose node (0, 0) is grid node (x0, y0), with
+// x0 + y0 even, so a node's colour is (tx + ty) & 1.  Each colour is stored on its own: node
+// (tx, ty) sits at [colour][ty * W/2 + tx/2].  A red-black half-sweep then reads the other
+// colour's neighbours at consecutive FP64 words across a warp (the interleaved layout reads
+// them at a stride of two words, two-way bank conflicts), and the rows of one colour share
+// the parity of tx, so W/E neighbours are at q - 1 + (tx & 1) and q + (tx & 1).
 template <int W>
-__device__ __forceinline__ void tile_half_sweep(double* s_phi, const double* s_rb, const uint8_t* s_m, int x0, int y0,
-                                                int colour, double h2) {
-  constexpr int HALF = (W - 2) / 2;
-  constexpr int CNT = (W - 2) * HALF;
+struct Tile {
+  static constexpr int HW = W / 2;
+  double p[2][HW * W];    // phi
+  double rb[2][HW * W];   // rhs (FLUID), phi_bc (DIRICHLET with phi_bc), 0 otherwise
+  uint8_t m[2][HW * W];   // the caller's node kinds; kFixed on the grid boundary and outside
+  __device__ __forceinline__ static int at(int tx, int ty) { return ty * HW + (tx >> 1); }
+  __device__ __forceinline__ static int colour(int tx, int ty) { return (tx + ty) & 1; }
+  __device__ __forceinline__ double phi(int tx, int ty) const { return p[colour(tx, ty)][at(tx, ty)]; }
+  __device__ __forceinline__ uint8_t kind(int tx, int ty) const { return m[colour(tx, ty)][at(tx, ty)]; }
+  // residual_kernel's expression at an interior tile node: rhs - (S + N + W + E - 4 phi) / h^2
+  __device__ __forceinline__ double residual(int tx, int ty, double h2i) const {
+    const int c = colour(tx, ty), o = c ^ 1, i = at(tx, ty);
+    if (m[c][i] != kFluid) return 0.0;
+    const int w = i - 1 + (tx & 1);
+    const double lap = p[o][i - HW] + p[o][i + HW] + p[o][w] + p[o][w + 1] - 4.0 * p[c][i];
+    return rb[c][i] - h2i * lap;
+  }
+};
+
+// One colour of smooth_redblack on the interior tile nodes: thread k takes row 1 + k / H and
+// the k-th node of that colour in it (H = (W-2)/2 per row), so no thread skips nodes.  FLUID
+// nodes relax, DIRICHLET nodes take their phi_bc when the caller gave one, others stay.
+template <int W>
+__device__ __forceinline__ void tile_half_sweep(Tile<W>& T, int colour, double h2, bool has_bc) {
+  constexpr int HW = W / 2, HALF = (W - 2) / 2, CNT = (W - 2) * HALF;
+  double* __restrict__ own = T.p[colour];
+  const double* __restrict__ oth = T.p[colour ^ 1];
+  const double* __restrict__ rb = T.rb[colour];
+  const uint8_t* __restrict__ mk = T.m[colour];
   for (int k = threadIdx.x; k < CNT; k += kSmoothThreads) {
     const int r = k / HALF;
     const int ty = 1 + r;
-    const int par = (colour - x0 - y0 - ty) & 1;     // tile column parity of this colour
-    const int tx = (par ? 1 : 2) + 2 * (k - r * HALF);
-    const int t = ty * W + tx;
-    const uint8_t m = s_m[t];
+    const int odd = (colour - ty) & 1;              // tx parity of this colour in row ty
+    const int i = ty * HW + (k - r * HALF) + (odd ? 0 : 1);
+    const uint8_t m = mk[i];
     if (m == kFluid) {
-      const double sum = s_phi[t - W] + s_phi[t + W] + s_phi[t - 1] + s_phi[t + 1];
-      s_phi[t] = 0.25 * (sum - h2 * s_rb[t]);
-    } else if (m == kDir) {
-      s_phi[t] = s_rb[t];
+      const int w = i - 1 + odd;
+      const double sum = oth[i - HW] + oth[i + HW] + oth[w] + oth[w + 1];
+      own[i] = 0.25 * (sum - h2 * rb[i]);
+    } else if (m == kDir && has_bc) {
+      own[i] = rb[i];
     }
   }
 }
 
+// Stages the tile: phi, the node kind and the rhs slot of every node.  Every load of a thread
+// is issued before any is used, so a tile waits for one memory latency; the DIRICHLET values
+// (rare) and, with PRO, the coarse correction of the FLUID nodes follow in a second round.
+template <int W, bool PRO>
+__device__ __forceinline__ void stage_tile(Tile<W>& T, const double* __restrict__ phi, const double* __restrict__ rhs,
+                                           const uint8_t* __restrict__ mask, const double* __restrict__ bc,
+                                           const double* __restrict__ coarse, int nx, int ny, int nxc, int x0, int y0,
+                                           bool bilinear) {
+  constexpr int IT = (W * W + kSmoothThreads - 1) / kSmoothThreads;
+  double p[IT], r[IT];
+  uint8_t m[IT];
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int k = threadIdx.x + it * kSmoothThreads;
+    p[it] = 0.0; r[it] = 0.0; m[it] = kFixed;
+    if (k < W * W) {
+      const int ty = k / W, tx = k - ty * W;
+      const int gx = x0 + tx, gy = y0 + ty;
+      if (gx >= 0 && gy >= 0 && gx < nx && gy < ny) {
+        const size_t id = (size_t)gy * nx + gx;
+        p[it] = phi[id];
+        if (gx > 0 && gy > 0 && gx < nx - 1 && gy < ny - 1) {
+          m[it] = mask[id];
+          r[it] = rhs[id];
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int it = 0; it < IT; ++it) {
+    const int k = threadIdx.x + it * kSmoothThreads;
+    if (k < W * W) {
+      const int ty = k / W, tx = k - ty * W;
+      const int gx = x0 + tx, gy = y0 + ty;
+      double pv = p[it], rv = r[it];
+      if (m[it] == kFluid) {
+        if (PRO) pv += prolong_at(coarse, nxc, gx, gy, bilinear);
+      } else {
+        rv = (m[it] == kDir && bc) ? bc[(size_t)gy * nx + gx] : 0.0;
+      }
+      const int c = Tile<W>::colour(tx, ty), i = Tile<W>::at(tx, ty);
+      T.p[c][i] = pv; T.rb[c][i] = rv; T.m[c][i] = m[it];
+    }
+  }
+}
+
+// The 32 x 32 output region of a staged tile (halo H) back to global memory.
+template <int W, int H>
+__device__ __forceinline__ void store_tile(const Tile<W>& T, double* __restrict__ out, int nx, int ny, int x0,
+                                           int y0) {
+  for (int k = threadIdx.x; k < kTile * kTile; k += kSmoothThreads) {
+    const int ty = k / kTile, tx = k - ty * kTile;
+    const int gx = x0 + H + tx, gy = y0 + H + ty;
+    if (gx < nx && gy < ny) out[(size_t)gy * nx + gx] = T.phi(tx + H, ty + H);
+  }
+}
+
+// NU sweeps (post-smoothing with PRO: after adding the coarse correction) of one tile.
 template <int NU, bool PRO>
 __global__ void __launch_bounds__(kSmoothThreads) emb_smooth_kernel(
     const double* __restrict__ phi_in, double* __restrict__ phi_out, const double* __restrict__ rhs,
     const uint8_t* __restrict__ mask, const double* __restrict__ bc, const double* __restrict__ coarse, int nx, int ny,
     int nxc, double h2, int bilinear) {
   constexpr int H = 2 * NU, W = kTile + 2 * H;
-  __shared__ double s_phi[W * W];
-  __shared__ double s_rb[W * W];
-  __shared__ uint8_t s_m[W * W];
+  __shared__ Tile<W> T;
   const int x0 = blockIdx.x * kTile - H, y0 = blockIdx.y * kTile - H;
-  for (int k = threadIdx.x; k < W * W; k += kSmoothThreads) {
-    const int ty = k / W, tx = k - ty * W;
-    const int gx = x0 + tx, gy = y0 + ty;
-    double p = 0.0, rb = 0.0;
-    uint8_t m = kFixed;
-    if (gx >= 0 && gy >= 0 && gx < nx && gy < ny) {
-      const size_t id = (size_t)gy * nx + gx;
-      p = phi_in[id];
-      if (gx > 0 && gy > 0 && gx < nx - 1 && gy < ny - 1) {
-        m = smoother_kind(mask[id], bc != nullptr);
-        if (m == kFluid) {
-          rb = rhs[id];
-          if (PRO) p += prolong_at(coarse, nxc, gx, gy, bilinear != 0);
-        } else if (m == kDir) {
-          rb = bc[id];
-        }
-      }
-    }
-    s_phi[k] = p; s_rb[k] = rb; s_m[k] = m;
-  }
+  stage_tile<W, PRO>(T, phi_in, rhs, mask, bc, coarse, nx, ny, nxc, x0, y0, bilinear != 0);
   __syncthreads();
 #pragma unroll 1
   for (int s = 0; s < 2 * NU; ++s) {
-    tile_half_sweep<W>(s_phi, s_rb, s_m, x0, y0, s & 1, h2);
+    tile_half_sweep<W>(T, s & 1, h2, bc != nullptr);
     __syncthreads();
   }
-  for (int k = threadIdx.x; k < kTile * kTile; k += kSmoothThreads) {
-    const int ty = k / kTile, tx = k - ty * kTile;
-    const int gx = x0 + H + tx, gy = y0 + H + ty;
-    if (gx < nx && gy < ny) phi_out[(size_t)gy * nx + gx] = s_phi[(ty + H) * W + tx + H];
-  }
+  store_tile<W, H>(T, phi_out, nx, ny, x0, y0);
 }
 
-// Residual of fine node id (interior): restatement of residual_kernel's expression.
-__device__ __forceinline__ double fine_residual(const double* phi, const double* rhs, const uint8_t* mask, size_t id,
-                                                int nx, double h2i) {
-  if (mask[id] != kFluid) return 0.0;
-  const double lap = phi[id - nx] + phi[id + nx] + phi[id - 1] + phi[id + 1] - 4.0 * phi[id];
-  return rhs[id] - h2i * lap;
-}
-
-// Coarse node kind from the fine mask around fine node id = (2ic, 2jc).
-__device__ __forceinline__ uint8_t coarse_kind(const uint8_t* mask, size_t id, int nx, bool any) {
-  if (!any) return mask[id];
+// Coarse node kind from the fine kinds around fine node (tx, ty): the kind of that node, or
+// (any) DIRICHLET if any of the 3x3 is, else SOLID if any is not FLUID, else FLUID.
+template <class M>
+__device__ __forceinline__ uint8_t coarse_kind_of(M kind, bool any) {
+  if (!any) return kind(0, 0);
   bool dir = false, other = false;
 #pragma unroll
   for (int dj = -1; dj <= 1; ++dj)
 #pragma unroll
     for (int di = -1; di <= 1; ++di) {
-      const uint8_t m = mask[id + (ptrdiff_t)dj * nx + di];
+      const uint8_t m = kind(di, dj);
       dir |= m == kDir;
       other |= m != kFluid && m != kDir;
     }
   return dir ? kDir : other ? kSolid : kFluid;
 }
 
-// Full weighting of the fine residual (restrict_kernel's sum order) at fine node id.
+// Full weighting of the fine residual (restrict_kernel's sum order) around a fine node;
+// res(di, dj) is the residual at offset (di, dj).
 template <class R>
-__device__ __forceinline__ double full_weight(R res, size_t id, int nx) {
+__device__ __forceinline__ double full_weight(R res) {
   double sum = 0.0;
-  sum += res(id);
-  sum += 0.5 * (res(id - 1) + res(id + 1) + res(id - nx) + res(id + nx));
-  sum += 0.25 * (res(id - nx - 1) + res(id - nx + 1) + res(id + nx - 1) + res(id + nx + 1));
+  sum += res(0, 0);
+  sum += 0.5 * (res(-1, 0) + res(1, 0) + res(0, -1) + res(0, 1));
+  sum += 0.25 * (res(-1, -1) + res(1, -1) + res(-1, 1) + res(1, 1));
   return sum / 4.0;
 }
 
-__global__ void emb_restrict_kernel(const double* __restrict__ phi, const double* __restrict__ rhs,
-                                    const uint8_t* __restrict__ mask, int nx, double h2i, double* __restrict__ rhs_c,
-                                    uint8_t* __restrict__ mask_c, double* __restrict__ phi_c, int nxc, int nyc,
-                                    int coarsen_any) {
-  const int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y * blockDim.y + threadIdx.y;
+// Pre-smoothing of one tile fused with the restriction: NU sweeps on a tile with a halo of
+// 2 NU + 2 (so the smoothed phi is exact two nodes beyond the output region), the 32 x 32
+// output region written back, then for the 16 x 16 coarse nodes whose fine node (2i, 2j)
+// lies in the output region: the residual of the nine fine nodes from shared memory
+// (residual_kernel's expression), full weighting, the coarse kind, and coarse phi = 0.
+template <int NU>
+__global__ void __launch_bounds__(kSmoothThreads) emb_down_kernel(
+    const double* __restrict__ phi_in, double* __restrict__ phi_out, const double* __restrict__ rhs,
+    const uint8_t* __restrict__ mask, const double* __restrict__ bc, int nx, int ny, double h2,
+    double* __restrict__ rhs_c, uint8_t* __restrict__ mask_c, double* __restrict__ phi_c, int nxc, int nyc, int any) {
+  constexpr int H = 2 * NU + 2, W = kTile + 2 * H;
+  __shared__ Tile<W> T;
+  const int x0 = blockIdx.x * kTile - H, y0 = blockIdx.y * kTile - H;
+  stage_tile<W, false>(T, phi_in, rhs, mask, bc, nullptr, nx, ny, 0, x0, y0, false);
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 0; s < 2 * NU; ++s) {
+    tile_half_sweep<W>(T, s & 1, h2, bc != nullptr);
+    __syncthreads();
+  }
+  store_tile<W, H>(T, phi_out, nx, ny, x0, y0);
+  const double h2i = 1.0 / h2;
+  const int k = threadIdx.x;            // 256 threads, one coarse node each
+  const int ic = blockIdx.x * (kTile / 2) + (k & 15), jc = blockIdx.y * (kTile / 2) + (k >> 4);
   if (ic >= nxc || jc >= nyc) return;
   const size_t idc = (size_t)jc * nxc + ic;
   phi_c[idc] = 0.0;
@@ -185,11 +262,18 @@ __global__ void emb_restrict_kernel(const double* __restrict__ phi, const double
     mask_c[idc] = kFluid;
     return;
   }
-  const size_t idf = (size_t)(2 * jc) * nx + 2 * ic;
-  const uint8_t m = coarse_kind(mask, idf, nx, coarsen_any != 0);
-  mask_c[idc] = m;
-  rhs_c[idc] = m == kFluid ? full_weight([&](size_t id) { return fine_residual(phi, rhs, mask, id, nx, h2i); }, idf, nx)
-                           : 0.0;
+  const int tx = 2 * ic - x0, ty = 2 * jc - y0;
+  const uint8_t kc = coarse_kind_of([&](int di, int dj) { return T.kind(tx + di, ty + dj); }, any != 0);
+  mask_c[idc] = kc;
+  rhs_c[idc] = kc == kFluid ? full_weight([&](int di, int dj) { return T.residual(tx + di, ty + dj, h2i); }) : 0.0;
+}
+
+// Residual of fine node id (interior): restatement of residual_kernel's expression.
+__device__ __forceinline__ double fine_residual(const double* phi, const double* rhs, const uint8_t* mask, size_t id,
+                                                int nx, double h2i) {
+  if (mask[id] != kFluid) return 0.0;
+  const double lap = phi[id - nx] + phi[id + nx] + phi[id - 1] + phi[id + 1] - 4.0 * phi[id];
+  return rhs[id] - h2i * lap;
 }
 
 // ---------------------------------------------------------------- one-CTA lower V-cycle
@@ -271,14 +355,15 @@ __global__ void __launch_bounds__(kCoarseThreads) emb_coarse_kernel(CoarseLevelA
       uint8_t kc = kFluid;
       double fc = 0.0;
       if (ic > 0 && jc > 0 && ic < nxc - 1 && jc < nyc - 1) {
-        const size_t idf = (size_t)(2 * jc) * nx + 2 * ic;
-        kc = coarse_kind(mk, idf, nx, A.coarsen_any != 0);
+        const ptrdiff_t idf = (ptrdiff_t)(2 * jc) * nx + 2 * ic;
+        kc = coarse_kind_of([&](int di, int dj) { return mk[idf + (ptrdiff_t)dj * nx + di]; }, A.coarsen_any != 0);
         if (kc == kFluid)
-          fc = full_weight([&](size_t id) {
+          fc = full_weight([&](int di, int dj) {
+                 const ptrdiff_t id = idf + (ptrdiff_t)dj * nx + di;
                  if (mk[id] != kFluid) return 0.0;
                  const double lap = pf[id - nx] + pf[id + nx] + pf[id - 1] + pf[id + 1] - 4.0 * pf[id];
                  return rbf[id] - h2i * lap;
-               }, idf, nx);
+               });
       }
       A.mask[l + 1][k] = kc;       // the reference writes the coarse kinds and rhs of every level
       A.rhs[l + 1][k] = fc;
@@ -327,18 +412,22 @@ __device__ double cta_sum(double v, double* red) {
   return s;
 }
 
+// CTA b sums the interior rows 1 + b, 1 + b + gridDim.x, ... (threads along the row), so every
+// partial is formed in a fixed order.
 __global__ void __launch_bounds__(256) emb_norm_kernel(const double* __restrict__ phi, const double* __restrict__ rhs,
                                                        const uint8_t* __restrict__ mask, int nx, int ny, double h2i,
                                                        double* __restrict__ partials) {
   __shared__ double red[8];
   double r2 = 0.0, f2 = 0.0;
-  const int64_t N = (int64_t)nx * ny;
-  for (int64_t k = blockIdx.x * 256 + threadIdx.x; k < N; k += (int64_t)gridDim.x * 256) {
-    const int j = (int)(k / nx), i = (int)(k - (int64_t)j * nx);
-    if (i == 0 || j == 0 || i == nx - 1 || j == ny - 1 || mask[k] != kFluid) continue;
-    const double r = fine_residual(phi, rhs, mask, (size_t)k, nx, h2i);
-    r2 += r * r;
-    f2 += rhs[k] * rhs[k];
+  for (int j = 1 + blockIdx.x; j < ny - 1; j += gridDim.x) {
+    const size_t row = (size_t)j * nx;
+    for (int i = 1 + threadIdx.x; i < nx - 1; i += 256) {
+      const size_t k = row + i;
+      if (mask[k] != kFluid) continue;
+      const double r = fine_residual(phi, rhs, mask, k, nx, h2i);
+      r2 += r * r;
+      f2 += rhs[k] * rhs[k];
+    }
   }
   const double a = cta_sum(r2, red);
   const double b = cta_sum(f2, red);
@@ -410,6 +499,15 @@ void smooth_chunk(const EmbLevels& P, int l, int nu, bool pro, const double* in,
   }
 }
 
+template <int NU>
+void launch_down(const EmbLevels& P, int l, const double* in, double* out, int any, cudaStream_t s) {
+  const dim3 grid((P.nx[l] + kTile - 1) / kTile, (P.ny[l] + kTile - 1) / kTile);
+  const double h2 = P.h * P.h * std::ldexp(1.0, 2 * l);
+  emb_down_kernel<NU><<<grid, kSmoothThreads, 0, s>>>(in, out, P.rhs[l], P.mask[l], P.bc[l], P.nx[l], P.ny[l], h2,
+                                                     P.rhs[l + 1], P.mask[l + 1], P.phi[l + 1], P.nx[l + 1],
+                                                     P.ny[l + 1], any);
+}
+
 // nu sweeps of level l (chunks of at most 4 per launch; the first applies the prolongation
 // when pro is set); `cur` tracks which of phi[l] / alt[l] holds the level's current values.
 void smooth_level(const EmbLevels& P, int l, int nu, bool pro, double*& cur, bool bilinear, cudaStream_t s) {
@@ -440,19 +538,29 @@ int emb_vcycle(const EmbLevels& P, int l0, int nu1, int nu2, int options, cudaSt
   double* cur[PIC_MAX_LEVELS];
   for (int l = l0; l < lc; ++l) {
     cur[l] = P.phi[l];
+    if (l < P.L - 1) {
+      // all but the last (up to 4) pre-sweeps, then those fused with the restriction
+      const int last = nu1 == 0 ? 0 : (nu1 - 1) % 4 + 1;
+      smooth_level(P, l, nu1 - last, false, cur[l], bilinear, s);
+      double* out = cur[l] == P.phi[l] ? P.alt[l] : P.phi[l];
+      switch (last) {
+        case 0: launch_down<0>(P, l, cur[l], out, any, s); break;
+        case 1: launch_down<1>(P, l, cur[l], out, any, s); break;
+        case 2: launch_down<2>(P, l, cur[l], out, any, s); break;
+        case 3: launch_down<3>(P, l, cur[l], out, any, s); break;
+        default: launch_down<4>(P, l, cur[l], out, any, s); break;
+      }
+      cur[l] = out;
+      continue;
+    }
     smooth_level(P, l, nu1, false, cur[l], bilinear, s);
-    if (l == P.L - 1) {   // coarsest level on the tile path: pre-sweeps only
+    {   // coarsest level on the tile path: pre-sweeps only
       if (cur[l] != P.phi[l]) {
         const cudaError_t e = cudaMemcpyAsync(P.phi[l], cur[l], sizeof(double) * P.nx[l] * P.ny[l],
                                               cudaMemcpyDeviceToDevice, s);
         if (e != cudaSuccess) return pic_fail(PIC_ERR_CUDA, cudaGetErrorString(e));
       }
-      break;
     }
-    const dim3 blk(32, 8), grd((P.nx[l + 1] + 31) / 32, (P.ny[l + 1] + 7) / 8);
-    const double h2i = 1.0 / (P.h * P.h * std::ldexp(1.0, 2 * l));
-    emb_restrict_kernel<<<grd, blk, 0, s>>>(cur[l], P.rhs[l], P.mask[l], P.nx[l], h2i, P.rhs[l + 1], P.mask[l + 1],
-                                            P.phi[l + 1], P.nx[l + 1], P.ny[l + 1], any);
   }
   if (lc < P.L) {
     CoarseLevelArgs A{};
@@ -482,8 +590,7 @@ int emb_vcycle(const EmbLevels& P, int l0, int nu1, int nu2, int options, cudaSt
 // ||r||^2 and ||rhs||^2 over level 0's FLUID nodes into out (device, 2 doubles).
 int emb_norms(const EmbLevels& P, double* partials, double* out, cudaStream_t s) {
   const double h2i = 1.0 / (P.h * P.h);
-  const int64_t N = (int64_t)P.nx[0] * P.ny[0];
-  const int nb = (int)std::min<int64_t>(kNormBlocks, (N + 255) / 256);
+  const int nb = std::max(1, std::min(kNormBlocks, P.ny[0] - 2));
   emb_norm_kernel<<<nb, 256, 0, s>>>(P.phi[0], P.rhs[0], P.mask[0], P.nx[0], P.ny[0], h2i, partials);
   emb_norm_final_kernel<<<1, 256, 0, s>>>(partials, nb, out);
   const cudaError_t e = cudaGetLastError();

@@ -206,7 +206,7 @@ class Engine:
         st = L.EngineStats()
         L.check(L.lib().pic_engine_get_stats(self.h, C.byref(st), 1 if reset else 0), "pic_engine_get_stats")
         d = {k: getattr(st, k) for k, _ in st._fields_ if k != "phase_ms"}
-        d["phase_ms"] = dict(zip(("sort", "particles", "compact_ionize", "field"), list(st.phase_ms)))
+        d["phase_ms"] = dict(zip(("sort", "particles", "compact", "field"), list(st.phase_ms)))
         return d
 
     def close(self) -> None:
