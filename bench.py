@@ -307,6 +307,18 @@ def run_ours(args):
                 "mover_share_of_step": mover_ms / (ms / args.steps) if ms > 0 else None,
                 "timing": f"CUDA events around each mover launch over {prof_steps} stream-ordered steps"}
 
+    # the whole step against HBM (per GPU): B = Np Bp + Nnodes (16 + k_vc Bvc) + k_dc Nnodes 40,
+    # Bvc = (4/3)(12 (nu_pre + nu_post) + 16) + 8 bytes per node and V-cycle, one FP64 defect
+    # correction update per V-cycle (k_dc = k_vc), k_vc measured over the timed steps
+    nodes = cfg.nx * cfg.ny
+    kvc = st["vcycles"] / max(st["steps"], 1)
+    bvc = (4.0 / 3.0) * (12 * (cfg.nu_pre + cfg.nu_post) + 16) + 8
+    step_bytes = particles * bpp + nodes * (16 + kvc * bvc) + kvc * nodes * 40
+    step_ach = step_bytes / (ms / args.steps / 1000.0) / 1e9
+    step_roofline = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
+                     "bytes_per_step": step_bytes, "vcycles_per_step": kvc,
+                     "formula": "Np*Bp + Nnodes*(16 + k_vc*Bvc) + k_vc*Nnodes*40"}
+
     # end to end through the public API with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -325,6 +337,7 @@ def run_ours(args):
                    "step_path": ("pic_step_graph (CUDA graph per step, V-cycle loop as a conditional WHILE node)"
                                  if args.step_path == "graph" else "pic_step (stream-ordered launches)")},
         "roofline": roofline,
+        "step_roofline": step_roofline,
         "gpu_launches": st["kernel_launches"],
         "clocks": clk.summary(),
         "e2e": e2e,
