@@ -161,7 +161,11 @@ typedef struct pic_diagnostics {
   int32_t converged;                     /* last solve reached tol                      */
   double relres;                         /* last solve's FP64 relative residual         */
   double total_charge;                   /* sum of rho over nodes (FP64)                */
-  double kinetic_energy[PIC_MAX_SPECIES];/* sum 1/2 m W v^2 (FP64; J in SI units)        */
+  /* sum 1/2 m W v^2 (FP64 sum; J in SI units) over the velocities the last particle pass
+   * produced: after a step, those that drifted in it; after a read-back (which first applies
+   * the pending kick and collisions), those it returned (pairs created by that read-back's
+   * ionisations excepted).  Without MCC vz never changes and only vx, vy are counted. */
+  double kinetic_energy[PIC_MAX_SPECIES];
   uint32_t status;                       /* sticky device status bits (PIC_ERR_* << k)  */
 } pic_diagnostics;
 

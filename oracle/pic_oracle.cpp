@@ -10,11 +10,14 @@
 //   wall segment test     collisions.cu:7-54  (ref-faithful, absolute EPSILON 1e-10)
 //   box absorption        the region updateDensity deposits from (kernels.cu:53)
 //   particle removal      particles.cu:217-262, intended semantics (remove exactly the hit
-//                         set; the reference's copy loses survivors)
+//                         set; the reference's copy can move hit tail particles into holes
+//                         and fills at most 256 holes per step, particles.cu:63-66, 255)
 //   CIC deposit           kernels.cu:26-69 (charge per node, skip rule)
 //   multigrid solve       Multigrid.cu:192-642 (red-black SOR, red = (i+j) odd first,
 //                         residual, full weighting, bilinear prolongation, warm start,
 //                         coarse zeroing, ||r||/||rho|| convergence)
+//   embedded-boundary MG  Multigrid_embedded.cu:15-188 (masked red-black Gauss-Seidel,
+//                         residual, restriction with coarse node kinds, prolongation)
 //   E field               kernels.cu:134-191
 //   gather + kick         kernels.cu:71-131
 //   reference MCC form    kernels.cu:196-263 + mcc.cu:56-85 (with Philox instead of cuRAND)

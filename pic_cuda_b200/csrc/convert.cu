@@ -158,6 +158,14 @@ __global__ void step_begin_kernel(JobState* st, const JobDev* jobs, int njobs, c
   }
 }
 
+// Before a flush pass (the pending kick and collisions of the last step, applied ahead of a
+// read-back): the kinetic energy of the jobs it applies to restarts, so that afterwards it is
+// the energy of the velocities the read-back returns.
+__global__ void ke_reset_pending_kernel(JobState* st, int njobs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs || !st[j].kick_pending) return;
+  for (int s = 0; s < PIC_MAX_SPECIES; ++s) st[j].ke[s] = 0.0;
+}
 __global__ void step_end_kernel(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= njobs || (job_mask && !job_mask[j])) return;
@@ -248,6 +256,11 @@ void launch_zero_rho(const JobDev*, int64_t nodes, int deposit_mode, void* rho, 
 }
 void launch_efield_f64(const double* phi, double* exy, int nx, int ny, double dx, double dy, cudaStream_t s) {
   efield_f64_kernel<<<grid_for((int64_t)nx * ny), 256, 0, s>>>(phi, exy, nx, ny, dx, dy);
+}
+int launch_ke_reset_pending(JobState* st, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return 0;
+  ke_reset_pending_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(st, njobs);
+  return 1;
 }
 int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s) {
   if (!njobs) return 0;

@@ -515,6 +515,7 @@ int flush(pic_engine* E, cudaStream_t s) {
   for (int j = 0; j < E->njobs_hw; ++j) any |= E->jobs[j].alive && E->jobs[j].pending;
   if (!any) return PIC_OK;
   EngineLaunch L = make_launch(E, nullptr);
+  E->launches += launch_ke_reset_pending(E->d_st, E->njobs_hw, s);
   E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_GATED_I, 0, s);
   E->launches += launch_ionize(L, false, s);
   E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 0, 0, s);

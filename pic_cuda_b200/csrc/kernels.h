@@ -47,6 +47,7 @@ int launch_compact(const EngineLaunch& L, cudaStream_t s);
 int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
 int launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
 int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
+int launch_ke_reset_pending(JobState* st, int njobs, cudaStream_t s);
 int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);
 void launch_pid_max(const SlotDev* slot_dev, int64_t n, JobState* st, cudaStream_t s);
 int launch_zero_rho_all(const EngineLaunch& L, int max_nodes, cudaStream_t s);

@@ -260,3 +260,22 @@ def test_extrapolated_warm_start_matches_oracle(engine, orc):
         job.destroy()
     assert sum(runs[1][0][2:]) < sum(runs[0][0][2:])
     assert rel_l2(runs[1][1], runs[0][1]) < 1e-6
+
+
+def test_kinetic_energy_diagnostic(engine):
+    """The FP64 kinetic-energy diagnostic equals sum 1/2 m W v^2 over the velocities a read-back
+    returns (collisionless plasma, so no pair is created by the read-back's own pass; without
+    collisions vz never changes and the diagnostic counts the in-plane velocity)."""
+    cfg, job = _small_plasma(engine, n=100_000)
+    try:
+        engine.step(3)
+        ex = [job.export_species(s) for s in (0, 1)]
+        d = job.diagnostics()
+        for s in (0, 1):
+            e = ex[s]
+            v2 = e["vx"].astype(np.float64) ** 2 + e["vy"].astype(np.float64) ** 2
+            sp = cfg.species[s]
+            ref = 0.5 * sp.mass * sp.weight * v2.sum()
+            assert abs(d["kinetic_energy"][s] - ref) <= 1e-6 * ref, (s, d["kinetic_energy"][s], ref)
+    finally:
+        job.destroy()
