@@ -450,33 +450,60 @@ def run_batched_bench(args):
 
 def run_served_bench(args):
     """Poisson request stream through the continuous-batching server, against the same
-    stream served one job at a time (each job's measured alone time, replayed FIFO)."""
+    stream served one job at a time (each job's measured alone time, replayed FIFO).  Under
+    torchrun the stream holds N times the requests at N times the rate and every rank serves
+    every N-th request in arrival order (shard.shard_requests), so each GPU sees the one-GPU
+    load; the line reports the whole stream (work summed, makespan the slowest rank's,
+    p50/p99 over all requests)."""
     import torch
-    from pic_cuda_b200 import serve
+    from pic_cuda_b200 import serve, shard
     from pic_cuda_b200.engine import Engine
-    n_req = args.jobs or 48
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n_req = (args.jobs or 48) * world
     scale = args.ppc_scale if args.ppc_scale is not None else 0.05
     sscale = args.steps_scale if args.steps_scale is not None else 0.1
-    reqs = serve.served_requests(n_req, seed=5, ppc_scale=scale, steps_scale=sscale)
+    all_reqs = serve.served_requests(n_req, seed=5, ppc_scale=scale, steps_scale=sscale,
+                                     capacity=serve.B200_CAPACITY * world)
+    reqs = [all_reqs[k] for k in shard.shard_requests([r.arrival for r in all_reqs], world, rank)]
     budget = int((args.budget_gb or 150.0) * 1e9)
-    dev = torch.device("cuda", 0)
-    eng = Engine(0)
-    with ClockSampler(0) as clk:
+    dev = torch.device("cuda", local)
+    eng = Engine(local)
+    with ClockSampler(local) as clk:
         out = serve.Server(engine=eng, budget_bytes=budget, quantum=20, device=dev).run(reqs)
         eng.close()
-        durations = [serve.run_alone(r.spec)[0] for r in reqs]
+        durations = [serve.run_alone(r.spec, device=local)[0] for r in reqs]
     seq = serve.fifo_replay(reqs, durations)
-    line = {"metric": METRIC, "value": out["rate"], "unit": UNIT, "n_gpus": 1, "steps": None, "warmup": 0,
+    makespan, work = shard.reduce_timing(out["makespan"], out["particle_steps"], dist, dev)
+    seq_makespan, seq_work = shard.reduce_timing(seq["makespan"], seq["particle_steps"], dist, dev)
+    lat = shard.gather_latencies([c.latency for c in out["completions"]], dist)
+    seq_lat = shard.gather_latencies(seq["latencies"], dist)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    pct, seq_pct = serve.percentiles(lat), serve.percentiles(seq_lat)
+    rate, seq_rate = work / makespan, seq_work / seq_makespan
+    line = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": None, "warmup": 0,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "mode": "served",
             "config": {"workload": "served", "requests": n_req, "ppc_scale": scale, "steps_scale": sscale,
-                       "grids": "uniform over {129,257,513,1025}^2", "arrivals": "Poisson, 1.5x saturation",
-                       "budget_gb": budget / 1e9, "quantum_steps": 20},
-            "p50_s": out["p50"], "p99_s": out["p99"], "makespan_s": out["makespan"],
+                       "grids": "uniform over {129,257,513,1025}^2", "arrivals": "Poisson, 1.5x saturation per GPU",
+                       "budget_gb": budget / 1e9, "quantum_steps": 20,
+                       "parallelism": f"every {world}-th request per rank" if world > 1 else "single GPU"},
+            "p50_s": pct["p50"], "p99_s": pct["p99"], "makespan_s": makespan,
             "server_seconds_in": out["seconds_in"],
-            "sequential": {"value": seq["rate"], "p50_s": seq["p50"], "p99_s": seq["p99"],
-                           "makespan_s": seq["makespan"]},
-            "speedup_vs_sequential": out["rate"] / seq["rate"] if seq["rate"] > 0 else None,
+            "sequential": {"value": seq_rate, "p50_s": seq_pct["p50"], "p99_s": seq_pct["p99"],
+                           "makespan_s": seq_makespan},
+            "speedup_vs_sequential": rate / seq_rate if seq_rate > 0 else None,
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 

@@ -178,7 +178,7 @@ def fifo_replay(requests: list[Request], durations: list[float]) -> dict:
     makespan = t - min(r.arrival for r in requests) if requests else 0.0
     ps = sum(r.spec.particle_steps for r in requests)
     return {"makespan": makespan, "particle_steps": ps, "rate": ps / makespan if makespan > 0 else 0.0,
-            **percentiles(lat)}
+            "latencies": lat, **percentiles(lat)}
 
 
 def run_alone(spec: JobSpec, device: int = 0, keep_result: bool = False, clock=time.perf_counter):

@@ -27,6 +27,24 @@ def shard_jobs(work: Sequence[float], world: int) -> list[list[int]]:
     return [sorted(o) for o in out]
 
 
+def shard_requests(arrivals: Sequence[float], world: int, rank: int) -> list[int]:
+    """The requests rank `rank` serves: every world-th one in arrival order (ties by index), so
+    each rank sees a Poisson stream at 1/world of the rate.  Returns indices in arrival order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    order = sorted(range(len(arrivals)), key=lambda k: (float(arrivals[k]), k))
+    return order[rank::world]
+
+
+def gather_latencies(lat: Sequence[float], dist=None) -> list[float]:
+    """Every rank's request latencies, concatenated in rank order (one rank: a copy)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(x) for x in lat]
+    out: list = [None] * dist.get_world_size()
+    dist.all_gather_object(out, [float(x) for x in lat])
+    return [x for part in out for x in part]
+
+
 def reduce_timing(ms: float, work: float, dist=None, device=None) -> tuple[float, float]:
     """(max over ranks of the timed region in ms, sum over ranks of the work).  Without a
     process group (one rank) the inputs come back unchanged."""
