@@ -323,6 +323,12 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(args, cfg, n, Te, Ti, Ld, steps_job, local, rank)
+        if dist:
+            # the whole job over all ranks: every rank's particle-steps over the slowest rank's time
+            sec, work = shard.reduce_timing(e2e["seconds"], e2e["value"] * e2e["seconds"], dist, dev)
+            e2e.update(value=work / sec, seconds=sec, ranks=world,
+                       h2d_bytes_per_step=e2e["h2d_bytes_per_step"] * world,
+                       d2h_bytes_per_step=e2e["d2h_bytes_per_step"] * world)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
