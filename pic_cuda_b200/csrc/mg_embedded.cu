@@ -35,6 +35,7 @@
 //   emb_norm_kernel / emb_norm_final_kernel  ||r||^2 and ||rhs||^2 over the FLUID nodes in a
 //       fixed order (per-CTA partials, then one CTA), for the convergence test.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <mutex>
@@ -525,12 +526,16 @@ void smooth_level(const EmbLevels& P, int l, int nu, bool pro, double*& cur, boo
 
 // One V-cycle of Multigrid::vcycle(l0) on the level arrays of P (results in P.phi[l]).
 int emb_vcycle(const EmbLevels& P, int l0, int nu1, int nu2, int options, cudaStream_t s) {
-  static int smem_set[64] = {};
+  // the one-CTA kernel's shared memory above the 48 KB default, once per device
+  static std::atomic<int> smem_set[64];
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !smem_set[dev]) {
-    cudaFuncSetAttribute(emb_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    smem_set[dev] = 1;
+  cudaError_t e0 = cudaGetDevice(&dev);
+  if (e0 != cudaSuccess) return pic_fail(PIC_ERR_CUDA, cudaGetErrorString(e0));
+  if (dev >= 64) return pic_fail(PIC_ERR_ARG, "device index beyond the solver's table");
+  if (!smem_set[dev].load()) {
+    e0 = cudaFuncSetAttribute(emb_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e0 != cudaSuccess) return pic_fail(PIC_ERR_CUDA, cudaGetErrorString(e0));
+    smem_set[dev].store(1);
   }
   const bool bilinear = options & PIC_EMB_PROLONG_BILINEAR;
   const int any = (options & PIC_EMB_COARSEN_ANY) ? 1 : 0;
