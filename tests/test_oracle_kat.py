@@ -292,3 +292,87 @@ def test_embedded_reference_operators_diverge_coarsen_any_converges(orc):
     out, cyc, rel = orc.emb_solve(phi, rhs, mask, bc, h, 8, tol=1e-10, max_cycles=100, options=1)
     assert rel < 1e-10 and cyc < 100
     assert np.all(out[mask == 1] == 2.5)
+
+
+def _np_emb_vcycle(phi, rhs, mask, bc, h, l, L, options, nu1=2, nu2=2):
+    """Independent numpy statement of Multigrid::vcycle (Multigrid_embedded.cu:159-188) with
+    the intended colour test, for cross-checking the oracle's recursion."""
+    ny, nx = phi.shape
+    h2 = h * h * 4.0 ** l
+    J, I = np.mgrid[0:ny, 0:nx]
+    inner = (I > 0) & (J > 0) & (I < nx - 1) & (J < ny - 1)
+
+    def sweep(colour):
+        for j in range(1, ny - 1):
+            for i in range(1 + ((1 + j + colour) & 1), nx - 1, 2):
+                if mask[j, i] == 0:
+                    s = phi[j - 1, i] + phi[j + 1, i] + phi[j, i - 1] + phi[j, i + 1]
+                    phi[j, i] = 0.25 * (s - h2 * rhs[j, i])
+                elif mask[j, i] == 1 and bc is not None:
+                    phi[j, i] = bc[j, i]
+
+    for _ in range(nu1):
+        sweep(0)
+        sweep(1)
+    if l == L - 1:
+        return
+    r = np.zeros_like(phi)
+    lap = phi[:-2, 1:-1] + phi[2:, 1:-1] + phi[1:-1, :-2] + phi[1:-1, 2:] - 4.0 * phi[1:-1, 1:-1]
+    r[1:-1, 1:-1] = np.where(mask[1:-1, 1:-1] == 0, rhs[1:-1, 1:-1] - (1.0 / h2) * lap, 0.0)
+    nyc, nxc = (ny - 1) // 2 + 1, (nx - 1) // 2 + 1
+    rc = np.zeros((nyc, nxc))
+    mc = np.zeros((nyc, nxc), np.uint8)
+    for jc in range(1, nyc - 1):
+        for ic in range(1, nxc - 1):
+            j, i = 2 * jc, 2 * ic
+            if options & 1:
+                blk = mask[j - 1:j + 2, i - 1:i + 2]
+                m = 1 if (blk == 1).any() else (2 if (blk != 0).any() else 0)
+            else:
+                m = mask[j, i]
+            mc[jc, ic] = m
+            if m == 0:
+                s = r[j, i]
+                s += 0.5 * (r[j, i - 1] + r[j, i + 1] + r[j - 1, i] + r[j + 1, i])
+                s += 0.25 * (r[j - 1, i - 1] + r[j - 1, i + 1] + r[j + 1, i - 1] + r[j + 1, i + 1])
+                rc[jc, ic] = s / 4.0
+    pc = np.zeros((nyc, nxc))
+    _np_emb_vcycle(pc, rc, mc, None, h, l + 1, L, options, nu1, nu2)
+    for j in range(1, ny - 1):
+        for i in range(1, nx - 1):
+            if mask[j, i] != 0:
+                continue
+            a = (j // 2, i // 2)
+            if not (options & 2) or (i % 2 == 0 and j % 2 == 0):
+                v = pc[a]
+            elif i % 2 == 1 and j % 2 == 0:
+                v = 0.5 * (pc[a] + pc[a[0], a[1] + 1])
+            elif i % 2 == 0 and j % 2 == 1:
+                v = 0.5 * (pc[a] + pc[a[0] + 1, a[1]])
+            else:
+                v = 0.25 * (pc[a] + pc[a[0], a[1] + 1] + pc[a[0] + 1, a[1]] + pc[a[0] + 1, a[1] + 1])
+            phi[j, i] += v
+    for _ in range(nu2):
+        sweep(0)
+        sweep(1)
+
+
+@pytest.mark.parametrize("options", [0, 1, 3])
+@pytest.mark.parametrize("nx,ny,levels", [(33, 25, 4), (34, 17, 3)])
+def test_embedded_vcycle_matches_numpy_statement(orc, options, nx, ny, levels):
+    """The oracle's embedded V-cycle (recursion, level sizes, kinds, options) equals an
+    independent numpy statement on rectangular grids, odd and even sizes, with and without
+    phi_bc."""
+    rng = np.random.default_rng(nx * 100 + options)
+    mask = np.zeros((ny, nx), np.uint8)
+    mask[ny // 4: ny // 2, nx // 4: nx // 2 + 1] = 1
+    mask[3 * ny // 5: 3 * ny // 4 + 1, 3 * nx // 5: 4 * nx // 5] = 2
+    rhs = rng.standard_normal((ny, nx))
+    phi = 0.1 * rng.standard_normal((ny, nx))
+    for bc in (np.where(mask == 1, 1.5, 0.0), None):
+        h = 1.0 / (nx - 1)
+        ref = phi.copy()
+        for _ in range(2):
+            _np_emb_vcycle(ref, rhs, mask, bc, h, 0, levels, options)
+        got = orc.emb_vcycles(phi, rhs, mask, bc, h, levels, 2, options=options)
+        assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
