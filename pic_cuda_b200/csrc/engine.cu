@@ -320,9 +320,9 @@ int dev_alloc(pic_engine* E, JobHost& J, void** p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (E->pool_bytes > 0 && E->used_bytes + (int64_t)bytes > E->pool_bytes)
     return fail(PIC_ERR_OOM, "engine memory budget exceeded");
+  // stream-ordered on E->stream: the caller synchronises that stream once before the first
+  // synchronous copy or memset touches the new blocks (then they are usable from any stream)
   cudaError_t e = cudaMallocFromPoolAsync(p, bytes, E->pool, E->stream);
-  // usable from any stream and by synchronous copies once the allocation has completed
-  if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(PIC_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
@@ -955,6 +955,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     }
     double* dw = nullptr;
     ALLOC(dw, w.size() * 8);
+    CK(cudaStreamSynchronize(E->stream));
     CK(cudaMemcpy(dw, w.data(), w.size() * 8, cudaMemcpyHostToDevice));
     D.walls = dw;
   }
@@ -971,6 +972,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
       for (int k = 0; k < p.n_points; ++k) { tab[k] = (float)p.energy_ev[k]; tab[p.n_points + k] = (float)p.sigma_m2[k]; }
       float* dt_ = nullptr;
       ALLOC(dt_, tab.size() * 4);
+      CK(cudaStreamSynchronize(E->stream));
       CK(cudaMemcpy(dt_, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice));
       ProcDev pd{};
       pd.type = p.type; pd.species = p.species; pd.threshold = (float)p.threshold_ev; pd.n = p.n_points;
@@ -986,6 +988,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     }
     ProcDev* dp = nullptr;
     ALLOC(dp, procs.size() * sizeof(ProcDev));
+    CK(cudaStreamSynchronize(E->stream));
     CK(cudaMemcpy(dp, procs.data(), procs.size() * sizeof(ProcDev), cudaMemcpyHostToDevice));
     D.procs = dp;
     D.n_proc = (int)procs.size();
@@ -1016,6 +1019,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     ALLOC(S.hits, cap * 4); ALLOC(S.scratch, cap * 4); ALLOC(S.scratch2, cap * 4);
     ALLOC(S.cell_count, ncells * 4);
     ALLOC(S.scan_part, ((ncells + 2047) / 2048 + 1) * 4);
+    CK(cudaStreamSynchronize(E->stream));
     CK(cudaMemset(S.scratch, 0, cap * 4));
     // zero the vector tails so the mover's whole-chunk loads read defined values
     CK(cudaMemset(S.cell, 0, cap * 4)); CK(cudaMemset(S.fx, 0, cap * 4)); CK(cudaMemset(S.fy, 0, cap * 4));
@@ -1044,6 +1048,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     }
   }
 #undef ALLOC
+  CK(cudaStreamSynchronize(E->stream));   // every allocation of the job has completed
   CK(cudaMemset(D.phi64[0], 0, N * 8));
   CK(cudaMemset(D.phi64[1], 0, N * 8));
   if (D.phi64[2]) CK(cudaMemset(D.phi64[2], 0, N * 8));
