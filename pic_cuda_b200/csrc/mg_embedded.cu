@@ -34,6 +34,8 @@
 //       CTA's shared memory (one launch for the whole lower V-cycle).
 //   emb_norm_kernel / emb_norm_final_kernel  ||r||^2 and ||rhs||^2 over the FLUID nodes in a
 //       fixed order (per-CTA partials, then one CTA), for the convergence test.
+// The shared tiles store each colour's nodes contiguously (struct Tile), so a red-black
+// half-sweep reads its FP64 neighbours at unit stride.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
