@@ -245,7 +245,15 @@ def solve_embedded_f64(phi, rhs, mask, phi_bc, levels: int, h: float, nu_pre: in
     """Embedded-boundary multigrid (Multigrid_embedded.cu:110-188) on CUDA torch tensors:
     phi, rhs, phi_bc FP64 and mask uint8 (PIC_NODE_*), all (ny, nx); phi in place; phi_bc may
     be None.  Returns (cycles, relative residual, converged)."""
+    import torch
     ny, nx = phi.shape
+    for name, a, dt in (("phi", phi, torch.float64), ("rhs", rhs, torch.float64), ("mask", mask, torch.uint8),
+                        ("phi_bc", phi_bc, torch.float64)):
+        if a is None and name == "phi_bc":
+            continue
+        if not (isinstance(a, torch.Tensor) and a.is_cuda and a.dtype == dt and a.is_contiguous()
+                and tuple(a.shape) == (ny, nx)):
+            raise ValueError(f"{name}: a contiguous CUDA {dt} tensor of shape {(ny, nx)} is required")
     cyc = C.c_int()
     rel = C.c_double()
     bc = C.c_void_p(phi_bc.data_ptr()) if phi_bc is not None else None

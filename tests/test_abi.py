@@ -94,3 +94,16 @@ def test_program_written_against_reference_headers_links(tmp_path):
     import compat_io
     exe = compat_io.build_driver(tmp_path)
     assert exe.exists()
+
+
+def test_embedded_solver_checks_its_arrays_on_the_host():
+    """solve_embedded_f64 rejects host, mistyped or misshaped arrays before any device call."""
+    import pytest
+    import torch
+    from pic_cuda_b200.engine import solve_embedded_f64
+    a = torch.zeros((9, 9), dtype=torch.float64)
+    m = torch.zeros((9, 9), dtype=torch.uint8)
+    with pytest.raises(ValueError):
+        solve_embedded_f64(a, a, m, None, 2, 0.1)            # host tensors
+    with pytest.raises(ValueError):
+        solve_embedded_f64(a, a, m.to(torch.int32), None, 2, 0.1)
