@@ -1,11 +1,13 @@
 #!/usr/bin/env python
 """Benchmark of the full 2D electrostatic PIC step (particle-steps/s).
 
-Workload (default, `--workload mcc_mixed`): 1025^2 nodes over 5 cm^2, 1e7 electrons + 1e7
-Ar+ (FP32 state), Te 3 eV, argon 3.2e21 m^-3 null-collision MCC with 512-point synthetic
-tables, FP32 V-cycles inside FP64 defect correction to 1e-9 relative residual, absorbing
-walls, sort every 10 steps.  Synthetic seeded data; the particle state (~0.6 GB) is larger
-than L2, so no explicit flush is needed between steps.
+Workload (default, `--workload large`): 4097^2 nodes over 20 cm^2, 1e8 electrons + 1e8 Ar+
+(FP32 state, uniform positions, Maxwellian Te 2 eV, Ti 0.03 eV), argon 3.2e21 m^-3
+null-collision MCC with 512-point synthetic tables, FP32 V-cycles inside FP64 defect
+correction to 1e-9 relative residual, absorbing walls, counting sort every 10 steps; the
+FP32 deposit gives `value`, the int64 fixed-point deposit is timed beside it (`int64`).
+Synthetic seeded data; the particle state (~5.6 GB) is larger than L2, so no flush is needed
+between steps.  `--workload mcc_mixed` is the 1025^2, 2e7-particle configuration.
 
   value     device-timed throughput (CUDA events on the launching stream, inputs resident)
   e2e       one complete job through the public C ABI with host buffers: load from pinned
@@ -13,6 +15,8 @@ than L2, so no explicit flush is needed between steps.
             every step, export to pinned host memory
   roofline  the fused particle pass (dominant kernel): algorithmic bytes / event time
   cpu_baseline  the FP64 CPU oracle (OpenMP) on a bounded sample of the same workload
+  reference_particle_kernels  the reference's own four FP64 particle kernels (built from its
+            sources) on the same particle count and grid on the same GPU, against the mover
 
 `--impl reference` times the reference path's CPU implementation: the reference has none
 (its only implementation is CUDA), so the FP64 oracle port of its step runs on all host
@@ -46,7 +50,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="mcc_mixed",
+    ap.add_argument("--workload", default="large",
                     choices=["plain_small", "mcc_mixed", "large", "batched", "served", "embedded"])
     ap.add_argument("--jobs", type=int, default=None, help="batched: jobs; served: requests")
     ap.add_argument("--ppc-scale", type=float, default=None, help="batched/served: particles-per-cell factor")
@@ -57,8 +61,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=None,
+                    help="oracle steps timed for the CPU baseline (default 1 on large, else 3)")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-int64", action="store_true", help="large: skip the int64-deposit timing")
     ap.add_argument("--step-path", choices=["graph", "stream"], default="graph",
                     help="timed steps as CUDA-graph launches (default) or stream-ordered launches")
     return ap.parse_args()
@@ -135,23 +141,33 @@ def workload(args):
     return cfg, n, w["Te"], w["Ti"], cfg.Lx, steps_job
 
 
-def cpu_baseline(args, cfg, n, Te, Ti, Ld, state=None):
-    """FP64 oracle step on the host cores, bounded sample: args.cpu_steps full steps."""
+def cpu_steps(args):
+    if args.cpu_steps is not None:
+        return max(1, args.cpu_steps)
+    return 1 if args.workload == "large" else 3
+
+
+def cpu_baseline(args, cfg, n, Te, Ti, Ld, steps=None):
+    """FP64 oracle step on the host cores, bounded sample: `steps` full steps of the whole
+    workload (every particle, the full grid) after one untimed step."""
+    import gc
     from oracle import oracle as orc
     from pic_cuda_b200 import configs as cf
+    steps = steps or cpu_steps(args)
     sim = orc.Sim(cfg)
-    if state is None:
-        state = (cf.maxwellian_state(n, Ld, Te, cf.ME, 1234), cf.maxwellian_state(n, Ld, Ti, cf.M_AR, 1235))
-    sim.load(0, *state[0])
-    sim.load(1, *state[1])
+    for k, (T, m, seed) in enumerate(((Te, cf.ME, 1234), (Ti, cf.M_AR, 1235))):
+        st = cf.maxwellian_state(n, Ld, T, m, seed)
+        sim.load(k, *st)
+        del st
+        gc.collect()
     sim.step(1)  # warm-up (first-touch allocation of the multigrid hierarchy)
     t0 = time.perf_counter()
-    sim.step(args.cpu_steps)
+    sim.step(steps)
     dt = time.perf_counter() - t0
-    np_ = len(sim.export(0)["x"]) + len(sim.export(1)["x"])
-    return {"value": np_ * args.cpu_steps / dt, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
-            "sample": f"{args.cpu_steps} full FP64 oracle steps of {args.workload} ({2 * n} particles, "
-                      f"{cfg.nx}x{cfg.ny}) after 1 warm-up step", "seconds": dt}
+    np_ = sum(len(sim.export(k)["x"]) for k in (0, 1))
+    return {"value": np_ * steps / dt, "unit": UNIT, "cores": orc.num_threads(), "kind": "port",
+            "sample": f"{steps} full FP64 oracle step(s) of {args.workload} ({2 * n} particles, "
+                      f"{cfg.nx}x{cfg.ny}) after 1 untimed step", "seconds": dt, "steps": steps}
 
 
 def run_reference(args):
@@ -159,8 +175,8 @@ def run_reference(args):
     if rank != 0:
         return
     cfg, n, Te, Ti, Ld, _ = workload(args)
-    steps = max(1, min(args.steps, args.cpu_steps))
-    cb = cpu_baseline(argparse.Namespace(**{**vars(args), "cpu_steps": steps}), cfg, n, Te, Ti, Ld)
+    steps = max(1, min(args.steps, args.cpu_steps or (2 if args.workload == "large" else 3)))
+    cb = cpu_baseline(args, cfg, n, Te, Ti, Ld, steps=steps)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
             "warmup": 1, "ms_per_step": 1000.0 * cb["seconds"] / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
@@ -181,7 +197,7 @@ REF_WALLS = [[0, 0, 1, 0], [1, 0, 1, 1], [1, 1, 0, 1], [0, 1, 0, 0], [0.25, 0.25
              [0.75, 0.25, 0.75, 0.75]]
 
 
-def reference_cuda(local, n_per_species=100_000, grid=129, steps=100, warmup=3):
+def reference_cuda(local, n_per_species=100_000, grid=129, steps=30, warmup=3):
     """The reference's own CUDA step (its kernels built from its sources into oracle/_ref,
     re-sequenced headless as main.cu:60-135, CUDA events around the step loop) and this
     engine on the same seeded state, grid, species, walls and solver settings, in the
@@ -231,25 +247,14 @@ def reference_cuda(local, n_per_species=100_000, grid=129, steps=100, warmup=3):
             "timing": "CUDA events around each implementation's step loop on the same B200"}
 
 
-def run_ours(args):
+def timed_steps(args, cfg, n, Te, Ti, Ld, local, rank, dist, clocks=None):
+    """One job of the workload on a fresh engine: W untimed steps, then K steps timed with CUDA
+    events on the launching stream (barriers and synchronisation on both sides), then a
+    stream-ordered region with CUDA events around every particle pass and phase."""
     import torch
-    from pic_cuda_b200 import _lib as L
     from pic_cuda_b200 import configs as cf
     from pic_cuda_b200.engine import Engine
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-
-    cfg, n, Te, Ti, Ld, steps_job = workload(args)
     eng = Engine(local)
     job = eng.add_job(cfg)
     cf.load_plasma(job, n, Ld, Te, Ti, seed=1234 + 17 * rank, device=dev)
@@ -258,15 +263,14 @@ def run_ours(args):
     run_steps = eng.step_graph if args.step_path == "graph" else eng.step
     run_steps(args.warmup, stream=sptr)
     torch.cuda.synchronize(dev)
-    d0 = job.diagnostics()
-    n0 = sum(d0["count"])
+    n0 = sum(job.diagnostics()["count"])
     eng.stats(reset=True)
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # timed region: whole steps as CUDA graph launches (no host synchronisation inside)
-    with ClockSampler(local) as clk:
+    with (clocks if clocks is not None else ClockSampler(local)) as clk:
         ev0.record(stream)
         run_steps(args.steps, stream=sptr)
         ev1.record(stream)
@@ -285,10 +289,72 @@ def run_ours(args):
     torch.cuda.synchronize(dev)
     pst = eng.stats(reset=True)
     eng.profile(False)
-    particles = 0.5 * (n0 + n1)
+    job.destroy()
+    eng.close()
+    return {"ms": ms, "stats": st, "prof": pst, "prof_steps": prof_steps, "particles": 0.5 * (n0 + n1),
+            "relres": d1["relres"], "clocks": clk}
+
+
+def reference_particle_kernels(cfg, particles, mover_ms, Te, Ti, iters=5):
+    """The reference's own FP64 particle kernels of a step (update_coordinates,
+    detect_intersections with its memsets, updateDensity with the rho memset,
+    updateParticleVelocities; kernels.cu:8-131, collisions.cu:7-54, launched as
+    main.cu:64-127 does) on the same particle count and grid, on this GPU, against the fused
+    particle pass.  The reference's multigrid cannot run at these sizes (its cooperative
+    launch fails above 513^2), so only the particle work is compared."""
+    import math
+    from oracle import refh
+    from pic_cuda_b200 import configs as cf
+    if not refh.available():
+        return {"unavailable": "oracle/_ref/libpicref.so not built or no device"}
+    n = int(particles)
+    vmax = (math.sqrt(3.0 * Te * cf.QE / cf.ME), math.sqrt(3.0 * Ti * cf.QE / cf.M_AR))
+    q = [cfg.species[0].charge * cfg.species[0].weight, cfg.species[1].charge * cfg.species[1].weight]
+    m = [cfg.species[0].mass * cfg.species[0].weight, cfg.species[1].mass * cfg.species[1].weight]
+    ms = refh.particle_kernels_timed(n, cfg.nx, cfg.ny, cfg.Lx, cfg.Ly, cfg.dt, q, m, vmax, iters=iters)
+    total = sum(ms)
+    return {"particles": n, "grid": f"{cfg.nx}x{cfg.ny}",
+            "ms": {"update_coordinates": ms[0], "detect_intersections": ms[1], "updateDensity": ms[2],
+                   "updateParticleVelocities": ms[3]},
+            "ms_per_pass": total, "ours_mover_ms": mover_ms, "speedup_per_pass": total / mover_ms,
+            "note": "reference FP64 AoS state, unsorted (it never sorts), box walls, no collisions, CUDA events per "
+                    "kernel over %d launches; ours: the fused pass including the null-collision MCC" % iters}
+
+
+def run_ours(args):
+    import torch
+    from pic_cuda_b200 import _lib as L
     from pic_cuda_b200 import shard
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    cfg, n, Te, Ti, Ld, steps_job = workload(args)
+    r = timed_steps(args, cfg, n, Te, Ti, Ld, local, rank, dist)
+    ms, st, pst, prof_steps, particles = r["ms"], r["stats"], r["prof"], r["prof_steps"], r["particles"]
     ms_max, particles_all = shard.reduce_timing(ms, particles, dist, dev)
     value = particles_all * args.steps / (ms_max / 1000.0)
+
+    # the int64 fixed-point deposit on the same workload (every rank takes the same steps)
+    int64 = None
+    if args.workload == "large" and args.deposit == "f32" and not args.no_int64:
+        a64 = argparse.Namespace(**{**vars(args), "deposit": "i64"})
+        cfg64 = workload(a64)[0]
+        r64 = timed_steps(a64, cfg64, n, Te, Ti, Ld, local, rank, dist)
+        ms64, p64 = shard.reduce_timing(r64["ms"], r64["particles"], dist, dev)
+        int64 = {"ms_per_step": ms64 / args.steps, "value": p64 * args.steps / (ms64 / 1000.0), "unit": UNIT,
+                 "vcycles_per_step": r64["stats"]["vcycles"] / max(r64["stats"]["steps"], 1),
+                 "mover_ms": r64["prof"]["mover_ms"] / max(r64["prof"]["mover_launches"], 1),
+                 "clocks": r64["clocks"].summary()}
 
     # roofline of the fused particle pass
     peak, peak_kind = peaks()
@@ -300,7 +366,9 @@ def run_ours(args):
     tf = ROOT / "profiles" / "mover_traffic.json"
     if tf.exists():
         t = json.loads(tf.read_text())
-        traffic = t["bytes_per_particle"] * particles
+        t = t.get(args.workload, t) if isinstance(t, dict) else t
+        if "bytes_per_particle" in t:
+            traffic = t["bytes_per_particle"] * particles
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "mover_kernel (fused kick/MCC/drift/walls/deposit)",
                 "bytes_per_particle": bpp, "mover_ms": mover_ms, "peak_source": f"{peak_kind} hbm_gbs",
@@ -338,23 +406,27 @@ def run_ours(args):
                    "precision": "FP32 particles and V-cycles, FP64 defect correction and diagnostics",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "state larger than L2 (no flush needed)",
-                   "vcycles_per_step": st["vcycles"] / max(st["steps"], 1),
+                   "vcycles_per_step": kvc,
                    "phase_ms_per_step_stream_ordered": {k: v / prof_steps for k, v in pst["phase_ms"].items()},
                    "step_path": ("pic_step_graph (CUDA graph per step, V-cycle loop as a conditional WHILE node)"
                                  if args.step_path == "graph" else "pic_step (stream-ordered launches)")},
+        "int64": int64,
         "roofline": roofline,
         "step_roofline": step_roofline,
         "gpu_launches": st["kernel_launches"],
-        "clocks": clk.summary(),
+        "clocks": r["clocks"].summary(),
         "e2e": e2e,
     }
+    if rank == 0 and world == 1 and not args.no_ref_cuda:
+        if args.workload in ("large", "mcc_mixed"):
+            try:
+                line["reference_particle_kernels"] = reference_particle_kernels(cfg, particles, mover_ms, Te, Ti)
+            except (OSError, AssertionError) as e:
+                line["reference_particle_kernels"] = {"unavailable": str(e)}
+        line["reference_cuda_demo"] = reference_cuda(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(args, cfg, n, Te, Ti, Ld)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    if rank == 0 and world == 1 and not args.no_ref_cuda:
-        line["reference_cuda"] = reference_cuda(local)
-    job.destroy()
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -167,6 +167,7 @@ typedef struct pic_diagnostics {
    * ionisations excepted).  Without MCC vz never changes and only vx, vy are counted. */
   double kinetic_energy[PIC_MAX_SPECIES];
   uint32_t status;                       /* sticky device status bits (PIC_ERR_* << k)  */
+  uint32_t next_pid;                     /* id the next created particle receives        */
 } pic_diagnostics;
 
 typedef struct pic_engine_stats {
@@ -297,9 +298,14 @@ int pic_solve_embedded_f64(double* phi, const double* rhs, const uint8_t* mask, 
  * code in a time-critical loop that must not stall other streams (cudaMalloc/cudaFree may
  * synchronise the whole device; the other entry point's first call per shape also builds
  * an internal engine).
+ * - Argument limits (both solvers): levels in [0, levels of a full hierarchy], nu_pre and
+ *   nu_post in [0, 16], nu_coarse in [0, 1000], omega in (0, 2), max_cycles >= 1, tol >= 0;
+ *   anything else returns PIC_ERR_ARG.
  * - The first call on each device looks up the array's address for that device
  *   (cudaGetSymbolAddress, with that device current); make that first call before any
- *   stream capture.
+ *   stream capture.  The address is kept for the life of the process: do not call this
+ *   across a cudaDeviceReset (or a destroyed and re-created primary context) on that
+ *   device, which would leave the kept address pointing at freed memory.
  * - Nothing needs to be zero beforehand: each call clears the correction on every level
  *   and recomputes every scratch value before reading it.
  * - The array is shared by all calls on a device: calls that overlap in time (on

@@ -60,6 +60,7 @@ def lib():
             "orc_sim_export": (None, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _U32]),
             "orc_sim_get_grid": (None, [C.c_void_p, C.c_int, _D]),
             "orc_sim_set_grid": (None, [C.c_void_p, C.c_int, _D]),
+            "orc_sim_set_counters": (None, [C.c_void_p, _I64, C.c_uint32]),
             "orc_sim_stats": (None, [C.c_void_p, C.POINTER(_I64), C.POINTER(C.c_int), _D, C.POINTER(_I64),
                                      C.POINTER(_I64), C.POINTER(_I64)]),
             "orc_sim_drift_walls": (None, [C.c_void_p]),
@@ -315,6 +316,10 @@ class Sim:
 
     def numax(self, k):
         return lib().orc_sim_numax(self.h, k)
+
+    def set_counters(self, step, next_pid):
+        """Continue a running engine job: its completed step count and next particle id."""
+        lib().orc_sim_set_counters(self.h, int(step), int(next_pid))
 
     def stats(self):
         step, cyc, rel, nio = C.c_int64(), C.c_int(), C.c_double(), C.c_int64()

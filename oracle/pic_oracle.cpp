@@ -743,6 +743,13 @@ ORC_API void orc_sim_set_grid(void* h, int which, const double* in) {
   std::copy(in, in + g.size(), g.begin());
   if (which == PIC_GRID_PHI) s->have_prev = false;
 }
+// Step index (the Philox key of the next collision phase) and the id the next created
+// particle receives: set from a running engine job so that the oracle continues it.
+ORC_API void orc_sim_set_counters(void* h, int64_t step, uint32_t next_pid) {
+  OracleSim* s = (OracleSim*)h;
+  s->step = step;
+  s->next_pid = next_pid;
+}
 ORC_API void orc_sim_stats(void* h, int64_t* step, int* cycles, double* relres, int64_t* absorbed,
                            int64_t* ncoll, int64_t* nioniz) {
   OracleSim* s = (OracleSim*)h;
@@ -886,59 +893,74 @@ ORC_API void orc_sim_mcc(void* h) {
     // (the configuration guarantees nu_max dt <= 1).
     const double numax = s->numax[k];
     const double pnull = numax * s->dt;
-    for (int64_t p = 0; p < n; ++p) {
-      double u[4];
-      draw4(c.seed, S.pid[p], step, 0u, u);
-      if (!(u[0] < pnull)) continue;
-      const double v2 = S.vx[p] * S.vx[p] + S.vy[p] * S.vy[p] + S.vz[p] * S.vz[p];
-      const double sp = std::sqrt(v2);
-      const double E = 0.5 * S.m * v2 / kQe;
-      const double target = u[1] * numax;
-      double acc = 0.0;
-      int chosen = -1;
-      for (int q : mine) {
-        acc += ng * s->procs[q].t.eval(E) * sp;
-        if (target < acc) { chosen = q; break; }
+    // particles are independent: OpenMP over them, per-thread counters and pair lists (the
+    // pairs are ordered by parent pid afterwards, so the result does not depend on threads)
+    std::vector<int64_t> cnt(PIC_MAX_PROCESSES, 0);
+#pragma omp parallel
+    {
+      std::vector<int64_t> my_cnt(PIC_MAX_PROCESSES, 0);
+      std::vector<NewPair> my_pairs;
+#pragma omp for schedule(static)
+      for (int64_t p = 0; p < n; ++p) {
+        double u[4];
+        draw4(c.seed, S.pid[p], step, 0u, u);
+        if (!(u[0] < pnull)) continue;
+        const double v2 = S.vx[p] * S.vx[p] + S.vy[p] * S.vy[p] + S.vz[p] * S.vz[p];
+        const double sp = std::sqrt(v2);
+        const double E = 0.5 * S.m * v2 / kQe;
+        const double target = u[1] * numax;
+        double acc = 0.0;
+        int chosen = -1;
+        for (int q : mine) {
+          acc += ng * s->procs[q].t.eval(E) * sp;
+          if (target < acc) { chosen = q; break; }
+        }
+        if (chosen < 0) continue;
+        const Proc& P = s->procs[chosen];
+        double d[3];
+        if (P.type == PIC_PROC_ELASTIC) {
+          iso_dir(u[2], u[3], d);
+          const double cosx = sp > 0 ? (S.vx[p] * d[0] + S.vy[p] * d[1] + S.vz[p] * d[2]) / sp : 1.0;
+          const double Ep = E * (1.0 - 2.0 * S.m / c.gas_mass * (1.0 - cosx));
+          const double vn = speed_of_energy(std::max(0.0, Ep), S.m);
+          S.vx[p] = vn * d[0]; S.vy[p] = vn * d[1]; S.vz[p] = vn * d[2];
+        } else if (P.type == PIC_PROC_EXCITATION) {
+          if (E < P.thr) continue;
+          iso_dir(u[2], u[3], d);
+          const double vn = speed_of_energy(E - P.thr, S.m);
+          S.vx[p] = vn * d[0]; S.vy[p] = vn * d[1]; S.vz[p] = vn * d[2];
+        } else if (P.type == PIC_PROC_IONIZATION) {
+          if (E < P.thr) continue;
+          double u2[4];
+          draw4(c.seed, S.pid[p], step, 1u, u2);
+          const double Er = E - P.thr, B = 10.0;
+          const double Eej = B * std::tan(u2[0] * std::atan(Er / (2.0 * B)));
+          const double Esc = std::max(0.0, Er - Eej);
+          iso_dir(u[2], u[3], d);
+          const double vs = speed_of_energy(Esc, S.m);
+          NewPair np;
+          np.parent = S.pid[p]; np.x = S.x[p]; np.y = S.y[p];
+          double d2[3];
+          iso_dir(u2[1], u2[2], d2);
+          const double ve = speed_of_energy(Eej, s->sp[c.ionization_electron_species].m);
+          for (int a = 0; a < 3; ++a) np.ve[a] = ve * d2[a];
+          neutral_velocity(c.seed, S.pid[p], step, vth_n, np.vi);
+          my_pairs.push_back(np);
+          S.vx[p] = vs * d[0]; S.vy[p] = vs * d[1]; S.vz[p] = vs * d[2];
+        } else if (P.type == PIC_PROC_CHARGE_EXCHANGE) {
+          double vn[3];
+          neutral_velocity(c.seed, S.pid[p], step, vth_n, vn);
+          S.vx[p] = vn[0]; S.vy[p] = vn[1]; S.vz[p] = vn[2];
+        }
+        my_cnt[chosen]++;
       }
-      if (chosen < 0) continue;
-      const Proc& P = s->procs[chosen];
-      double d[3];
-      if (P.type == PIC_PROC_ELASTIC) {
-        iso_dir(u[2], u[3], d);
-        const double cosx = sp > 0 ? (S.vx[p] * d[0] + S.vy[p] * d[1] + S.vz[p] * d[2]) / sp : 1.0;
-        const double Ep = E * (1.0 - 2.0 * S.m / c.gas_mass * (1.0 - cosx));
-        const double vn = speed_of_energy(std::max(0.0, Ep), S.m);
-        S.vx[p] = vn * d[0]; S.vy[p] = vn * d[1]; S.vz[p] = vn * d[2];
-      } else if (P.type == PIC_PROC_EXCITATION) {
-        if (E < P.thr) continue;
-        iso_dir(u[2], u[3], d);
-        const double vn = speed_of_energy(E - P.thr, S.m);
-        S.vx[p] = vn * d[0]; S.vy[p] = vn * d[1]; S.vz[p] = vn * d[2];
-      } else if (P.type == PIC_PROC_IONIZATION) {
-        if (E < P.thr) continue;
-        double u2[4];
-        draw4(c.seed, S.pid[p], step, 1u, u2);
-        const double Er = E - P.thr, B = 10.0;
-        const double Eej = B * std::tan(u2[0] * std::atan(Er / (2.0 * B)));
-        const double Esc = std::max(0.0, Er - Eej);
-        iso_dir(u[2], u[3], d);
-        const double vs = speed_of_energy(Esc, S.m);
-        NewPair np;
-        np.parent = S.pid[p]; np.x = S.x[p]; np.y = S.y[p];
-        double d2[3];
-        iso_dir(u2[1], u2[2], d2);
-        const double ve = speed_of_energy(Eej, s->sp[c.ionization_electron_species].m);
-        for (int a = 0; a < 3; ++a) np.ve[a] = ve * d2[a];
-        neutral_velocity(c.seed, S.pid[p], step, vth_n, np.vi);
-        pairs.push_back(np);
-        S.vx[p] = vs * d[0]; S.vy[p] = vs * d[1]; S.vz[p] = vs * d[2];
-      } else if (P.type == PIC_PROC_CHARGE_EXCHANGE) {
-        double vn[3];
-        neutral_velocity(c.seed, S.pid[p], step, vth_n, vn);
-        S.vx[p] = vn[0]; S.vy[p] = vn[1]; S.vz[p] = vn[2];
+#pragma omp critical
+      {
+        for (int q = 0; q < PIC_MAX_PROCESSES; ++q) cnt[q] += my_cnt[q];
+        pairs.insert(pairs.end(), my_pairs.begin(), my_pairs.end());
       }
-      s->ncoll[k][chosen]++;
     }
+    for (int q = 0; q < PIC_MAX_PROCESSES; ++q) s->ncoll[k][q] += cnt[q];
   }
   // New pairs in ascending parent-pid order: electron pid = next + 2r, ion pid = next + 2r + 1.
   std::sort(pairs.begin(), pairs.end(), [](const NewPair& a, const NewPair& b) { return a.parent < b.parent; });

@@ -317,3 +317,93 @@ RH_API int refh_elastic(int n, double* vx, double* vy, double mass, double densi
   cudaFree(xs.energies); cudaFree(xs.sigmas);
   return bad;
 }
+
+// Timing of the reference's four particle kernels of a step on n particles of the reference's
+// FP64 AoS state (Particles2D), on an m x nn grid over X x Y with the four domain walls
+// (main.cu:190-193), in the order and launch shape of updateSimulationCUDA (main.cu:60-127):
+//   ms_out[0] update_coordinates (kernels.cu:8)
+//   ms_out[1] the hit-list memsets (main.cu:72-73) + detect_intersections (collisions.cu:7)
+//   ms_out[2] the rho memset (main.cu:93) + updateDensity (kernels.cu:26)
+//   ms_out[3] updateParticleVelocities (kernels.cu:71)
+// each averaged over `iters` launches after one untimed round (CUDA events, legacy stream).
+// The state is filled on the device: positions uniform in the domain, velocities uniform in
+// [-vmax_s, vmax_s] for species s = type (half the particles each, interleaved at random), as
+// the reference holds particles unsorted.  Removal and the field solve are not timed.
+namespace {
+__device__ __forceinline__ unsigned long long rh_mix(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double rh_u01(unsigned long long z) { return (double)(z >> 11) * (1.0 / 9007199254740992.0); }
+__global__ void rh_fill_state(double2* r, double2* r_old, double2* v, int* type, int n, double X, double Y,
+                              double vmax0, double vmax1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long b = 4ull * (unsigned long long)i;
+  const int t = (int)(rh_mix(b) & 1ull);
+  const double vm = t ? vmax1 : vmax0;
+  const double2 p = make_double2(X * rh_u01(rh_mix(b + 1)), Y * rh_u01(rh_mix(b + 2)));
+  const unsigned long long zv = rh_mix(b + 3);
+  r[i] = p;
+  r_old[i] = p;
+  v[i] = make_double2(vm * (2.0 * rh_u01(zv) - 1.0), vm * (2.0 * rh_u01(rh_mix(zv)) - 1.0));
+  type[i] = t;
+}
+}  // namespace
+
+RH_API int refh_particle_kernels_timed(int n, int m, int nn, double X, double Y, double dt, const double* q,
+                                       const double* mass, double vmax0, double vmax1, int iters, float* ms_out) {
+  if (n <= 0 || iters <= 0) return 1;
+  Particles2D particles(n);
+  particles.change_species(0, mass[0], q[0]);
+  particles.add_species(mass[1], q[1]);
+  Grid2D grid(m, nn, X, Y);
+  Boundaries2D boundaries((int)X, (int)Y, m, nn);
+  boundaries.add_wall(0, 0, X, 0);
+  boundaries.add_wall(X, 0, X, Y);
+  boundaries.add_wall(X, Y, 0, Y);
+  boundaries.add_wall(0, Y, 0, 0);
+  boundaries.compile_walls();
+  const int tpb = 256, pb = (n + tpb - 1) / tpb;
+  rh_fill_state<<<pb, tpb>>>(particles.r, particles.r_old, particles.v, particles.type, n, X, Y, vmax0, vmax1);
+  cudaMemset(grid.phi, 0, sizeof(double) * m * nn);
+  cudaMemset(grid.E, 0, sizeof(double2) * m * nn);
+  particles.last_alive = n;
+  int bad = ck(cudaDeviceSynchronize());
+  if (bad) return bad;
+  cudaEvent_t ev[5];
+  for (auto& e : ev) cudaEventCreate(&e);
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  for (int it = 0; it <= iters; ++it) {
+    cudaEventRecord(ev[0]);
+    update_coordinates<<<pb, tpb>>>(particles.r, particles.r_old, particles.v, n, dt);
+    cudaEventRecord(ev[1]);
+    cudaMemset(particles.collision_counter, 0, sizeof(int));
+    cudaMemset(particles.collided_indices, -1, n * sizeof(int));
+    detect_intersections<<<pb, tpb>>>(particles.r_old, particles.r, boundaries.d_walls, particles.collided_indices,
+                                      particles.collision_counter, n, boundaries.wall_count);
+    cudaEventRecord(ev[2]);
+    cudaMemset(grid.rho, 0, grid.m * grid.n * sizeof(double));
+    updateDensity<<<pb, tpb>>>(grid.rho, particles.r, particles.q, particles.type, grid.m, grid.n, grid.dx, grid.dy,
+                               n);
+    cudaEventRecord(ev[3]);
+    updateParticleVelocities<<<pb, tpb>>>(particles.v, grid.E, particles.r, particles.type, particles.q, particles.m,
+                                          n, grid.dx, grid.dy, grid.m, grid.n, dt);
+    cudaEventRecord(ev[4]);
+    bad |= ck(cudaEventSynchronize(ev[4]));
+    if (it == 0) continue;
+    for (int k = 0; k < 4; ++k) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      acc[k] += ms;
+    }
+  }
+  for (int k = 0; k < 4; ++k) ms_out[k] = acc[k] / iters;
+  bad |= ck(cudaGetLastError());
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (boundaries.d_walls) cudaFree(boundaries.d_walls);
+  if (boundaries.d_walls_int) cudaFree(boundaries.d_walls_int);
+  return bad;
+}

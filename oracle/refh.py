@@ -33,6 +33,8 @@ def lib():
         L.refh_emb_kernels.argtypes = [C.c_int, C.c_int, _D, _D, _U8, _D, C.c_double, _D, _D, _D, _D, _U8, _D]
         L.refh_emb_vcycles.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, _D, _D, _U8, _D,
                                        C.POINTER(C.c_float)]
+        L.refh_particle_kernels_timed.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D,
+                                                  _D, C.c_double, C.c_double, C.c_int, C.POINTER(C.c_float)]
         _lib = L
     return _lib
 
@@ -137,3 +139,15 @@ def emb_vcycles_timed(phi, rhs, mask, bc, h, levels, cycles, warmup=2):
                                 mask.ctypes.data_as(C.POINTER(C.c_uint8)), _d(bc), C.byref(ms))
     assert rc == 0
     return phi, ms.value
+
+
+def particle_kernels_timed(n, m, nn, X, Y, dt, q, mass, vmax, iters=5):
+    """The reference's four particle kernels of a step (update_coordinates, memsets +
+    detect_intersections, rho memset + updateDensity, updateParticleVelocities) on n
+    particles of its FP64 AoS state, each timed with CUDA events; ms per launch in that order."""
+    q = np.ascontiguousarray(q, np.float64)
+    mass = np.ascontiguousarray(mass, np.float64)
+    ms = (C.c_float * 4)()
+    rc = lib().refh_particle_kernels_timed(n, m, nn, X, Y, dt, _d(q), _d(mass), vmax[0], vmax[1], iters, ms)
+    assert rc == 0
+    return list(ms)

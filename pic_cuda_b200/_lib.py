@@ -57,6 +57,7 @@ class Diagnostics(C.Structure):
         ("collisions", (C.c_int64 * MAX_PROCESSES) * MAX_SPECIES), ("ionizations", C.c_int64),
         ("vcycles", C.c_int32), ("converged", C.c_int32), ("relres", C.c_double), ("total_charge", C.c_double),
         ("kinetic_energy", C.c_double * MAX_SPECIES), ("status", C.c_uint32),
+        ("next_pid", C.c_uint32),
     ]
 
 

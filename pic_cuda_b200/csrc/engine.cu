@@ -1378,6 +1378,7 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
   out->relres = T.relres;
   out->total_charge = T.total_charge;
   out->status = T.status;
+  out->next_pid = T.next_pid;
   return PIC_OK;
 }
 
@@ -1587,6 +1588,13 @@ int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int 
   if (!phi || !rho) return fail(PIC_ERR_ARG, "null grid pointers");
   if (!is_pow2p1(nx) || nx != ny) return fail(PIC_ERR_ARG, "grid must be square with 2^k+1 nodes per side");
   if (!(h > 0)) return fail(PIC_ERR_ARG, "h must be positive");
+  // the limits of a job's solver configuration, checked on every call (a cached solver would
+  // otherwise take an omega or cycle budget that a fresh one rejects)
+  if (levels < 0 || levels > auto_levels(nx)) return fail(PIC_ERR_ARG, "levels out of range");
+  if (nu_pre < 0 || nu_pre > 16 || nu_post < 0 || nu_post > 16 || nu_coarse < 0 || nu_coarse > 1000)
+    return fail(PIC_ERR_ARG, "sweep counts out of range");
+  if (!(omega > 0 && omega < 2)) return fail(PIC_ERR_ARG, "omega must be in (0, 2)");
+  if (max_cycles < 1 || !(tol >= 0)) return fail(PIC_ERR_ARG, "max_cycles >= 1 and tol >= 0 required");
   int device = 0;
   CK(cudaGetDevice(&device));
   std::lock_guard<std::mutex> lk(g_solver_mu);

@@ -162,7 +162,7 @@ class Job:
             "collisions": [[d.collisions[s][p] for p in range(L.MAX_PROCESSES)] for s in range(ns)],
             "ionizations": d.ionizations, "vcycles": d.vcycles, "converged": bool(d.converged), "relres": d.relres,
             "total_charge": d.total_charge, "kinetic_energy": [d.kinetic_energy[s] for s in range(ns)],
-            "status": d.status,
+            "status": d.status, "next_pid": d.next_pid,
         }
 
     def destroy(self) -> None:
@@ -227,39 +227,77 @@ def bytes_needed(cfg: L.JobConfig) -> int:
     return b.value
 
 
+def check_device_arrays(arrays, shape, device=None):
+    """Validate the arrays of a stateless solver call on the host, before anything launches.
+
+    arrays: (name, tensor or None, torch dtype, optional) tuples.  Every given array must be a
+    contiguous CUDA tensor of `shape` and its dtype, and all of them must sit on one device
+    (the first array's, or `device`).  Returns that device.  Raises ValueError otherwise: a
+    kernel handed a host pointer, a wrong-sized buffer or another GPU's memory would read out
+    of bounds or over the peer link."""
+    dev = device
+    for name, a, dt, optional in arrays:
+        if a is None:
+            if optional:
+                continue
+            raise ValueError(f"{name}: an array is required")
+        if not (getattr(a, "is_cuda", False) and a.dtype == dt and a.is_contiguous()
+                and tuple(a.shape) == tuple(shape)):
+            raise ValueError(f"{name}: a contiguous CUDA {dt} tensor of shape {tuple(shape)} is required")
+        if dev is None:
+            dev = a.device
+        elif a.device != dev:
+            raise ValueError(f"{name}: on {a.device}, but the call runs on {dev}; all arrays must share one device")
+    return dev
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
 def solve_multigrid_f64(phi, rho, nx: int, ny: int, levels: int, h: float, omega: float = 1.25, nu_pre: int = 3,
-                        nu_post: int = 3, nu_coarse: int = 20, tol: float = 1e-5, max_cycles: int = 50):
-    """solve_multigrid (Multigrid.cu:573) on CUDA torch tensors (FP64, in place on phi)."""
+                        nu_post: int = 3, nu_coarse: int = 20, tol: float = 1e-5, max_cycles: int = 50, stream=None,
+                        static: bool = False):
+    """solve_multigrid (Multigrid.cu:573) on CUDA torch tensors (FP64, (ny, nx), in place on
+    phi), on the arrays' device.  static=True calls pic_solve_multigrid_f64_static (no device
+    allocation; grids up to PIC_STATIC_MG_MAX_SIDE nodes per side).  Returns (cycles,
+    relative residual, converged)."""
+    import torch
+    dev = check_device_arrays([("phi", phi, torch.float64, False), ("rho", rho, torch.float64, False)], (ny, nx))
+    fn = L.lib().pic_solve_multigrid_f64_static if static else L.lib().pic_solve_multigrid_f64
     cyc = C.c_int()
     rel = C.c_double()
-    rc = L.lib().pic_solve_multigrid_f64(C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()), nx, ny, levels, h,
-                                         omega, nu_pre, nu_post, nu_coarse, tol, max_cycles, None, C.byref(cyc),
-                                         C.byref(rel))
+    with torch.cuda.device(dev):
+        rc = fn(C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()), nx, ny, levels, h, omega, nu_pre, nu_post,
+                nu_coarse, tol, max_cycles, _stream_ptr(stream), C.byref(cyc), C.byref(rel))
     if rc not in (L.PIC_OK, L.PIC_ERR_NOT_CONVERGED):
-        L.check(rc, "pic_solve_multigrid_f64")
+        L.check(rc, "pic_solve_multigrid_f64_static" if static else "pic_solve_multigrid_f64")
     return cyc.value, rel.value, rc == L.PIC_OK
 
 
 def solve_embedded_f64(phi, rhs, mask, phi_bc, levels: int, h: float, nu_pre: int = 2, nu_post: int = 2,
-                       options: int = 0, tol: float = 1e-10, max_cycles: int = 100):
+                       options: int = 0, tol: float = 1e-10, max_cycles: int = 100, stream=None):
     """Embedded-boundary multigrid (Multigrid_embedded.cu:110-188) on CUDA torch tensors:
-    phi, rhs, phi_bc FP64 and mask uint8 (PIC_NODE_*), all (ny, nx); phi in place; phi_bc may
-    be None.  Returns (cycles, relative residual, converged)."""
+    phi, rhs, phi_bc FP64 and mask uint8 (PIC_NODE_*), all (ny, nx) and on one device; phi in
+    place; phi_bc may be None.  Runs on the arrays' device.  Returns (cycles, relative
+    residual, converged)."""
     import torch
+    if not hasattr(phi, "shape") or len(phi.shape) != 2:
+        raise ValueError("phi: a 2-D CUDA float64 tensor is required")
     ny, nx = phi.shape
-    for name, a, dt in (("phi", phi, torch.float64), ("rhs", rhs, torch.float64), ("mask", mask, torch.uint8),
-                        ("phi_bc", phi_bc, torch.float64)):
-        if a is None and name == "phi_bc":
-            continue
-        if not (isinstance(a, torch.Tensor) and a.is_cuda and a.dtype == dt and a.is_contiguous()
-                and tuple(a.shape) == (ny, nx)):
-            raise ValueError(f"{name}: a contiguous CUDA {dt} tensor of shape {(ny, nx)} is required")
+    dev = check_device_arrays([("phi", phi, torch.float64, False), ("rhs", rhs, torch.float64, False),
+                               ("mask", mask, torch.uint8, False), ("phi_bc", phi_bc, torch.float64, True)],
+                              (ny, nx))
     cyc = C.c_int()
     rel = C.c_double()
     bc = C.c_void_p(phi_bc.data_ptr()) if phi_bc is not None else None
-    rc = L.lib().pic_solve_embedded_f64(C.c_void_p(phi.data_ptr()), C.c_void_p(rhs.data_ptr()),
-                                        C.c_void_p(mask.data_ptr()), bc, nx, ny, levels, h, nu_pre, nu_post, options,
-                                        tol, max_cycles, None, C.byref(cyc), C.byref(rel))
+    with torch.cuda.device(dev):
+        rc = L.lib().pic_solve_embedded_f64(C.c_void_p(phi.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                            C.c_void_p(mask.data_ptr()), bc, nx, ny, levels, h, nu_pre, nu_post,
+                                            options, tol, max_cycles, _stream_ptr(stream), C.byref(cyc),
+                                            C.byref(rel))
     if rc not in (L.PIC_OK, L.PIC_ERR_NOT_CONVERGED):
         L.check(rc, "pic_solve_embedded_f64")
     return cyc.value, rel.value, rc == L.PIC_OK

@@ -107,3 +107,44 @@ def test_embedded_solver_checks_its_arrays_on_the_host():
         solve_embedded_f64(a, a, m, None, 2, 0.1)            # host tensors
     with pytest.raises(ValueError):
         solve_embedded_f64(a, a, m.to(torch.int32), None, 2, 0.1)
+
+
+class _FakeCudaTensor:
+    """Stands in for a CUDA tensor on a given device index (no GPU is touched)."""
+
+    def __init__(self, index, shape, dtype):
+        import torch
+        self.is_cuda = True
+        self.device = torch.device("cuda", index)
+        self.shape = shape
+        self.dtype = dtype
+
+    def is_contiguous(self):
+        return True
+
+    def data_ptr(self):
+        raise AssertionError("a pointer was taken: the call got past validation")
+
+
+def test_solver_bindings_reject_arrays_on_different_devices():
+    """Arrays spread over two GPUs are rejected on the host, before a pointer is taken or a
+    kernel launched (a kernel on one device would otherwise read the other's memory)."""
+    import pytest
+    import torch
+    from pic_cuda_b200.engine import check_device_arrays, solve_embedded_f64, solve_multigrid_f64
+    f64, u8 = torch.float64, torch.uint8
+    a0, a1 = _FakeCudaTensor(0, (9, 9), f64), _FakeCudaTensor(1, (9, 9), f64)
+    m0 = _FakeCudaTensor(0, (9, 9), u8)
+    with pytest.raises(ValueError, match="one device"):
+        solve_embedded_f64(a0, a1, m0, None, 2, 0.1)
+    with pytest.raises(ValueError, match="one device"):
+        solve_embedded_f64(a0, a0, m0, a1, 2, 0.1)
+    with pytest.raises(ValueError, match="one device"):
+        solve_multigrid_f64(a0, a1, 9, 9, 0, 0.1)
+    with pytest.raises(ValueError, match="one device"):
+        solve_multigrid_f64(a1, a0, 9, 9, 0, 0.1, static=True)
+    with pytest.raises(ValueError):
+        solve_multigrid_f64(a0, a0, 17, 17, 0, 0.1)               # shape does not match nx, ny
+    with pytest.raises(ValueError):
+        solve_multigrid_f64(a0, torch.zeros((9, 9), dtype=f64), 9, 9, 0, 0.1)  # host array
+    assert check_device_arrays([("a", a1, f64, False), ("b", a1, f64, False)], (9, 9)) == torch.device("cuda", 1)

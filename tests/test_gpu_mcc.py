@@ -99,3 +99,46 @@ def test_reference_elastic_form_statistics(engine):
         np.testing.assert_array_equal(a["vz"], b["vz"])
     finally:
         job.destroy()
+
+
+def test_file_cross_sections_match_oracle_per_particle(engine, orc):
+    """The reference's argon tables (csf/Ar.txt elastic and csf/Ar+.txt ionisation, non-uniform
+    energy grids from 0 eV and from 15.76 eV, committed as tests/golden/csf_argon.npz) in the
+    null-collision engine: the table lookup takes its bisection branch.  Per particle against
+    the oracle on the same Philox streams, as the synthetic-table test above."""
+    from pathlib import Path
+    from pic_cuda_b200 import xs
+    g = np.load(Path(__file__).resolve().parent / "golden" / "csf_argon.npz")
+    mcc = xs.argon_file_mcc(3.2e21, (g["elastic_E"], g["elastic_sigma"]), (g["ionization_E"], g["ionization_sigma"]))
+    n = 200_000
+    cfg = cf.plasma(65, 0.01, n, dt=1e-11, mcc=mcc, walls=L.WALLS_NONE)
+    cfg.species[0].capacity = cfg.species[1].capacity = n + 50_000
+    job = engine.add_job(cfg)
+    try:
+        cf.load_plasma(job, n, 0.01, 25.0, 0.03, seed=17)  # hot electrons: ionisation fires
+        init = [job.export_species(s) for s in (0, 1)]
+        sim = orc.Sim(cfg)
+        for s in (0, 1):
+            d = init[s]
+            sim.load(s, d["x"], d["y"], d["vx"], d["vy"], d["vz"], d["pid"])
+        sim.set_counters(5, job.diagnostics()["next_pid"])
+        job.run_phases(L.PHASE_MCC, step=5)
+        sim.mcc()
+        st = sim.stats()
+        dg = job.diagnostics()
+        for s in (0, 1):
+            a, b = _by_pid(job.export_species(s)), _by_pid(sim.export(s))
+            assert abs(len(a["pid"]) - len(b["pid"])) <= 2
+            common = np.intersect1d(a["pid"], b["pid"])
+            ia, ib = np.searchsorted(a["pid"], common), np.searchsorted(b["pid"], common)
+            va = np.stack([a["vx"][ia], a["vy"][ia], a["vz"][ia]])
+            vb = np.stack([b["vx"][ib], b["vy"][ib], b["vz"][ib]])
+            bad = np.linalg.norm(va - vb, axis=0) > 3e-4 * np.linalg.norm(vb, axis=0) + 1e-3
+            assert bad.sum() <= max(3, 1e-4 * len(common)), (s, bad.sum())
+            for p in range(4):
+                assert abs(dg["collisions"][s][p] - st["collisions"][s][p]) <= 3, (s, p)
+        assert st["collisions"][0][0] > 1000          # elastic from Ar.txt
+        assert st["ionizations"] > 100                 # ionisation from Ar+.txt
+        assert abs(dg["ionizations"] - st["ionizations"]) <= 2
+    finally:
+        job.destroy()

@@ -376,3 +376,35 @@ def test_embedded_vcycle_matches_numpy_statement(orc, options, nx, ny, levels):
             _np_emb_vcycle(ref, rhs, mask, bc, h, 0, levels, options)
         got = orc.emb_vcycles(phi, rhs, mask, bc, h, levels, 2, options=options)
         assert np.max(np.abs(got - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_read_cross_section_semantics(tmp_path):
+    """read_cross_section (mcc.cu:17-41): comments and blank lines skipped, unparsable lines
+    skipped, extra fields ignored, a missing file gives empty lists."""
+    from pic_cuda_b200.xs import process_table, read_cross_section
+    p = tmp_path / "t.txt"
+    p.write_text("# header\n\n0.0\t1e-20\n1.5 2e-20 extra\nbad line\n3.0\n10 3.5e-20")
+    e, s = read_cross_section(p)
+    assert e == [0.0, 1.5, 10.0] and s == [1e-20, 2e-20, 3.5e-20]
+    assert read_cross_section(tmp_path / "missing.txt") == ([], [])
+    E, S = process_table(e, s)
+    assert E.dtype == np.float64 and np.array_equal(E, E.astype(np.float32).astype(np.float64))
+    with pytest.raises(ValueError):
+        process_table([1.0, 1.0], [0.0, 0.0])
+
+
+def test_csf_fixture_matches_reference_files():
+    """tests/golden/csf_argon.npz holds exactly what the reader returns for the reference's
+    csf/Ar.txt and csf/Ar+.txt (checked where the reference tree is present)."""
+    from pathlib import Path
+    from pic_cuda_b200.xs import read_cross_section
+    g = np.load(Path(__file__).resolve().parent / "golden" / "csf_argon.npz")
+    assert g["elastic_E"][0] == 0.0 and g["ionization_E"][0] == 15.76
+    assert np.all(np.diff(g["elastic_E"]) > 0) and np.all(np.diff(g["ionization_E"]) > 0)
+    ref = Path("/root/reference/csf")
+    if not ref.exists():
+        pytest.skip("reference tree not present")
+    e, s = read_cross_section(ref / "Ar.txt")
+    assert np.array_equal(g["elastic_E"], e) and np.array_equal(g["elastic_sigma"], s)
+    e, s = read_cross_section(ref / "Ar+.txt")
+    assert np.array_equal(g["ionization_E"], e) and np.array_equal(g["ionization_sigma"], s)

@@ -58,3 +58,77 @@ def test_static_solver_rejects_grid_beyond_scratch():
     rc, _, _ = _solve("pic_solve_multigrid_f64_static", phi, rho, n, 1.0 / (n - 1))
     assert rc == L.PIC_ERR_ARG
     assert b"257" in L.lib().pic_last_error()
+
+
+@pytest.mark.parametrize("n,levels", [(3, 0), (5, 0), (65, 2), (257, 3)])
+def test_static_solver_small_grids_and_partial_hierarchies(n, levels):
+    """The smallest grids (one and two levels) and hierarchies cut short of 3 x 3 give the
+    allocating solver's result."""
+    h = 1.0 / (n - 1)
+    phi_a, rho = _problem(n, 11)
+    phi_b = phi_a.clone()
+    rc_a, cyc_a, rel_a = _solve("pic_solve_multigrid_f64", phi_a, rho, n, h, levels)
+    rc_b, cyc_b, rel_b = _solve("pic_solve_multigrid_f64_static", phi_b, rho, n, h, levels)
+    assert rc_a == L.PIC_OK and rc_b == L.PIC_OK, (rc_a, rc_b, L.lib().pic_last_error())
+    assert abs(cyc_a - cyc_b) <= 1
+    assert rel_l2(phi_b.cpu().numpy(), phi_a.cpu().numpy()) < 1e-7
+
+
+def test_static_solver_fixed_cycle_budget_reports_not_converged():
+    """tol = 0 runs exactly max_cycles V-cycles and returns PIC_ERR_NOT_CONVERGED, as the
+    allocating solver does, with the same potential."""
+    import torch
+    n, cycles = 129, 4
+    h = 1.0 / (n - 1)
+    phi_a, rho = _problem(n, 5)
+    phi_b = phi_a.clone()
+    out = []
+    for name, phi in (("pic_solve_multigrid_f64", phi_a), ("pic_solve_multigrid_f64_static", phi_b)):
+        torch.cuda.synchronize()
+        cyc, rel = C.c_int(), C.c_double()
+        rc = getattr(L.lib(), name)(C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()), n, n, 0, h, OMEGA,
+                                    NU_PRE, NU_POST, NU_COARSE, 0.0, cycles, None, C.byref(cyc), C.byref(rel))
+        torch.cuda.synchronize()
+        out.append((rc, cyc.value, rel.value))
+    assert out[0][0] == L.PIC_ERR_NOT_CONVERGED and out[1][0] == L.PIC_ERR_NOT_CONVERGED
+    assert out[0][1] == cycles and out[1][1] == cycles
+    assert rel_l2(phi_b.cpu().numpy(), phi_a.cpu().numpy()) < 1e-7
+
+
+def test_static_solver_allocates_no_device_memory():
+    """After a first call (which looks up the array's address), a second call leaves the
+    device's free memory exactly as it was: nothing is allocated or freed."""
+    import torch
+    n = 257
+    h = 1.0 / (n - 1)
+    phi, rho = _problem(n, 3)
+    rc, _, _ = _solve("pic_solve_multigrid_f64_static", phi.clone(), rho, n, h)
+    assert rc == L.PIC_OK
+    work = phi.clone()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc, _, _ = _solve("pic_solve_multigrid_f64_static", work, rho, n, h)
+    free1, _ = torch.cuda.mem_get_info()
+    assert rc == L.PIC_OK
+    assert free1 == free0
+
+
+def test_both_solvers_apply_the_same_argument_limits():
+    """Arguments outside the solvers' limits give PIC_ERR_ARG from both entry points, before
+    any launch."""
+    import torch
+    n = 33
+    phi, rho = _problem(n, 1)
+    bad = [dict(omega=2.0), dict(omega=0.0), dict(nu_pre=17), dict(nu_post=-1), dict(nu_coarse=1001),
+           dict(max_cycles=0), dict(tol=-1.0), dict(levels=9)]
+    for b in bad:
+        a = dict(levels=0, omega=OMEGA, nu_pre=NU_PRE, nu_post=NU_POST, nu_coarse=NU_COARSE, tol=TOL,
+                 max_cycles=MAX_CYCLES)
+        a.update(b)
+        for name in ("pic_solve_multigrid_f64", "pic_solve_multigrid_f64_static"):
+            cyc, rel = C.c_int(), C.c_double()
+            rc = getattr(L.lib(), name)(C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()), n, n, a["levels"],
+                                        1.0 / (n - 1), a["omega"], a["nu_pre"], a["nu_post"], a["nu_coarse"],
+                                        a["tol"], a["max_cycles"], None, C.byref(cyc), C.byref(rel))
+            assert rc == L.PIC_ERR_ARG, (name, b, rc)
+    torch.cuda.synchronize()
