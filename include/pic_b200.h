@@ -155,7 +155,8 @@ typedef struct pic_diagnostics {
   int64_t step;                          /* steps completed by this job                */
   int64_t count[PIC_MAX_SPECIES];        /* live macro-particles per species            */
   int64_t absorbed[PIC_MAX_SPECIES];     /* absorbed during the last step               */
-  int64_t collisions[PIC_MAX_SPECIES][PIC_MAX_PROCESSES]; /* real collisions last step  */
+  int64_t collisions[PIC_MAX_SPECIES][PIC_MAX_PROCESSES]; /* real collisions last step,
+                                            [species][index of the process in pic_job_config] */
   int64_t ionizations;                   /* electron-ion pairs appended last step       */
   int32_t vcycles;                       /* V-cycles of the last field solve            */
   int32_t converged;                     /* last solve reached tol                      */
@@ -192,7 +193,8 @@ int pic_engine_num_jobs(pic_engine* e, int* n);
 
 /* Load n particles of one species (replaces what was there).  Positions in domain
  * units (FP64), velocities (FP64); pid may be NULL (ids assigned from the job's counter).
- * memory = PIC_MEM_HOST (pageable or pinned) or PIC_MEM_DEVICE. */
+ * memory = PIC_MEM_HOST (pageable or pinned) or PIC_MEM_DEVICE; device arrays may be
+ * written by work still running on any stream: the call first waits for the device. */
 int pic_job_load_species(pic_engine* e, int job, int species, int64_t n,
                          const double* x, const double* y,
                          const double* vx, const double* vy, const double* vz,
@@ -252,7 +254,9 @@ int pic_job_get_hits(pic_engine* e, int job, int species, int64_t capacity,
 /* solve_multigrid (Multigrid.cu:573): lap(phi) = rho on an nx*ny grid, Dirichlet values
  * taken from phi's boundary, warm start from phi.  FP32 V-cycles (nu_pre/nu_post
  * red-black SOR sweeps with omega, nu_coarse on the coarsest level) inside FP64 defect
- * correction.  Scratch comes from a per-device cache keyed by (nx, ny, levels). */
+ * correction.  Scratch comes from a per-device cache keyed by (nx, ny, levels).  stream
+ * NULL: the solve first waits for all work issued on the device (the caller's writes of
+ * phi and rho), then runs on the solver's own stream; the call returns when it is done. */
 int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int levels,
                             double h, double omega, int nu_pre, int nu_post, int nu_coarse,
                             double tol, int max_cycles, void* stream,

@@ -424,7 +424,9 @@ static State& state_of(Particles2D& p, pic_compat::State*& slot) {
   if (!slot) {
     auto* s = new State();
     cuda_ok(cudaGetDevice(&s->device), "cudaGetDevice");
-    cuda_ok(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // a blocking stream: it follows the legacy default stream, on which the reference's
+    // host code and kernels (and so the caller's writes of its arrays) run
+    cuda_ok(cudaStreamCreate(&s->stream), "cudaStreamCreate");
     cuda_ok(cudaEventCreate(&s->ev0), "cudaEventCreate");
     cuda_ok(cudaEventCreate(&s->ev1), "cudaEventCreate");
     s->err = dalloc<int>(1);

@@ -1113,6 +1113,9 @@ int pic_job_load_species(pic_engine* E, int job, int species, int64_t n, const d
   if (rc) return rc;
   const double *dx_ = x, *dy_ = y, *dvx = vx, *dvy = vy, *dvz = vz;
   const uint32_t* dpid = pid;
+  // device arrays may still be in the making on another stream (the engine's streams do not
+  // wait for the legacy default stream): wait for all work issued so far on the device
+  if (memory == PIC_MEM_DEVICE && n > 0) CK(cudaDeviceSynchronize());
   if (memory == PIC_MEM_HOST && n > 0) {
     const size_t nb = (size_t)n * 8;
     rc = ensure_stage(E, nb * 5 + (size_t)n * 4);
@@ -1370,7 +1373,11 @@ int pic_job_diagnostics(pic_engine* E, int job, pic_diagnostics* out) {
     out->count[k] = cnt[k];
     out->absorbed[k] = ab[k];
     out->kinetic_energy[k] = T.ke[k];
-    for (int q = 0; q < PIC_MAX_PROCESSES; ++q) out->collisions[k][q] = q < 8 ? (int64_t)T.collisions[k][q] : 0;
+    // the device counts per process of the species, in configuration order; the diagnostics
+    // report them at the process's index in the job configuration
+    int q = 0;
+    for (int p = 0; p < J.cfg.n_processes && p < PIC_MAX_PROCESSES; ++p)
+      if (J.cfg.processes[p].species == k) out->collisions[k][p] = q < 8 ? (int64_t)T.collisions[k][q++] : 0;
   }
   out->ionizations = T.ionizations;
   out->vcycles = T.cycles;
@@ -1493,6 +1500,7 @@ int pic_job_set_grid(pic_engine* E, int job, int which, const double* in, int me
   const int64_t N = (int64_t)J.dev.nx * J.dev.ny;
   cudaStream_t s = E->stream;
   const double* src = in;
+  if (memory == PIC_MEM_DEVICE) CK(cudaDeviceSynchronize());   // the caller's writes of `in`
   if (memory == PIC_MEM_HOST) {
     rc = ensure_stage(E, N * 8);
     if (rc) return rc;
@@ -1628,6 +1636,9 @@ int pic_solve_multigrid_f64(double* phi, const double* rho, int nx, int ny, int 
   J.dev.omega = (float)omega;
   J.dev.tol = tol;
   J.dev.max_cycles = max_cycles;
+  // without a stream the solve runs on the solver's own stream, after all work issued so far
+  // on the device (the caller's writes of phi and rho)
+  if (!stream) CK(cudaDeviceSynchronize());
   cudaStream_t s = stream ? (cudaStream_t)stream : E->stream;
   CK(cudaMemcpyAsync(E->d_jobs + ctx->job, &J.dev, sizeof(JobDev), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(&E->d_st[ctx->job].phi_cur, 0, sizeof(int), s));

@@ -30,44 +30,23 @@ __global__ void sort_zero(const JobDev* jobs, const SlotDev* slots, const uint8_
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncells; k += gridDim.x * blockDim.x) S.cell_count[k] = 0;
 }
 
-// Particles per lane of a histogram / scatter item: one 16-byte vector load per array and lane.
-constexpr int kSortPPL = 4;
-constexpr int kSortItem = 32 * kSortPPL;
-constexpr uint32_t kNoKey = 0xFFFFFFFFu;   // a particle beyond the slot's count
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;   // a lane past the slot's count
 
-// The cells and keys of a lane's kSortPPL consecutive particles of item `it` (kNoKey past n).
-// Slot arrays hold a multiple of PIC_CHUNK entries, so the vector load stays inside them.
-__device__ __forceinline__ void item_keys(const SlotDev& S, int it, int n, int ncx, uint32_t ncells,
-                                          uint32_t (&c)[kSortPPL], uint32_t (&key)[kSortPPL]) {
-  const int p0 = it * kSortItem + kSortPPL * lane_id();
-  if (p0 + kSortPPL <= n) {
-    const uint4 v = *reinterpret_cast<const uint4*>(S.cell + p0);
-    c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-  } else {
-#pragma unroll
-    for (int k = 0; k < kSortPPL; ++k) c[k] = p0 + k < n ? S.cell[p0 + k] : PIC_CELL_OUT;
-  }
-#pragma unroll
-  for (int k = 0; k < kSortPPL; ++k) key[k] = p0 + k < n ? dense_key(c[k], ncx, ncells) : kNoKey;
-}
-
-// Segments of equal last-run keys over the warp, in lane order: the first and last lane of
-// this lane's segment.  Particles are sorted by cell between sorts and drift slowly, so equal
-// keys mostly sit in neighbouring lanes; where they do not, a key forms several segments,
-// each counted on its own (still correct, one more atomic).
-__device__ __forceinline__ void run_segment(uint32_t rk, int& first, int& last) {
+// Segments of equal keys over the warp, in lane order: the first and last lane of this
+// lane's segment.  Particles are sorted by cell between sorts and drift slowly, so equal keys
+// mostly sit in neighbouring lanes; where they do not, a key forms several segments, each
+// counted on its own (still correct, one more atomic).
+__device__ __forceinline__ void run_segment(uint32_t key, int& first, int& last) {
   const int lane = lane_id();
-  const uint32_t prev = __shfl_up_sync(0xffffffffu, rk, 1);
-  const bool head = lane == 0 || rk != prev;
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool head = lane == 0 || key != prev;
   const unsigned heads = __ballot_sync(0xffffffffu, head);
   first = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
   const unsigned after = lane == 31 ? 0u : heads & (0xfffffffeu << lane);
   last = (after ? __ffs(after) - 1 : 32) - 1;
 }
 
-// Histogram of cell keys: runs of equal keys inside a lane are counted in registers (one
-// atomic per run but the lane's last), the lanes' last runs are summed over warp segments
-// (one atomic per segment).
+// Histogram of cell keys, one atomic per warp segment of equal keys.
 __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
   const int s = blockIdx.y;
   if (!mask[s]) return;
@@ -75,30 +54,13 @@ __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* c
   const JobDev& J = jobs[S.job];
   const int n = counts[s];
   const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
-  const int nitems = (n + kSortItem - 1) / kSortItem;
   const int lane = lane_id();
-  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += (gridDim.x * blockDim.x) >> 5) {
-    uint32_t c[kSortPPL], key[kSortPPL];
-    item_keys(S, it, n, J.ncx, ncells, c, key);
-    uint32_t rk = key[0];
-    int cnt = 1;
-#pragma unroll
-    for (int k = 1; k < kSortPPL; ++k) {
-      if (key[k] == rk) { ++cnt; continue; }
-      if (rk != kNoKey) atomicAdd(S.cell_count + rk, cnt);
-      rk = key[k];
-      cnt = 1;
-    }
+  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
+    const int p = wb + lane;
+    const uint32_t key = p < n ? dense_key(S.cell[p], J.ncx, ncells) : kNoKey;
     int first, last;
-    run_segment(rk, first, last);
-    // inclusive scan of the last runs' lengths inside each segment; its last lane holds the total
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane - o >= first) incl += v;
-    }
-    if (lane == last && rk != kNoKey) atomicAdd(S.cell_count + rk, incl);
+    run_segment(key, first, last);
+    if (lane == last && key != kNoKey) atomicAdd(S.cell_count + key, last - first + 1);
   }
 }
 
@@ -198,9 +160,9 @@ __global__ void __launch_bounds__(256) sort_apply(const JobDev* jobs, const Slot
   }
 }
 
-// Scatter of all seven fields to the positions the scanned counts give: as in sort_hist, one
-// atomic per in-lane run and per warp segment of last runs (it returns the run's first
-// position); a lane's particles are read with one vector load per array.
+// Scatter of all seven fields to the positions the scanned counts give: one atomic per warp
+// segment of equal keys returns the segment's first position.  Every field is loaded before
+// the atomic, so the loads and the atomic's round trip overlap.
 __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
   const int s = blockIdx.y;
   if (!mask[s]) return;
@@ -208,73 +170,24 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
   const JobDev& J = jobs[S.job];
   const int n = counts[s];
   const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
-  const int nitems = (n + kSortItem - 1) / kSortItem;
   const int lane = lane_id();
-  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += (gridDim.x * blockDim.x) >> 5) {
-    uint32_t c[kSortPPL], key[kSortPPL];
-    item_keys(S, it, n, J.ncx, ncells, c, key);
-    int at[kSortPPL];
-    // in-lane runs but the last: positions from their own atomics
-    uint32_t rk = key[0];
-    int cnt = 1, r0 = 0;
-#pragma unroll
-    for (int k = 1; k < kSortPPL; ++k) {
-      if (key[k] == rk) { ++cnt; continue; }
-      if (rk != kNoKey) {
-        const int b = atomicAdd(S.cell_count + rk, cnt);
-#pragma unroll
-        for (int q = 0; q < kSortPPL; ++q)
-          if (q >= r0 && q < k) at[q] = b + (q - r0);
-      }
-      rk = key[k];
-      cnt = 1;
-      r0 = k;
-    }
-    // the lanes' last runs: segmented inclusive scan of their lengths; the segment's last lane
-    // reserves the segment's positions and every lane takes its share in lane order
+  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
+    const int p = wb + lane;
+    const bool in = p < n;
+    const int q = in ? p : 0;
+    const uint32_t c = S.cell[q];
+    const float fx = S.fx[q], fy = S.fy[q], vx = S.vx[q], vy = S.vy[q], vz = S.vz[q];
+    const uint32_t pid = S.pid[q];
+    const uint32_t key = in ? dense_key(c, J.ncx, ncells) : kNoKey;
     int first, last;
-    run_segment(rk, first, last);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane - o >= first) incl += v;
-    }
+    run_segment(key, first, last);
     int base = 0;
-    if (lane == last && rk != kNoKey) base = atomicAdd(S.cell_count + rk, incl);
+    if (lane == last && in) base = atomicAdd(S.cell_count + key, last - first + 1);
     base = __shfl_sync(0xffffffffu, base, last);
-    if (rk != kNoKey) {
-      const int b = base + incl - cnt;
-#pragma unroll
-      for (int q = 0; q < kSortPPL; ++q)
-        if (q >= r0) at[q] = b + (q - r0);
-    }
-    const int p0 = it * kSortItem + kSortPPL * lane;
-    if (p0 + kSortPPL <= n) {
-      const float4 fx = *reinterpret_cast<const float4*>(S.fx + p0);
-      const float4 fy = *reinterpret_cast<const float4*>(S.fy + p0);
-      const float4 vx = *reinterpret_cast<const float4*>(S.vx + p0);
-      const float4 vy = *reinterpret_cast<const float4*>(S.vy + p0);
-      const float4 vz = *reinterpret_cast<const float4*>(S.vz + p0);
-      const uint4 pd = *reinterpret_cast<const uint4*>(S.pid + p0);
-      const float afx[4] = {fx.x, fx.y, fx.z, fx.w}, afy[4] = {fy.x, fy.y, fy.z, fy.w};
-      const float avx[4] = {vx.x, vx.y, vx.z, vx.w}, avy[4] = {vy.x, vy.y, vy.z, vy.w};
-      const float avz[4] = {vz.x, vz.y, vz.z, vz.w};
-      const uint32_t apd[4] = {pd.x, pd.y, pd.z, pd.w};
-#pragma unroll
-      for (int q = 0; q < kSortPPL; ++q) {
-        const int d = at[q];
-        S.cell_b[d] = c[q]; S.fx_b[d] = afx[q]; S.fy_b[d] = afy[q];
-        S.vx_b[d] = avx[q]; S.vy_b[d] = avy[q]; S.vz_b[d] = avz[q]; S.pid_b[d] = apd[q];
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < kSortPPL; ++q)
-        if (p0 + q < n) {
-          const int d = at[q], p = p0 + q;
-          S.cell_b[d] = c[q]; S.fx_b[d] = S.fx[p]; S.fy_b[d] = S.fy[p];
-          S.vx_b[d] = S.vx[p]; S.vy_b[d] = S.vy[p]; S.vz_b[d] = S.vz[p]; S.pid_b[d] = S.pid[p];
-        }
+    if (in) {
+      const int at = base + lane - first;
+      S.cell_b[at] = c; S.fx_b[at] = fx; S.fy_b[at] = fy;
+      S.vx_b[at] = vx; S.vy_b[at] = vy; S.vz_b[at] = vz; S.pid_b[at] = pid;
     }
   }
 }
