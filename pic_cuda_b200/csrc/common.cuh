@@ -62,6 +62,8 @@ struct SlotDev {
   float numax;            // nu_max (1/s)
   float mass;             // kg (or ref units)
   int first_proc, n_proc; // this species' MCC processes in the job's process list
+  ProcDev total;          // sum of this species' cross sections on the union of their energy
+                          // grids (the null-collision test: real iff u nu_max < n sigma_T v)
   long long qfix;         // llrint(qdep * 2^40)
   double ke_factor;       // 0.5 m W (diagnostics)
 };
@@ -149,22 +151,6 @@ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32
 // (2*(x>>9)+1) * 2^-24, exactly representable, in (0, 1).
 __device__ __forceinline__ float u01(uint32_t x) {
   return (float)(2u * (x >> 9) + 1u) * 5.9604644775390625e-8f;
-}
-// First output word of Philox-4x32-10 only (the last round computes just that word): the
-// null-collision candidate test needs u[0] of draw4, nothing else.
-__device__ __forceinline__ float draw_first(uint64_t seed, uint32_t pid, uint32_t step, uint32_t lane) {
-  uint32_t c[4] = {pid, step, lane, 0u};
-  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-#pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
-    const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
-    const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
-  }
-  k0 += 0x9E3779B9u;
-  return u01(__umulhi(0xCD9E8D57u, c[2]) ^ c[1] ^ k0);
 }
 __device__ __forceinline__ void draw4(uint64_t seed, uint32_t pid, uint32_t step, uint32_t lane, float u[4]) {
   uint32_t c[4] = {pid, step, lane, 0u};

@@ -961,6 +961,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   }
   // MCC tables
   std::vector<ProcDev> procs;
+  std::vector<std::vector<float>> proc_tabs;   // host copies of the FP32 tables, as on the device
   if (c.mcc_mode) {
     // order processes by species so each species' processes are contiguous
     std::vector<int> order(c.n_processes);
@@ -985,6 +986,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
       pd.log_e0 = logsp ? (float)std::log(p.energy_ev[0]) : 0.f;
       pd.inv_dlog = logsp ? (float)(1.0 / r0) : 0.f;
       procs.push_back(pd);
+      proc_tabs.push_back(tab);
     }
     ProcDev* dp = nullptr;
     ALLOC(dp, procs.size() * sizeof(ProcDev));
@@ -1040,6 +1042,47 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
     }
     S.first_proc = first;
     S.n_proc = cnt;
+    if (c.mcc_mode == PIC_MCC_NULL_COLLISION && cnt) {
+      // the species' total cross section: every table is piecewise linear, so their sum is
+      // piecewise linear on the union of their energy points (evaluated as the device does:
+      // clamped outside each table, linear inside)
+      std::vector<float> ug;
+      for (int k = first; k < first + cnt; ++k)
+        ug.insert(ug.end(), proc_tabs[k].begin(), proc_tabs[k].begin() + procs[k].n);
+      std::sort(ug.begin(), ug.end());
+      ug.erase(std::unique(ug.begin(), ug.end()), ug.end());
+      const int nu = (int)ug.size();
+      std::vector<float> tt(2 * (size_t)nu);
+      for (int u = 0; u < nu; ++u) {
+        double sum = 0.0;
+        for (int k = first; k < first + cnt; ++k) {
+          const int np = procs[k].n;
+          const float* e = proc_tabs[k].data();
+          const float* sg = e + np;
+          const float E = ug[u];
+          if (E <= e[0]) { sum += sg[0]; continue; }
+          if (E >= e[np - 1]) { sum += sg[np - 1]; continue; }
+          const int q = (int)(std::upper_bound(e, e + np, E) - e) - 1;
+          const double t = ((double)E - e[q]) / ((double)e[q + 1] - e[q]);
+          sum += sg[q] + t * ((double)sg[q + 1] - sg[q]);
+        }
+        tt[u] = ug[u];
+        tt[nu + u] = (float)sum;
+      }
+      float* dtt = nullptr;
+      ALLOC(dtt, tt.size() * 4);
+      CK(cudaStreamSynchronize(E->stream));
+      CK(cudaMemcpy(dtt, tt.data(), tt.size() * 4, cudaMemcpyHostToDevice));
+      ProcDev& T = S.total;
+      T = ProcDev{};
+      T.type = 0; T.species = s; T.n = nu; T.e = dtt; T.s = dtt + nu;
+      bool logsp = nu >= 2 && ug[0] > 0.f;
+      const double r0 = logsp ? std::log((double)ug[1] / ug[0]) : 0.0;
+      for (int k = 1; logsp && k < nu; ++k)
+        if (std::fabs(std::log((double)ug[k] / ug[k - 1]) - r0) > 1e-4 * std::fabs(r0)) logsp = false;
+      T.log_e0 = logsp ? (float)std::log((double)ug[0]) : 0.f;
+      T.inv_dlog = logsp ? (float)(1.0 / r0) : 0.f;
+    }
     if (c.mcc_mode == PIC_MCC_NULL_COLLISION && cnt) {
       const double numax = compute_numax(c, s);
       if (numax * c.dt > 1.0) { free_job(E, J); return fail(PIC_ERR_ARG, "nu_max * dt > 1: time step too large for MCC"); }

@@ -290,11 +290,12 @@ constexpr size_t kMoverSmem = (size_t)kWarps * kQFields * kQueue * sizeof(uint32
 //   loads    cell, fx, fy, vx, vy (+ vz, pid with collisions): one evict-first vector load
 //            per array and lane
 //   pass A   kick (E gathered from the per-step node field; particles are cell-sorted, so a
-//            warp's gathers hit a few cache lines) and the null-collision candidate test;
-//            candidates (~nu_max dt of the particles) leave the item for the warp's queue in
-//            shared memory.  Whenever 32 are queued (and when the warp leaves a slot), one
-//            round collides, drifts, deposits and stores them, one candidate per lane, after
-//            their owners have stored the rest of their items.
+//            warp's gathers hit a few cache lines) and the null-collision test: candidates
+//            (~nu_max dt of the particles) whose collision is real (u1 nu_max below the
+//            species' total n sigma_T v, one table lookup) leave the item for the warp's queue
+//            in shared memory.  Whenever 32 are queued (and when the warp leaves a slot), one
+//            round chooses the process and collides, drifts, deposits and stores them, one
+//            per lane, after their owners have stored the rest of their items.
 //   pass B   drift, absorption (hits appended with one atomic per item), CIC deposit
 //   stores   evict-first vector stores of what changed (vz only in the queue rounds; the
 //            cell word only when some particle of the warp crossed a cell edge)
@@ -464,7 +465,18 @@ mover_kernel(const JobDev* __restrict__ jobs, JobState* __restrict__ st, const S
         int ncand = 0;
 #pragma unroll
         for (int k = 0; k < kPPL; ++k) {
-          cand[k] = valid[k] && draw_first(J.seed, pid[k], mcc_step, 0u) < S.pnull;
+          // candidate with probability nu_max dt; a candidate's collision is real when
+          // u1 nu_max < n sigma_T(E) v (the process is chosen in the queue round, with the
+          // same draw).  Null candidates stay in the item like every other particle.
+          cand[k] = false;
+          if (valid[k]) {
+            float u[4];
+            draw4(J.seed, pid[k], mcc_step, 0u, u);
+            if (u[0] < S.pnull) {
+              const float v2 = vx[k] * vx[k] + vy[k] * vy[k] + vz[k] * vz[k];
+              cand[k] = u[1] * S.numax < J.gas_density * xs_lookup(S.total, S.half_m_over_e * v2) * sqrtf(v2);
+            }
+          }
           m[k] = __ballot_sync(0xffffffffu, cand[k]);
           before[k] = ncand;
           ncand += __popc(m[k]);

@@ -46,6 +46,12 @@ __device__ __forceinline__ void run_segment(uint32_t key, int& first, int& last)
   last = (after ? __ffs(after) - 1 : 32) - 1;
 }
 
+// A warp takes kSortRounds x 32 consecutive particles per iteration, lane-striped (round r,
+// lane l: particle 32 r + l), and issues all their loads before any dependent work, so each
+// warp keeps kSortRounds coalesced requests per array in flight.
+constexpr int kSortRounds = 4;
+constexpr int kSortItem = 32 * kSortRounds;
+
 // Histogram of cell keys, one atomic per warp segment of equal keys.
 __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
   const int s = blockIdx.y;
@@ -54,13 +60,24 @@ __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* c
   const JobDev& J = jobs[S.job];
   const int n = counts[s];
   const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
+  const uint32_t* __restrict__ cell = S.cell;
+  int* const cnt = S.cell_count;
+  const int ncx = J.ncx;
   const int lane = lane_id();
-  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
-    const int p = wb + lane;
-    const uint32_t key = p < n ? dense_key(S.cell[p], J.ncx, ncells) : kNoKey;
-    int first, last;
-    run_segment(key, first, last);
-    if (lane == last && key != kNoKey) atomicAdd(S.cell_count + key, last - first + 1);
+  const int nitems = (n + kSortItem - 1) / kSortItem;
+  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += (gridDim.x * blockDim.x) >> 5) {
+    uint32_t key[kSortRounds];
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+      const int p = it * kSortItem + 32 * r + lane;
+      key[r] = p < n ? dense_key(__ldg(cell + p), ncx, ncells) : kNoKey;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+      int first, last;
+      run_segment(key[r], first, last);
+      if (lane == last && key[r] != kNoKey) atomicAdd(cnt + key[r], last - first + 1);
+    }
   }
 }
 
@@ -161,8 +178,9 @@ __global__ void __launch_bounds__(256) sort_apply(const JobDev* jobs, const Slot
 }
 
 // Scatter of all seven fields to the positions the scanned counts give: one atomic per warp
-// segment of equal keys returns the segment's first position.  Every field is loaded before
-// the atomic, so the loads and the atomic's round trip overlap.
+// segment of equal keys returns the segment's first position.  Every field of the warp's
+// kSortRounds x 32 particles is loaded before the atomics, so loads and atomics overlap; the
+// stores of a round are consecutive across lanes where the order was kept since the last sort.
 __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
   const int s = blockIdx.y;
   if (!mask[s]) return;
@@ -170,25 +188,51 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
   const JobDev& J = jobs[S.job];
   const int n = counts[s];
   const uint32_t ncells = (uint32_t)(J.ncx * J.ncy);
+  const int ncx = J.ncx;
+  const uint32_t* __restrict__ cell = S.cell;
+  const float* __restrict__ fx = S.fx;
+  const float* __restrict__ fy = S.fy;
+  const float* __restrict__ vx = S.vx;
+  const float* __restrict__ vy = S.vy;
+  const float* __restrict__ vz = S.vz;
+  const uint32_t* __restrict__ pid = S.pid;
+  uint32_t* const cell_b = S.cell_b;
+  float* const fx_b = S.fx_b;
+  float* const fy_b = S.fy_b;
+  float* const vx_b = S.vx_b;
+  float* const vy_b = S.vy_b;
+  float* const vz_b = S.vz_b;
+  uint32_t* const pid_b = S.pid_b;
+  int* const cnt = S.cell_count;
   const int lane = lane_id();
-  for (int wb = blockIdx.x * blockDim.x + (threadIdx.x & ~31); wb < n; wb += gridDim.x * blockDim.x) {
-    const int p = wb + lane;
-    const bool in = p < n;
-    const int q = in ? p : 0;
-    const uint32_t c = S.cell[q];
-    const float fx = S.fx[q], fy = S.fy[q], vx = S.vx[q], vy = S.vy[q], vz = S.vz[q];
-    const uint32_t pid = S.pid[q];
-    const uint32_t key = in ? dense_key(c, J.ncx, ncells) : kNoKey;
-    int first, last;
-    run_segment(key, first, last);
-    int base = 0;
-    if (lane == last && in) base = atomicAdd(S.cell_count + key, last - first + 1);
-    base = __shfl_sync(0xffffffffu, base, last);
-    if (in) {
-      const int at = base + lane - first;
-      S.cell_b[at] = c; S.fx_b[at] = fx; S.fy_b[at] = fy;
-      S.vx_b[at] = vx; S.vy_b[at] = vy; S.vz_b[at] = vz; S.pid_b[at] = pid;
+  const int nitems = (n + kSortItem - 1) / kSortItem;
+  for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += (gridDim.x * blockDim.x) >> 5) {
+    uint32_t c[kSortRounds], pd[kSortRounds], key[kSortRounds];
+    float a[kSortRounds], b[kSortRounds], u[kSortRounds], v[kSortRounds], w[kSortRounds];
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+      const int p = it * kSortItem + 32 * r + lane;
+      const int q = p < n ? p : 0;
+      c[r] = __ldg(cell + q); a[r] = __ldg(fx + q); b[r] = __ldg(fy + q);
+      u[r] = __ldg(vx + q); v[r] = __ldg(vy + q); w[r] = __ldg(vz + q); pd[r] = __ldg(pid + q);
+      key[r] = p < n ? dense_key(c[r], ncx, ncells) : kNoKey;
     }
+    int at[kSortRounds];
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r) {
+      int first, last;
+      run_segment(key[r], first, last);
+      int base = 0;
+      if (lane == last && key[r] != kNoKey) base = atomicAdd(cnt + key[r], last - first + 1);
+      at[r] = __shfl_sync(0xffffffffu, base, last) + lane - first;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortRounds; ++r)
+      if (key[r] != kNoKey) {
+        const int d = at[r];
+        cell_b[d] = c[r]; fx_b[d] = a[r]; fy_b[d] = b[r];
+        vx_b[d] = u[r]; vy_b[d] = v[r]; vz_b[d] = w[r]; pid_b[d] = pd[r];
+      }
   }
 }
 
