@@ -548,8 +548,16 @@ def run_served_bench(args):
     n_req = (args.jobs or 48) * world
     scale = args.ppc_scale if args.ppc_scale is not None else 0.05
     sscale = args.steps_scale if args.steps_scale is not None else 0.1
+    # the arrival rate: 1.5 x the particle-steps/s this GPU sustains on a sample of the mix,
+    # measured here (every rank measures its own; rank 0's figure sets the stream)
+    sample = serve.served_requests(32, seed=6, ppc_scale=scale, steps_scale=sscale)
+    capacity = serve.measure_capacity([r.spec for r in sample], device=local)
+    if dist:
+        cap_t = torch.tensor([capacity], dtype=torch.float64, device=torch.device("cuda", local))
+        dist.broadcast(cap_t, 0)
+        capacity = float(cap_t.item())
     all_reqs = serve.served_requests(n_req, seed=5, ppc_scale=scale, steps_scale=sscale,
-                                     capacity=serve.B200_CAPACITY * world)
+                                     capacity=capacity * world)
     reqs = [all_reqs[k] for k in shard.shard_requests([r.arrival for r in all_reqs], world, rank)]
     budget = int((args.budget_gb or 150.0) * 1e9)
     dev = torch.device("cuda", local)
@@ -574,7 +582,9 @@ def run_served_bench(args):
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "mode": "served",
             "config": {"workload": "served", "requests": n_req, "ppc_scale": scale, "steps_scale": sscale,
-                       "grids": "uniform over {129,257,513,1025}^2", "arrivals": "Poisson, 1.5x saturation per GPU",
+                       "grids": "uniform over {129,257,513,1025}^2",
+                       "arrivals": "Poisson at 1.5x the capacity measured in this run on a 32-request sample",
+                       "capacity_measured": capacity,
                        "budget_gb": budget / 1e9, "quantum_steps": 20,
                        "parallelism": f"every {world}-th request per rank" if world > 1 else "single GPU"},
             "p50_s": pct["p50"], "p99_s": pct["p99"], "makespan_s": makespan,

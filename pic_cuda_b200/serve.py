@@ -29,9 +29,43 @@ class Request:
     index: int = 0
 
 
-# Aggregate particle-steps/s of one B200 on the batched mix (measured: 2.1e10), rounded up, so
-# that the default arrival rate keeps the GPU saturated.
+# Aggregate particle-steps/s of one B200 on the batched mix (measured: 2.1e10), rounded up: the
+# arrival rate used when no capacity measured in the run is given (see measure_capacity).
 B200_CAPACITY = 2.5e10
+
+
+def measure_capacity(specs: list[JobSpec], device: int = 0, budget_bytes: int = 40 * 10**9, steps: int = 20,
+                     warmup: int = 3) -> float:
+    """Particle-steps/s this GPU sustains on a sample of the request mix: the sample's jobs
+    (as many as fit `budget_bytes`) stepped together, `steps` steps timed with CUDA events
+    after `warmup` untimed ones.  The served bench sets its arrival rate from this figure."""
+    import torch
+    from .engine import Engine
+    eng = Engine(device)
+    jobs, used, work = [], 0, 0.0
+    try:
+        for sp in specs:
+            need = bytes_needed(job_config(sp))
+            if jobs and used + need > budget_bytes:
+                continue
+            job = eng.add_job(job_config(sp))
+            load_job(job, sp, device=torch.device("cuda", device))
+            jobs.append(job)
+            used += need
+            work += 2.0 * sp.n_per_species
+        stream = torch.cuda.Stream(device=device)
+        eng.step_graph(warmup, stream=stream.cuda_stream)
+        torch.cuda.synchronize(device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.step_graph(steps, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize(device)
+        return work * steps / (e0.elapsed_time(e1) / 1000.0)
+    finally:
+        for job in jobs:
+            job.destroy()
+        eng.close()
 
 
 def served_requests(n_requests: int = 2000, seed: int = 5, ppc_scale: float = 1.0, steps_scale: float = 1.0,
