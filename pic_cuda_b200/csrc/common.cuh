@@ -14,6 +14,7 @@
 //       levels (f32).
 #pragma once
 #include <cstdint>
+#include <cuda.h>            // CUtensorMap (the type only; nothing of the driver API is linked)
 #include <cuda_runtime.h>
 #include "pic_b200.h"
 
@@ -72,6 +73,10 @@ struct JobDev {
   int nx, ny, ncx, ncy;   // nodes and cells
   int levels, lc;         // multigrid levels; first level solved by the coarse kernel
   int nl[PIC_MAX_LEVELS]; // level sizes (square)
+  int pl[PIC_MAX_LEVELS]; // row pitch (floats) of level l's FP32 arrays e, f, eu (and f0b):
+                          // nl rounded up to a multiple of 4, so every row starts 16-byte
+                          // aligned (the tensor-map tile loads of the multigrid kernels)
+  const CUtensorMap* tmaps;  // per level l: mgt::kTmapsPerLevel tensor maps (mg_tiles.h)
   float* e[PIC_MAX_LEVELS];   // down leg: pre-smoothed correction (coarse solver output at lc)
   float* f[PIC_MAX_LEVELS];
   // Up-leg outputs go to separate arrays: an up kernel reads its level's e and f with halos

@@ -20,6 +20,7 @@
 #include "../../include/pic_b200.h"
 #include "common.cuh"
 #include "kernels.h"
+#include "mg_tiles.h"
 
 namespace {
 
@@ -206,9 +207,11 @@ Layout job_layout(const pic_job_config& c, int cluster_C = 0, int cluster_top = 
   L.ntiles0 = ((c.nx + 31) / 32) * ((c.ny + 31) / 32);
   const int64_t N = (int64_t)c.nx * c.ny;
   int64_t b = N * ((c.deposit_mode == PIC_DEPOSIT_I64 ? 8 : 4) + 8 + 16 + (c.mg_warm_start ? 8 : 0));
-  for (int l = 0; l < L.levels; ++l) b += 8ll * L.nl[l] * L.nl[l];
-  for (int l = 1; l < L.levels; ++l) b += 4ll * L.nl[l] * L.nl[l];   // up-leg corrections
-  b += 4 * N;                                                         // second level-0 rhs
+  // level arrays at a row pitch rounded up to 4 floats; the tile tensor maps
+  for (int l = 0; l < L.levels; ++l) b += 8ll * mgt::round4(L.nl[l]) * L.nl[l];
+  for (int l = 1; l < L.levels; ++l) b += 4ll * mgt::round4(L.nl[l]) * L.nl[l];   // up-leg corrections
+  b += 4ll * mgt::round4(c.nx) * c.ny;                                           // second level-0 rhs
+  b += (int64_t)sizeof(CUtensorMap) * mgt::kTmapsPerLevel * L.levels;
   b += 24ll * L.ntiles0;
   const int64_t ncells = (int64_t)(c.nx - 1) * (c.ny - 1) + 1;
   for (int s = 0; s < c.n_species; ++s) {
@@ -314,6 +317,75 @@ EngineLaunch make_launch(pic_engine* E, const uint8_t* active) {
   L.gbar = reinterpret_cast<unsigned*>(E->d_running + 2);  // the grid barrier's arrival counter
   L.absorbed = E->d_aux + 4 * kMaxJobs * kSlotsPerJob;
   return L;
+}
+
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point (the library
+// links only the CUDA runtime).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// A 2-D FP32 tensor map of an n x n level array with row pitch `pitch` floats, box bw x bh;
+// elements outside the n x n nodes (the pitch padding included) read as zero.
+int encode_level_map(CUtensorMap* m, const float* base, int n, int pitch, int bw, int bh) {
+  EncodeTiledFn fn = encode_tiled();
+  if (!fn) return fail(PIC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(PIC_ERR_CUDA, "cuTensorMapEncodeTiled rejected a multigrid tile map");
+  return PIC_OK;
+}
+
+// The tile tensor maps of every level the tile kernels process (levels above the coarse
+// solver's; mg_tiles.h lists them), copied to `dst` on the device.  Sweep counts above the
+// compile-time shapes run on the generic kernels, which read global memory directly.
+int make_tile_maps(const JobDev& D, int nu_pre, int nu_post, CUtensorMap* dst) {
+  std::vector<CUtensorMap> maps((size_t)mgt::kTmapsPerLevel * D.levels);
+  std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+  int rc = PIC_OK;
+  for (int l = 0; l < D.lc && !rc; ++l) {
+    CUtensorMap* m = maps.data() + (size_t)mgt::kTmapsPerLevel * l;
+    const int n = D.nl[l], p = D.pl[l];
+    if (nu_pre <= 4) {
+      const int bw = mgt::down_bw(nu_pre), bh = mgt::down_w(nu_pre);
+      rc = encode_level_map(m + mgt::kMapDownF, D.f[l], n, p, bw, bh);
+      if (!rc && l == 0) rc = encode_level_map(m + mgt::kMapDownF0b, D.f0b, n, p, bw, bh);
+    }
+    if (!rc && nu_post <= 4) {
+      const int x = l == 0 ? 1 : 0;
+      const int bw = mgt::up_bw(nu_post, x), bh = mgt::up_w(nu_post, x);
+      rc = encode_level_map(m + mgt::kMapUpE, D.e[l], n, p, bw, bh);
+      if (!rc) rc = encode_level_map(m + mgt::kMapUpF, D.f[l], n, p, bw, bh);
+      if (!rc && l == 0) rc = encode_level_map(m + mgt::kMapUpF0b, D.f0b, n, p, bw, bh);
+      if (!rc) {
+        const float* ec = l + 1 == D.lc ? D.e[l + 1] : D.eu[l + 1];
+        rc = encode_level_map(m + mgt::kMapUpC, ec, D.nl[l + 1], D.pl[l + 1], mgt::up_cbw(nu_post, x),
+                              mgt::up_cw(nu_post, x));
+      }
+    }
+  }
+  if (rc) return rc;
+  CK(cudaMemcpy(dst, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+  return PIC_OK;
 }
 
 int dev_alloc(pic_engine* E, JobHost& J, void** p, size_t bytes) {
@@ -905,7 +977,7 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   const pic_job_config& c = *cfg;
   D.nx = c.nx; D.ny = c.ny; D.ncx = c.nx - 1; D.ncy = c.ny - 1;
   D.levels = lay.levels; D.lc = lay.lc;
-  for (int l = 0; l < lay.levels; ++l) D.nl[l] = lay.nl[l];
+  for (int l = 0; l < lay.levels; ++l) { D.nl[l] = lay.nl[l]; D.pl[l] = mgt::round4(lay.nl[l]); }
   const double dx = c.Lx / (c.nx - 1), dy = c.Ly / (c.ny - 1);
   D.h = dx;
   D.dt = (float)c.dt;
@@ -941,11 +1013,19 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   if (c.mg_warm_start) ALLOC(D.phi64[2], N * 8);
   D.warm_start = c.mg_warm_start;
   for (int l = 0; l < lay.levels; ++l) {
-    ALLOC(D.e[l], 4ll * lay.nl[l] * lay.nl[l]);
-    ALLOC(D.f[l], 4ll * lay.nl[l] * lay.nl[l]);
-    if (l > 0) ALLOC(D.eu[l], 4ll * lay.nl[l] * lay.nl[l]);
+    ALLOC(D.e[l], 4ll * D.pl[l] * lay.nl[l]);
+    ALLOC(D.f[l], 4ll * D.pl[l] * lay.nl[l]);
+    if (l > 0) ALLOC(D.eu[l], 4ll * D.pl[l] * lay.nl[l]);
   }
-  ALLOC(D.f0b, N * 4);
+  ALLOC(D.f0b, 4ll * D.pl[0] * c.ny);
+  {
+    CUtensorMap* tm = nullptr;
+    ALLOC(tm, sizeof(CUtensorMap) * mgt::kTmapsPerLevel * lay.levels);
+    CK(cudaStreamSynchronize(E->stream));   // the pool allocations above have completed
+    const int rc = make_tile_maps(D, c.nu_pre, c.nu_post, tm);
+    if (rc) { free_job(E, J); return rc; }
+    D.tmaps = tm;
+  }
   ALLOC(D.partials, 24ll * lay.ntiles0);   // per level-0 tile: r^2, F^2 (pairs), then charge
   if (c.n_walls > 0) {
     std::vector<double> w(4 * c.n_walls);
@@ -1099,11 +1179,11 @@ int pic_job_create(pic_engine* E, const pic_job_config* cfg, int* job_id) {
   if (D.rho_f) CK(cudaMemset(D.rho_f, 0, N * 4));
   if (D.rho_i) CK(cudaMemset(D.rho_i, 0, N * 8));
   for (int l = 0; l < lay.levels; ++l) {
-    CK(cudaMemset(D.e[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
-    CK(cudaMemset(D.f[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
-    if (D.eu[l]) CK(cudaMemset(D.eu[l], 0, 4ll * lay.nl[l] * lay.nl[l]));
+    CK(cudaMemset(D.e[l], 0, 4ll * D.pl[l] * lay.nl[l]));
+    CK(cudaMemset(D.f[l], 0, 4ll * D.pl[l] * lay.nl[l]));
+    if (D.eu[l]) CK(cudaMemset(D.eu[l], 0, 4ll * D.pl[l] * lay.nl[l]));
   }
-  CK(cudaMemset(D.f0b, 0, N * 4));
+  CK(cudaMemset(D.f0b, 0, 4ll * D.pl[0] * c.ny));
   CK(cudaMemcpy(E->d_jobs + id, &D, sizeof(JobDev), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(E->d_slots + id * kSlotsPerJob, J.slot, sizeof(SlotDev) * kSlotsPerJob, cudaMemcpyHostToDevice));
   CK(cudaMemset(E->d_st + id, 0, sizeof(JobState)));

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) mg_cluster_kernel(const in
     for (int j = j0 + warp; j < j1; j += nwarp) {
       float* fr = row_ptr(cl, X, v, j, true);
       float* er = row_ptr(cl, X, v, j, false);
-      for (int i = lane; i < v.n; i += 32) { fr[i] = __ldg(fg + (size_t)j * v.n + i); er[i] = 0.f; }
+      for (int i = lane; i < v.n; i += 32) { fr[i] = __ldg(fg + (size_t)j * J.pl[lc] + i); er[i] = 0.f; }
     }
   }
   cl.sync();
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) mg_cluster_kernel(const in
     float* eg = J.e[lc];
     for (int j = j0 + warp; j < j1; j += nwarp) {
       const float* er = row_ptr(cl, X, v, j, false);
-      for (int i = lane; i < v.n; i += 32) eg[(size_t)j * v.n + i] = er[i];
+      for (int i = lane; i < v.n; i += 32) eg[(size_t)j * J.pl[lc] + i] = er[i];
     }
   }
   cl.sync();  // no CTA leaves while another may still read its shared memory

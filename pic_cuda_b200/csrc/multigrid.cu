@@ -22,13 +22,14 @@
 #include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
+#include "mg_tiles.h"
 #include "tma.cuh"
 
 namespace {
 
 constexpr int kTI = 32;   // level-0 residual / update tile
-constexpr int kTC = 16;   // down-leg coarse tile
-constexpr int kTU = 32;   // up-leg fine tile
+constexpr int kTC = mgt::kTC;   // down-leg coarse tile
+constexpr int kTU = mgt::kTU;   // up-leg fine tile
 
 // The charge grid of a job, copied to registers (see mg_up_kernel).
 struct RhoSrc {
@@ -113,6 +114,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   const double* __restrict__ pp = hist ? J.phi64[prev] : phi;
   double* guess = xs ? J.phi64[tgt] : nullptr;
   float* const f0 = T.fsel ? J.f0b : J.f[0];
+  const int pl0 = J.pl[0];
   const double a = hist ? 2.0 : 1.0, b = hist ? 1.0 : 0.0;
   const double inv_h2 = 1.0 / (J.h * J.h);
   const double rhs_scale = J.rhs_scale;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
       r = F - lap;
     }
     if (xs) guess[c] = g0;
-    f0[c] = (float)r;
+    f0[j * pl0 + i] = (float)r;
     ar += r * r;
     af += F * F;
     aq += rv;
@@ -260,7 +262,7 @@ __device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict
                           const JobState* __restrict__ st, int l, float* sm) {
   const JobDev& J = jobs[tr.job];
   if (st[tr.job].converged) return;
-  const int nf = J.nl[l], nc = J.nl[l + 1];
+  const int nf = J.nl[l], nc = J.nl[l + 1], pf = J.pl[l], pc = J.pl[l + 1];
   const double hl = J.h * (double)(1 << l);
   const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
   const int nu = J.nu_pre, H = 2 * nu;
@@ -281,7 +283,7 @@ __device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict
     const bool rowin = gy >= 0 && gy < nf;
     for (int lx = lane; lx < W; lx += 32) {
       const int gx = gx0 + lx;
-      f[ly * W + lx] = (rowin && gx >= 0 && gx < nf) ? __ldg(fg + (size_t)gy * nf + gx) : 0.f;
+      f[ly * W + lx] = (rowin && gx >= 0 && gx < nf) ? __ldg(fg + (size_t)gy * pf + gx) : 0.f;
       e[ly * W + lx] = 0.f;
     }
   }
@@ -292,7 +294,7 @@ __device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict
     const int gy = 2 * jc0 + oy;
     if (gy >= nf) break;
     const int gx = 2 * ic0 + lane;
-    if (gx < nf) eg[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+    if (gx < nf) eg[(size_t)gy * pf + gx] = e[(gy - gy0) * W + (gx - gx0)];
   }
   // residual + full weighting to the owned coarse nodes
   for (int k = g.rank(); k < kTC * kTC; k += G::kSize) {
@@ -314,7 +316,7 @@ __device__ void down_tile(const G& g, const TileRef tr, const JobDev* __restrict
                       r[0][0] + r[0][2] + r[2][0] + r[2][2];
       v = s * 0.0625f;
     }
-    fc[(size_t)jc * nc + ic] = v;
+    fc[(size_t)jc * pc + ic] = v;
   }
   g.sync();  // the tile's shared memory is free for the group's next tile
 }
@@ -473,7 +475,7 @@ __host__ __device__ inline size_t coarse_layout_bytes(const int* nl, int lc, int
 // while n^2 < 2^21: k + 0.5 is representable, and the product's rounding error
 // (< n 2^-22) stays below the fraction's distance from an integer (>= 0.5 / n).
 constexpr int kCoarseBatch = 5;
-__device__ __forceinline__ void coarse_load(float* dst, const float* __restrict__ src, int n) {
+__device__ __forceinline__ void coarse_load(float* dst, const float* __restrict__ src, int n, int pitch) {
   const int N = n * n, T = blockDim.x;
   const float inv_n = 1.f / (float)n;
   for (int k0 = 0; k0 < N; k0 += kCoarseBatch * T) {
@@ -481,7 +483,8 @@ __device__ __forceinline__ void coarse_load(float* dst, const float* __restrict_
 #pragma unroll
     for (int u = 0; u < kCoarseBatch; ++u) {
       const int k = k0 + (int)threadIdx.x + u * T;
-      v[u] = k < N ? __ldg(src + k) : 0.f;
+      const int j = (int)(((float)k + 0.5f) * inv_n);
+      v[u] = k < N ? __ldg(src + j * pitch + (k - j * n)) : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < kCoarseBatch; ++u) {
@@ -493,12 +496,12 @@ __device__ __forceinline__ void coarse_load(float* dst, const float* __restrict_
     }
   }
 }
-__device__ __forceinline__ void coarse_store(float* __restrict__ dst, const float* src, int n) {
+__device__ __forceinline__ void coarse_store(float* __restrict__ dst, const float* src, int n, int pitch) {
   const int N = n * n;
   const float inv_n = 1.f / (float)n;
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
     const int j = (int)(((float)k + 0.5f) * inv_n);
-    dst[k] = src[j * (n + 1) + (k - j * n)];
+    dst[j * pitch + (k - j * n)] = src[j * (n + 1) + (k - j * n)];
   }
 }
 
@@ -513,6 +516,7 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   const float omega = J.omega;
   const int nu_pre = J.nu_pre, nu_post = J.nu_post, nu_coarse = J.nu_coarse;
   float* const e_top = J.e[lc];
+  const int p_top = J.pl[lc];
   const float* const f_top = (lc == 0 && st[job].fsel) ? J.f0b : J.f[lc];
   __shared__ CoarseLevel lv[PIC_MAX_LEVELS];
   __shared__ int total;
@@ -538,7 +542,7 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
   for (int k = t; k < total / 4; k += T) reinterpret_cast<float4*>(sm)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
   tma::pdl_wait();
-  coarse_load(sm + lv[lc].off + lv[lc].n * (lv[lc].n + 1), f_top, lv[lc].n);
+  coarse_load(sm + lv[lc].off + lv[lc].n * (lv[lc].n + 1), f_top, lv[lc].n, p_top);
   __syncthreads();
   int l = lc;
   for (; l < L - 1 && lv[l].n > kCoarseSmallSide; ++l) {
@@ -567,7 +571,7 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
     level_prolong<false>(sm, lv[k], lv[k + 1], t, T);
     level_sweeps<false>(sm, lv[k], omega, nu_post, t, T);
   }
-  coarse_store(e_top, sm + lv[lc].off, lv[lc].n);
+  coarse_store(e_top, sm + lv[lc].off, lv[lc].n, p_top);
   __syncthreads();  // shared memory is free for the CTA's next job
 }
 
@@ -587,7 +591,7 @@ __device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__
                         int l, float* sm) {
   const JobDev& J = jobs[tr.job];
   if (st[tr.job].converged) return;
-  const int nf = J.nl[l];
+  const int nf = J.nl[l], pf = J.pl[l];
   const double hl = J.h * (double)(1 << l);
   const float h2 = (float)(hl * hl);
   const int nu = J.nu_post, H = 2 * nu;
@@ -598,7 +602,7 @@ __device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__
   float* f = sm + W * W;
   const float* eg = J.e[l];
   const float* fg = J.f[l];
-  const int nc = J.nl[l + 1];
+  const int pc = J.pl[l + 1];
   const float* ec = l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1];
   const float omega = J.omega;
   float* const eo = J.eu[l];
@@ -610,15 +614,15 @@ __device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__
       const int gx = gx0 + lx, gy = gy0 + ly;
       float ev = 0.f, fv = 0.f;
       if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) {
-        const size_t gi = (size_t)gy * nf + gx;
+        const size_t gi = (size_t)gy * pf + gx;
         ev = __ldg(eg + gi);
         fv = __ldg(fg + gi);
-        const float* cp = ec + (size_t)(gy >> 1) * nc + (gx >> 1);
+        const float* cp = ec + (size_t)(gy >> 1) * pc + (gx >> 1);
         const bool io = gx & 1, jo = gy & 1;
         const float c00 = __ldg(cp);
         const float c10 = io ? __ldg(cp + 1) : 0.f;
-        const float c01 = jo ? __ldg(cp + nc) : 0.f;
-        const float c11 = (io && jo) ? __ldg(cp + nc + 1) : 0.f;
+        const float c01 = jo ? __ldg(cp + pc) : 0.f;
+        const float c11 = (io && jo) ? __ldg(cp + pc + 1) : 0.f;
         float v;
         if (!io && !jo) v = c00;
         else if (io && !jo) v = 0.5f * (c00 + c10);
@@ -633,7 +637,7 @@ __device__ void up_tile(const G& g, const TileRef tr, const JobDev* __restrict__
   if (nu > 0) tile_sweeps(g, e, f, W, gx0, gy0, nf, h2, omega, nu);
   for (int oy = warp; oy < kTU; oy += 8) {
     const int gy = j0 + oy, gx = i0 + lane;
-    if (gy < nf && gx < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+    if (gy < nf && gx < nf) eo[(size_t)gy * pf + gx] = e[(gy - gy0) * W + (gx - gx0)];
   }
   g.sync();  // the tile's shared memory is free for the group's next tile
 }
@@ -647,7 +651,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
   if (T.converged) return;
-  const int nf = J.nl[l];
+  const int nf = J.nl[l], pf = J.pl[l];
   const double hl = J.h * (double)(1 << l);
   const float h2 = (float)(hl * hl);
   const int nu = mode == 2 ? 0 : J.nu_post, H = 2 * nu, X = (l == 0) ? 1 : 0;
@@ -660,7 +664,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   const float* eg = J.e[l];
   const float* fg = (l == 0 && fsel) ? J.f0b : J.f[l];
   const bool prolong = mode != 2;
-  const int nc = prolong ? J.nl[l + 1] : 0;
+  const int pcs = prolong ? J.pl[l + 1] : 0;
   // the coarser correction: the coarse solver's output at lc, else the up kernel's of l + 1
   const float* ec = prolong ? (l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1]) : nullptr;
   // everything else the kernel needs from the job, read before the first barrier (after it,
@@ -685,17 +689,17 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
     const int gx = gx0 + lx, gy = gy0 + ly;
     float ev = 0.f, fv = 0.f;
     if (gx >= 0 && gx < nf && gy >= 0 && gy < nf) {
-      const size_t g = (size_t)gy * nf + gx;
+      const size_t g = (size_t)gy * pf + gx;
       ev = __ldg(eg + g);
       fv = __ldg(fg + g);
       if (prolong) {
         // bilinear prolongation (Multigrid.cu:378-404) as weights on the 2x2 coarse block
-        const float* cp = ec + (size_t)(gy >> 1) * nc + (gx >> 1);
+        const float* cp = ec + (size_t)(gy >> 1) * pcs + (gx >> 1);
         const bool io = gx & 1, jo = gy & 1;
         const float c00 = __ldg(cp);
         const float c10 = io ? __ldg(cp + 1) : 0.f;
-        const float c01 = jo ? __ldg(cp + nc) : 0.f;
-        const float c11 = (io && jo) ? __ldg(cp + nc + 1) : 0.f;
+        const float c01 = jo ? __ldg(cp + pcs) : 0.f;
+        const float c11 = (io && jo) ? __ldg(cp + pcs + 1) : 0.f;
         float v;
         if (!io && !jo) v = c00;
         else if (io && !jo) v = 0.5f * (c00 + c10);
@@ -712,7 +716,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
   if (mode == 0) {
     for (int oy = warp; oy < kTU; oy += 8) {
       const int gy = j0 + oy, gx = i0 + lane;
-      if (gy < nf && gx < nf) eo[(size_t)gy * nf + gx] = e[(gy - gy0) * W + (gx - gx0)];
+      if (gy < nf && gx < nf) eo[(size_t)gy * pf + gx] = e[(gy - gy0) * W + (gx - gx0)];
     }
     return;
   }
@@ -741,7 +745,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(const TileRef* __restrict__ 
       r = F - lap;
     }
     pn[g] = P[q];
-    f0[g] = (float)r;
+    f0[(size_t)gy * pf + gx] = (float)r;
     ar += r * r;
   }
   const double sr = block_sum(ar);
@@ -815,54 +819,68 @@ __device__ __forceinline__ void tile_sweeps_cols(float* e, const float* f, int g
     }
 }
 
+// The tile loads of a fast kernel: thread 0 arms the CTA's mbarrier with the bytes of every
+// box and issues the tensor-map loads; every thread then waits for the phase (bounded).  A
+// wait that runs out flags PIC_ST_TIMEOUT on the job, waits once more for the copies in
+// flight and reports false, and the CTA leaves.
+__device__ __forceinline__ bool tiles_arrived(uint64_t* mbar, JobState* T) {
+  const bool ok = __syncthreads_and(tma::mbar_wait(mbar, 0) ? 1 : 0) != 0;
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&T->status, PIC_ST_TIMEOUT);
+    tma::mbar_wait(mbar, 0);
+  }
+  return ok;
+}
+
 // Down leg of level l (as mg_down_kernel): NU pre-sweeps from a zero correction on the tile
 // of 16 x 16 coarse nodes, the smoothed fine nodes it owns to e_l, the full-weighted
-// residual to f_{l+1}.
+// residual to f_{l+1}.  The right-hand side tile arrives by one tensor-map load.
 template <int NU, int NT>
 __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restrict__ tiles,
                                                           const JobDev* __restrict__ jobs,
                                                           const JobState* __restrict__ st, int l) {
-  constexpr int H = 2 * NU, W = 2 * kTC + 3 + 2 * H, P = W + 1;
-  constexpr int NL = (W * W + NT - 1) / NT;
-  __shared__ __align__(16) float e[W * P];
-  __shared__ __align__(16) float f[W * P];
+  constexpr int H = 2 * NU, W = mgt::down_w(NU), OFF = mgt::down_off(NU), P = mgt::down_bw(NU);
+  static_assert(W == 2 * kTC + 3 + 2 * H, "tile shape");
+  __shared__ __align__(128) float es[W * P];
+  __shared__ __align__(128) float fs[W * P];
+  __shared__ __align__(8) uint64_t mbar;
+  float* const e = es + OFF;
+  float* const f = fs + OFF;
   tma::pdl_trigger();
   // tile, job and job-state fields: none of them is written by the previous level's launch
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   const JobState& T = st[tr.job];
   if (T.converged) return;
-  const int nf = J.nl[l], nc = J.nl[l + 1];
+  const int nf = J.nl[l], nc = J.nl[l + 1], pf = J.pl[l], pc = J.pl[l + 1];
   const double hl = J.h * (double)(1 << l);
   const float h2 = (float)(hl * hl), inv_h2 = (float)(1.0 / (hl * hl));
   const int ic0 = tr.ti * kTC, jc0 = tr.tj * kTC;
   const int gx0 = 2 * ic0 - 2 - H, gy0 = 2 * jc0 - 2 - H;
-  const float* __restrict__ fg = (l == 0 && T.fsel) ? J.f0b : J.f[l];
+  const void* map = J.tmaps + mgt::kTmapsPerLevel * l + ((l == 0 && T.fsel) ? mgt::kMapDownF0b : mgt::kMapDownF);
   float* const eg = J.e[l];
   float* const fc = J.f[l + 1];
   const float omega = J.omega;
   const int t = threadIdx.x;
-  tma::pdl_wait();
-#pragma unroll
-  for (int u = 0; u < NL; ++u) {
-    const int q = t + u * NT;
-    if (q < W * W) {
-      const int ly = q / W, lx = q - ly * W;
-      const int gx = gx0 + lx, gy = gy0 + ly;
-      const bool in = (unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf;
-      tma::cp_async4(f + ly * P + lx, fg + (in ? gy * nf + gx : 0), in);
-      e[ly * P + lx] = 0.f;
-    }
+  if (t == 0) {
+    tma::mbar_init(&mbar, 1);
+    tma::fence_mbar_init();
   }
-  tma::cp_async_wait_all();
+  for (int q = t; q < W * P; q += NT) es[q] = 0.f;
   __syncthreads();
+  tma::pdl_wait();
+  if (t == 0) {
+    tma::mbar_arrive_expect_tx(&mbar, W * P * 4);
+    tma::tensor_load_2d(fs, map, gx0 - OFF, gy0, &mbar);
+  }
+  if (!tiles_arrived(&mbar, const_cast<JobState*>(&T))) return;
   tile_sweeps_cols<W, P, NU, NT, true>(e, f, gx0, gy0, nf, h2, omega);
   // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
 #pragma unroll
   for (int u = 0; u < (4 * kTC * kTC) / NT; ++u) {
     const int k = t + u * NT;
     const int gy = 2 * jc0 + (k >> 5), gx = 2 * ic0 + (k & 31);
-    if (gy < nf && gx < nf) eg[gy * nf + gx] = e[(gy - gy0) * P + (gx - gx0)];
+    if (gy < nf && gx < nf) eg[gy * pf + gx] = e[(gy - gy0) * P + (gx - gx0)];
   }
   // residual + full weighting to the owned coarse nodes
   if (t < kTC * kTC) {
@@ -884,7 +902,7 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
                           r[0][2] + r[2][0] + r[2][2];
         vv = sum * 0.0625f;
       }
-      fc[jc * nc + ic] = vv;
+      fc[jc * pc + ic] = vv;
     }
   }
 }
@@ -892,24 +910,29 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
 // Up leg (as mg_up_kernel modes 0 and 1).  MODE 0, level l >= 1: the bilinear prolongation
 // of the coarser correction added to the pre-smoothed one, NU post-sweeps, the owned nodes
 // to eu_l.  MODE 1, level 0 (NT = 256): the same with a one-node halo, then phi <- phi + e in
-// FP64, the new FP64 defect and the deterministic norm.  Every global input of the
-// tile (e, f, the coarse tile, and on level 0 phi64 and rho) is requested in one batch.
+// FP64, the new FP64 defect and the deterministic norm.  The e, f and coarse tiles arrive by
+// tensor-map loads; on level 0 phi64 (with a one-node halo) and rho of the owned nodes come
+// in one batch of asynchronous copies beside them.
 template <int NU, int MODE, int NT>
 __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const TileRef* __restrict__ tiles,
                                                                       const JobDev* __restrict__ jobs,
                                                                       JobState* __restrict__ st, int l, int* running) {
-  constexpr int H = 2 * NU, X = MODE, W = kTU + 2 * H + 2 * X, P = W;
-  constexpr int CW = W / 2 + 2, CP = CW + (CW & 1);
+  constexpr int H = 2 * NU, X = MODE, W = mgt::up_w(NU, X), OFF = mgt::up_off(NU, X), P = mgt::up_bw(NU, X);
+  constexpr int CW = mgt::up_cw(NU, X), COFF = mgt::up_coff(NU, X), CP = mgt::up_cbw(NU, X);
+  static_assert(W == kTU + 2 * H + 2 * X, "tile shape");
   constexpr int PW = kTU + 2;
   constexpr int NL = (W * W + NT - 1) / NT;
-  constexpr int NC = (CW * CW + NT - 1) / NT;
   constexpr int NP = MODE ? (PW * PW + NT - 1) / NT : 0;
   constexpr int NO = kTU * kTU / NT;
-  __shared__ __align__(16) float e[W * P];
-  __shared__ __align__(16) float f[W * P];
-  __shared__ __align__(16) float cs[CW * CP];
+  __shared__ __align__(128) float es[W * P];
+  __shared__ __align__(128) float fs[W * P];
+  __shared__ __align__(128) float css[CW * CP];
   __shared__ __align__(16) double P64[MODE ? PW * PW : 1];
   __shared__ __align__(16) double RH[MODE ? kTU * kTU : 1];   // rho of the owned nodes, raw
+  __shared__ __align__(8) uint64_t mbar;
+  float* const e = es + OFF;
+  float* const f = fs + OFF;
+  const float* const cs = css + COFF;
   tma::pdl_trigger();
   // tile, job and job-state fields: within a V-cycle only this kernel's own last CTA (level 0)
   // writes the state, so they are read before waiting for the previous launch
@@ -917,17 +940,17 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
   if (T.converged) return;
-  const int nf = J.nl[l];
+  const int nf = J.nl[l], pf = J.pl[l];
   const double hl = J.h * (double)(1 << l);
   const float h2 = (float)(hl * hl);
   const int i0 = tr.ti * kTU, j0 = tr.tj * kTU;
   const int gx0 = i0 - H - X, gy0 = j0 - H - X;
   const int cx0 = gx0 >> 1, cy0 = gy0 >> 1;   // floor, also for negative origins
   const int fsel = T.fsel;
-  const float* __restrict__ eg = J.e[l];
-  const float* __restrict__ fg = (l == 0 && fsel) ? J.f0b : J.f[l];
-  const int nc = J.nl[l + 1];
-  const float* __restrict__ ec = l + 1 == J.lc ? J.e[l + 1] : J.eu[l + 1];
+  const CUtensorMap* maps = J.tmaps + mgt::kTmapsPerLevel * l;
+  const void* map_e = maps + mgt::kMapUpE;
+  const void* map_f = maps + ((l == 0 && fsel) ? mgt::kMapUpF0b : mgt::kMapUpF);
+  const void* map_c = maps + mgt::kMapUpC;
   const float omega = J.omega;
   float* const eo = J.eu[l];
   const int cur = T.phi_cur, nxt = T.phi_nxt;
@@ -941,29 +964,18 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   const double tol = J.tol;
   const int max_cycles = J.max_cycles;
   const int t = threadIdx.x;
-  tma::pdl_wait();
-  // ---- one batch of asynchronous copies
-#pragma unroll
-  for (int u = 0; u < NL; ++u) {
-    const int q = t + u * NT;
-    if (q < W * W) {
-      const int ly = q / W, lx = q - ly * W;
-      const int gx = gx0 + lx, gy = gy0 + ly;
-      const bool in = (unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf;
-      const int gi = in ? gy * nf + gx : 0;
-      tma::cp_async4(e + ly * P + lx, eg + gi, in);
-      tma::cp_async4(f + ly * P + lx, fg + gi, in);
-    }
+  if (t == 0) {
+    tma::mbar_init(&mbar, 1);
+    tma::fence_mbar_init();
   }
-#pragma unroll
-  for (int u = 0; u < NC; ++u) {
-    const int q = t + u * NT;
-    if (q < CW * CW) {
-      const int cy = q / CW, cx = q - cy * CW;
-      const int gx = cx0 + cx, gy = cy0 + cy;
-      const bool in = (unsigned)gx < (unsigned)nc && (unsigned)gy < (unsigned)nc;
-      tma::cp_async4(cs + cy * CP + cx, ec + (in ? gy * nc + gx : 0), in);
-    }
+  __syncthreads();
+  tma::pdl_wait();
+  // ---- the tiles: three tensor-map loads, and on level 0 one batch of asynchronous copies
+  if (t == 0) {
+    tma::mbar_arrive_expect_tx(&mbar, (2 * W * P + CW * CP) * 4);
+    tma::tensor_load_2d(es, map_e, gx0 - OFF, gy0, &mbar);
+    tma::tensor_load_2d(fs, map_f, gx0 - OFF, gy0, &mbar);
+    tma::tensor_load_2d(css, map_c, cx0 - COFF, cy0, &mbar);
   }
   if constexpr (MODE == 1) {
 #pragma unroll
@@ -986,9 +998,9 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
       else if (rho.mode == 1) tma::cp_async8(RH + k, rho.i + g, in);
       else tma::cp_async8(RH + k, rho.d + g, in);
     }
+    tma::cp_async_wait_all();
   }
-  tma::cp_async_wait_all();
-  __syncthreads();
+  if (!tiles_arrived(&mbar, &T)) return;
   // ---- bilinear prolongation added to the pre-smoothed correction
 #pragma unroll
   for (int u = 0; u < NL; ++u) {
@@ -1009,7 +1021,7 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
     for (int u = 0; u < NO; ++u) {
       const int k = t + u * NT;
       const int gx = i0 + (k & 31), gy = j0 + (k >> 5);
-      if (gy < nf && gx < nf) eo[gy * nf + gx] = e[(gy - gy0) * P + (gx - gx0)];
+      if (gy < nf && gx < nf) eo[gy * pf + gx] = e[(gy - gy0) * P + (gx - gx0)];
     }
     return;
   } else {
@@ -1043,7 +1055,7 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
         r = F - lap;
       }
       pn[g] = P64[q];
-      f0[g] = (float)r;
+      f0[gy * pf + gx] = (float)r;
       ar += r * r;
     }
     const double sr = block_sum(ar);

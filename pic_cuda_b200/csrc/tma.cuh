@@ -51,6 +51,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
+// 2-D tensor-map tile load (cp.async.bulk.tensor, tile mode, this CTA only) of the box whose
+// first element is at column x (a multiple of 16 bytes) and row y of the map's tensor,
+// completing on mbarrier m.  Columns and rows outside the tensor read as zero.
+__device__ __forceinline__ void tensor_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* m) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(smem_addr(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(m))
+      : "memory");
+}
+
 // shared -> global bulk copy in the calling thread's bulk async-group.
 __device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
