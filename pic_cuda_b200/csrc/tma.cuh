@@ -1,7 +1,8 @@
-// tma.cuh — bulk asynchronous copies (cp.async.bulk, the 1-D form of the Tensor Memory
-// Accelerator), per-thread cp.async copies and mbarrier helpers, inline PTX for sm_100a.
-// No multicast form is used anywhere.  Every wait is bounded: after kMaxPolls unsuccessful
-// polls it gives up and reports false, so a kernel can flag PIC_ST_TIMEOUT and leave.
+// tma.cuh — Tensor Memory Accelerator tile loads (cp.async.bulk.tensor with a tensor map,
+// completing on an mbarrier), per-thread cp.async copies, mbarrier helpers and programmatic
+// dependent launch, inline PTX for sm_100a.  No multicast form is used anywhere.  Every wait
+// is bounded: after kMaxPolls unsuccessful polls it gives up and reports false, so a kernel
+// can flag PIC_ST_TIMEOUT and leave.
 #pragma once
 #include <cstdint>
 
@@ -43,14 +44,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* m, uint32_t parity) {
   return false;
 }
 
-// global -> shared bulk copy completing on mbarrier m (16-byte aligned, bytes % 16 == 0).
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_addr(dst)),
-               "l"(src), "r"(bytes), "r"(smem_addr(m))
-               : "memory");
-}
-
 // 2-D tensor-map tile load (cp.async.bulk.tensor, tile mode, this CTA only) of the box whose
 // first element is at column x (a multiple of 16 bytes) and row y of the map's tensor,
 // completing on mbarrier m.  Columns and rows outside the tensor read as zero.
@@ -61,21 +54,6 @@ __device__ __forceinline__ void tensor_load_2d(void* dst, const void* tmap, int 
       "l"(tmap), "r"(x), "r"(y), "r"(smem_addr(m))
       : "memory");
 }
-
-// shared -> global bulk copy in the calling thread's bulk async-group.
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// Wait until the sources (shared memory) of all committed bulk stores have been read.
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// Wait until all committed bulk stores are complete.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// Make this thread's generic-proxy shared-memory writes visible to the async proxy.
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Per-thread asynchronous global -> shared copy of 4 or 8 bytes (cp.async): nothing is held
 // in registers while the copy is in flight.  valid = false reads no global memory and writes
