@@ -365,9 +365,8 @@ def run_ours(args):
     traffic = None
     tf = ROOT / "profiles" / "mover_traffic.json"
     if tf.exists():
-        t = json.loads(tf.read_text())
-        t = t.get(args.workload, t) if isinstance(t, dict) else t
-        if "bytes_per_particle" in t:
+        t = json.loads(tf.read_text()).get(args.workload)
+        if t and "bytes_per_particle" in t:
             traffic = t["bytes_per_particle"] * particles
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "mover_kernel (fused kick/MCC/drift/walls/deposit)",
