@@ -236,6 +236,127 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
   }
 }
 
+// ---- band pass (particles in arbitrary order, e.g. freshly loaded)
+// A counting sort of randomly ordered particles scatters every 4-byte field to a random place:
+// each store touches its own 32-byte sector.  Before the cell sort such particles are first
+// grouped into kBands bands of cell rows: each CTA orders a chunk of kBandChunk particles by
+// band in shared memory and writes each band's run to consecutive places, so the scatter
+// writes runs; the cell sort that follows then writes inside one band's range at a time.
+constexpr int kBands = 64;
+constexpr int kBandThreads = 256;
+constexpr int kBandChunk = 1024;   // particles per CTA chunk (4 per thread)
+
+// band of a cell key: rows split into nb bands; particles outside the grid go last
+__device__ __forceinline__ int band_of(uint32_t c, int ncy, int nb) {
+  return c == PIC_CELL_OUT ? nb : (int)(((uint32_t)cell_j(c) * (uint32_t)nb) / (uint32_t)ncy);
+}
+__device__ __forceinline__ int bands_of(const JobDev& J) { return min(kBands, J.ncy); }
+
+// Band counts (cell_count[0 .. nb]) and, after sort_band_scan, band cursors
+// (cell_count[nb + 1 .. 2 nb + 1]); cell_count holds ncx ncy + 1 >= 2 (nb + 1) entries.
+__global__ void __launch_bounds__(kBandThreads) sort_band_hist(const JobDev* jobs, const SlotDev* slots,
+                                                               const int* counts, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int n = counts[s], nb = bands_of(J), ncy = J.ncy;
+  __shared__ int h[kBands + 1];
+  for (int b = threadIdx.x; b <= nb; b += blockDim.x) h[b] = 0;
+  __syncthreads();
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
+    atomicAdd(&h[band_of(S.cell[p], ncy, nb)], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b <= nb; b += blockDim.x)
+    if (h[b]) atomicAdd(S.cell_count + b, h[b]);
+}
+
+__global__ void sort_band_zero(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+  const int s = blockIdx.x;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const int nb = bands_of(jobs[S.job]);
+  for (int b = threadIdx.x; b < 2 * (nb + 1); b += blockDim.x) S.cell_count[b] = 0;
+}
+
+// exclusive scan of the band counts into the cursors (one thread per slot: nb + 1 <= 65)
+__global__ void sort_band_scan(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !mask[s]) return;
+  const SlotDev& S = slots[s];
+  const int nb = bands_of(jobs[S.job]);
+  int a = 0;
+  for (int b = 0; b <= nb; ++b) {
+    const int c = S.cell_count[b];
+    S.cell_count[nb + 1 + b] = a;
+    a += c;
+  }
+}
+
+// Each CTA: chunks of kBandChunk particles ordered by band in shared memory (the order inside
+// a band is the atomics'), one cursor atomic per band present, then consecutive stores.
+__global__ void __launch_bounds__(kBandThreads) sort_band_scatter(const JobDev* jobs, const SlotDev* slots,
+                                                                  const int* counts, const uint8_t* mask) {
+  const int s = blockIdx.y;
+  if (!mask[s]) return;
+  const SlotDev& S = slots[s];
+  const JobDev& J = jobs[S.job];
+  const int n = counts[s], nb = bands_of(J), ncy = J.ncy;
+  int* const cursor = S.cell_count + nb + 1;
+  __shared__ int h[kBands + 1], off[kBands + 1], base[kBands + 1], fill[kBands + 1];
+  __shared__ uint32_t st[7][kBandChunk];
+  __shared__ short bandof[kBandChunk];
+  constexpr int PER = kBandChunk / kBandThreads;
+  const int t = threadIdx.x;
+  for (int c0 = blockIdx.x * kBandChunk; c0 < n; c0 += gridDim.x * kBandChunk) {
+    const int m = min(kBandChunk, n - c0);
+    for (int b = t; b <= nb; b += kBandThreads) { h[b] = 0; fill[b] = 0; }
+    __syncthreads();
+    int bb[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int k = t + u * kBandThreads;
+      bb[u] = k < m ? band_of(S.cell[c0 + k], ncy, nb) : -1;
+      if (bb[u] >= 0) atomicAdd(&h[bb[u]], 1);
+    }
+    __syncthreads();
+    if (t == 0) {
+      int a = 0;
+      for (int b = 0; b <= nb; ++b) { off[b] = a; a += h[b]; }
+    }
+    __syncthreads();
+    for (int b = t; b <= nb; b += kBandThreads) base[b] = h[b] ? atomicAdd(cursor + b, h[b]) : 0;
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int k = t + u * kBandThreads;
+      if (bb[u] < 0) continue;
+      const int r = off[bb[u]] + atomicAdd(&fill[bb[u]], 1);
+      const int p = c0 + k;
+      st[0][r] = S.cell[p];
+      st[1][r] = __float_as_uint(S.fx[p]);
+      st[2][r] = __float_as_uint(S.fy[p]);
+      st[3][r] = __float_as_uint(S.vx[p]);
+      st[4][r] = __float_as_uint(S.vy[p]);
+      st[5][r] = __float_as_uint(S.vz[p]);
+      st[6][r] = S.pid[p];
+      bandof[r] = (short)bb[u];
+    }
+    __syncthreads();
+    for (int r = t; r < m; r += kBandThreads) {
+      const int b = bandof[r];
+      const int d = base[b] + (r - off[b]);
+      S.cell_b[d] = st[0][r];
+      S.fx_b[d] = __uint_as_float(st[1][r]);
+      S.fy_b[d] = __uint_as_float(st[2][r]);
+      S.vx_b[d] = __uint_as_float(st[3][r]);
+      S.vy_b[d] = __uint_as_float(st[4][r]);
+      S.vz_b[d] = __uint_as_float(st[5][r]);
+      S.pid_b[d] = st[6][r];
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void swp(T*& a, T*& b) { T* t = a; a = b; b = t; }
 
@@ -267,8 +388,22 @@ int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, int offset, cudaStrea
   return 1;
 }
 
-int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
+int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, bool banded,
+                cudaStream_t st) {
   if (L.nslots == 0) return 0;
+  int k = 0;
+  if (banded) {
+    // particles in arbitrary order: group them into bands of rows first (into the second
+    // array set), then the cell sort below runs on the band-ordered arrays
+    const int gb = std::min(std::max((max_particles + kBandChunk - 1) / kBandChunk, 1), 2 * L.num_sms);
+    const int gh = std::min(std::max((max_particles + 255) / 256, 1), 4 * L.num_sms);
+    sort_band_zero<<<L.nslots, 256, 0, st>>>(L.jobs, L.slots, mask);
+    sort_band_hist<<<dim3(gh, L.nslots), kBandThreads, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+    sort_band_scan<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.jobs, L.slots, mask, L.nslots);
+    sort_band_scatter<<<dim3(gb, L.nslots), kBandThreads, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+    sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
+    k += 5;
+  }
   const int ncells = max_cells + 1;
   const int ntiles = (ncells + kTile - 1) / kTile;
   const int gz = std::min(std::max((ncells + 255) / 256, 1), 4 * L.num_sms);
@@ -280,5 +415,5 @@ int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int m
   sort_apply<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_scatter<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
   sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
-  return 7;
+  return k + 7;
 }
