@@ -213,8 +213,8 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
     for (int r = 0; r < kSortRounds; ++r) {
       const int p = it * kSortItem + 32 * r + lane;
       const int q = p < n ? p : 0;
-      c[r] = __ldg(cell + q); a[r] = __ldg(fx + q); b[r] = __ldg(fy + q);
-      u[r] = __ldg(vx + q); v[r] = __ldg(vy + q); w[r] = __ldg(vz + q); pd[r] = __ldg(pid + q);
+      c[r] = __ldcs(cell + q); a[r] = __ldcs(fx + q); b[r] = __ldcs(fy + q);
+      u[r] = __ldcs(vx + q); v[r] = __ldcs(vy + q); w[r] = __ldcs(vz + q); pd[r] = __ldcs(pid + q);
       key[r] = p < n ? dense_key(c[r], ncx, ncells) : kNoKey;
     }
     int at[kSortRounds];
@@ -240,11 +240,14 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
 // A counting sort of randomly ordered particles scatters every 4-byte field to a random place:
 // each store touches its own 32-byte sector.  Before the cell sort such particles are first
 // grouped into kBands bands of cell rows: each CTA orders a chunk of kBandChunk particles by
-// band in shared memory and writes each band's run to consecutive places, so the scatter
-// writes runs; the cell sort that follows then writes inside one band's range at a time.
-constexpr int kBands = 64;
+// band in shared memory and writes each band's run to consecutive places (~8 particles, a
+// full 32-byte sector per array); the cell sort that follows then writes inside one band's
+// range at a time (a few MB per array, which stays in L2 until its sectors are complete).
+// Both passes read with evict-first loads, so the streamed input does not push the write
+// window out of L2.
+constexpr int kBands = 256;
 constexpr int kBandThreads = 256;
-constexpr int kBandChunk = 1024;   // particles per CTA chunk (4 per thread)
+constexpr int kBandChunk = 2048;   // particles per CTA chunk (8 per thread)
 
 // band of a cell key: rows split into nb bands; particles outside the grid go last
 __device__ __forceinline__ int band_of(uint32_t c, int ncy, int nb) {
@@ -279,7 +282,7 @@ __global__ void sort_band_zero(const JobDev* jobs, const SlotDev* slots, const u
   for (int b = threadIdx.x; b < 2 * (nb + 1); b += blockDim.x) S.cell_count[b] = 0;
 }
 
-// exclusive scan of the band counts into the cursors (one thread per slot: nb + 1 <= 65)
+// exclusive scan of the band counts into the cursors (one thread per slot: nb + 1 <= 257)
 __global__ void sort_band_scan(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask, int nslots) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots || !mask[s]) return;
@@ -304,8 +307,9 @@ __global__ void __launch_bounds__(kBandThreads) sort_band_scatter(const JobDev* 
   const int n = counts[s], nb = bands_of(J), ncy = J.ncy;
   int* const cursor = S.cell_count + nb + 1;
   __shared__ int h[kBands + 1], off[kBands + 1], base[kBands + 1], fill[kBands + 1];
-  __shared__ uint32_t st[7][kBandChunk];
-  __shared__ short bandof[kBandChunk];
+  extern __shared__ __align__(16) uint32_t band_smem[];
+  uint32_t (*st)[kBandChunk] = reinterpret_cast<uint32_t (*)[kBandChunk]>(band_smem);
+  short* const bandof = reinterpret_cast<short*>(band_smem + 7 * kBandChunk);
   constexpr int PER = kBandChunk / kBandThreads;
   const int t = threadIdx.x;
   for (int c0 = blockIdx.x * kBandChunk; c0 < n; c0 += gridDim.x * kBandChunk) {
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(kBandThreads) sort_band_scatter(const JobDev* 
 #pragma unroll
     for (int u = 0; u < PER; ++u) {
       const int k = t + u * kBandThreads;
-      bb[u] = k < m ? band_of(S.cell[c0 + k], ncy, nb) : -1;
+      bb[u] = k < m ? band_of(__ldcs(S.cell + c0 + k), ncy, nb) : -1;
       if (bb[u] >= 0) atomicAdd(&h[bb[u]], 1);
     }
     __syncthreads();
@@ -332,13 +336,13 @@ __global__ void __launch_bounds__(kBandThreads) sort_band_scatter(const JobDev* 
       if (bb[u] < 0) continue;
       const int r = off[bb[u]] + atomicAdd(&fill[bb[u]], 1);
       const int p = c0 + k;
-      st[0][r] = S.cell[p];
-      st[1][r] = __float_as_uint(S.fx[p]);
-      st[2][r] = __float_as_uint(S.fy[p]);
-      st[3][r] = __float_as_uint(S.vx[p]);
-      st[4][r] = __float_as_uint(S.vy[p]);
-      st[5][r] = __float_as_uint(S.vz[p]);
-      st[6][r] = S.pid[p];
+      st[0][r] = __ldcs(S.cell + p);
+      st[1][r] = __float_as_uint(__ldcs(S.fx + p));
+      st[2][r] = __float_as_uint(__ldcs(S.fy + p));
+      st[3][r] = __float_as_uint(__ldcs(S.vx + p));
+      st[4][r] = __float_as_uint(__ldcs(S.vy + p));
+      st[5][r] = __float_as_uint(__ldcs(S.vz + p));
+      st[6][r] = __ldcs(S.pid + p);
       bandof[r] = (short)bb[u];
     }
     __syncthreads();
@@ -400,7 +404,15 @@ int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int m
     sort_band_zero<<<L.nslots, 256, 0, st>>>(L.jobs, L.slots, mask);
     sort_band_hist<<<dim3(gh, L.nslots), kBandThreads, 0, st>>>(L.jobs, L.slots, L.counts, mask);
     sort_band_scan<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.jobs, L.slots, mask, L.nslots);
-    sort_band_scatter<<<dim3(gb, L.nslots), kBandThreads, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+    constexpr size_t smem = 7 * kBandChunk * sizeof(uint32_t) + kBandChunk * sizeof(short);
+    static bool configured[64] = {};   // once per device (function attributes are per context)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+      cudaFuncSetAttribute(sort_band_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (dev >= 0 && dev < 64) configured[dev] = true;
+    }
+    sort_band_scatter<<<dim3(gb, L.nslots), kBandThreads, smem, st>>>(L.jobs, L.slots, L.counts, mask);
     sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
     k += 5;
   }
