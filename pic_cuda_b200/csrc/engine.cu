@@ -615,7 +615,7 @@ int check_job(pic_engine* E, int job) {
 // One full step of every live job.
 // Counting sort (stream-ordered on s) of the jobs for which `due` holds.
 template <typename Due>
-int sort_jobs(pic_engine* E, const EngineLaunch& L, Due due, cudaStream_t s, bool* launched, bool banded = false) {
+int sort_jobs(pic_engine* E, const EngineLaunch& L, Due due, cudaStream_t s, bool* launched) {
   std::vector<uint8_t> mask(L.nslots, 0);
   bool any = false;
   int max_cells = 0;
@@ -634,7 +634,7 @@ int sort_jobs(pic_engine* E, const EngineLaunch& L, Due due, cudaStream_t s, boo
   if (!any) return PIC_OK;
   CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
   phase_mark(E, 0, true, s);
-  E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), banded, s);
+  E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
   phase_mark(E, 0, false, s);
   return PIC_OK;
 }
@@ -647,7 +647,7 @@ bool sort_after(const JobHost& J) { return (J.steps + 1) % J.cfg.sort_every == 0
 int step_once(pic_engine* E, cudaStream_t s) {
   EngineLaunch L = make_launch(E, nullptr);
   bool sorted = false;
-  int rc = sort_jobs(E, L, sort_before_first, s, &sorted, true);
+  int rc = sort_jobs(E, L, sort_before_first, s, &sorted);
   if (rc) return rc;
   E->launches += launch_step_begin(E->d_st, E->d_jobs, E->njobs_hw, nullptr, s);
   int max_nodes = 0;
@@ -730,7 +730,7 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
       max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
     }
     n += launch_sort_mask(L, E->d_mask, 1, E->side_stream);
-    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), false, E->side_stream);
+    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), E->side_stream);
   }
   if (err == cudaSuccess) err = cudaEventRecord(E->ev_join, E->side_stream);
   n += launch_mg_init(L, E->mg_all.L, s);
@@ -1403,7 +1403,7 @@ int pic_step_graph(pic_engine* E, int nsteps, void* stream) {
   cudaStream_t s = pick(E, stream);
   for (int k = 0; k < nsteps; ++k) {
     bool sorted = false;
-    rc = sort_jobs(E, make_launch(E, nullptr), sort_before_first, s, &sorted, true);
+    rc = sort_jobs(E, make_launch(E, nullptr), sort_before_first, s, &sorted);
     if (rc) return rc;
     bool sort_due = false;
     for (int j = 0; j < E->njobs_hw; ++j) {
@@ -1568,7 +1568,7 @@ int pic_job_sort(pic_engine* E, int job, void* stream) {
   int64_t maxp = 0;
   for (int k = 0; k < J.cfg.n_species; ++k) maxp = std::max<int64_t>(maxp, J.cfg.species[k].capacity);
   EngineLaunch L = make_launch(E, nullptr);
-  launch_sort(L, E->d_mask, J.dev.ncx * J.dev.ncy, (int)std::min<int64_t>(maxp, 1 << 30), J.steps == 0, s);
+  launch_sort(L, E->d_mask, J.dev.ncx * J.dev.ncy, (int)std::min<int64_t>(maxp, 1 << 30), s);
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   return PIC_OK;

@@ -45,10 +45,7 @@ int mover_blocks_per_sm();
 int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t s);
 int launch_compact(const EngineLaunch& L, cudaStream_t s);
 int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
-// banded: the particles are in arbitrary order (first sort after a load): group them into
-// bands of cell rows first, so the cell sort's stores stay local
-int launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, bool banded,
-                cudaStream_t s);
+int launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
 int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
 int launch_ke_reset_pending(JobState* st, int njobs, cudaStream_t s);
 int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);

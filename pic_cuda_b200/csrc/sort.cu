@@ -236,131 +236,6 @@ __global__ void sort_scatter(const JobDev* jobs, const SlotDev* slots, const int
   }
 }
 
-// ---- band pass (particles in arbitrary order, e.g. freshly loaded)
-// A counting sort of randomly ordered particles scatters every 4-byte field to a random place:
-// each store touches its own 32-byte sector.  Before the cell sort such particles are first
-// grouped into kBands bands of cell rows: each CTA orders a chunk of kBandChunk particles by
-// band in shared memory and writes each band's run to consecutive places (~8 particles, a
-// full 32-byte sector per array); the cell sort that follows then writes inside one band's
-// range at a time (a few MB per array, which stays in L2 until its sectors are complete).
-// Both passes read with evict-first loads, so the streamed input does not push the write
-// window out of L2.
-constexpr int kBands = 256;
-constexpr int kBandThreads = 256;
-constexpr int kBandChunk = 2048;   // particles per CTA chunk (8 per thread)
-
-// band of a cell key: rows split into nb bands; particles outside the grid go last
-__device__ __forceinline__ int band_of(uint32_t c, int ncy, int nb) {
-  return c == PIC_CELL_OUT ? nb : (int)(((uint32_t)cell_j(c) * (uint32_t)nb) / (uint32_t)ncy);
-}
-__device__ __forceinline__ int bands_of(const JobDev& J) { return min(kBands, J.ncy); }
-
-// Band counts (cell_count[0 .. nb]) and, after sort_band_scan, band cursors
-// (cell_count[nb + 1 .. 2 nb + 1]); cell_count holds ncx ncy + 1 >= 2 (nb + 1) entries.
-__global__ void __launch_bounds__(kBandThreads) sort_band_hist(const JobDev* jobs, const SlotDev* slots,
-                                                               const int* counts, const uint8_t* mask) {
-  const int s = blockIdx.y;
-  if (!mask[s]) return;
-  const SlotDev& S = slots[s];
-  const JobDev& J = jobs[S.job];
-  const int n = counts[s], nb = bands_of(J), ncy = J.ncy;
-  __shared__ int h[kBands + 1];
-  for (int b = threadIdx.x; b <= nb; b += blockDim.x) h[b] = 0;
-  __syncthreads();
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x)
-    atomicAdd(&h[band_of(S.cell[p], ncy, nb)], 1);
-  __syncthreads();
-  for (int b = threadIdx.x; b <= nb; b += blockDim.x)
-    if (h[b]) atomicAdd(S.cell_count + b, h[b]);
-}
-
-__global__ void sort_band_zero(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
-  const int s = blockIdx.x;
-  if (!mask[s]) return;
-  const SlotDev& S = slots[s];
-  const int nb = bands_of(jobs[S.job]);
-  for (int b = threadIdx.x; b < 2 * (nb + 1); b += blockDim.x) S.cell_count[b] = 0;
-}
-
-// exclusive scan of the band counts into the cursors (one thread per slot: nb + 1 <= 257)
-__global__ void sort_band_scan(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask, int nslots) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nslots || !mask[s]) return;
-  const SlotDev& S = slots[s];
-  const int nb = bands_of(jobs[S.job]);
-  int a = 0;
-  for (int b = 0; b <= nb; ++b) {
-    const int c = S.cell_count[b];
-    S.cell_count[nb + 1 + b] = a;
-    a += c;
-  }
-}
-
-// Each CTA: chunks of kBandChunk particles ordered by band in shared memory (the order inside
-// a band is the atomics'), one cursor atomic per band present, then consecutive stores.
-__global__ void __launch_bounds__(kBandThreads) sort_band_scatter(const JobDev* jobs, const SlotDev* slots,
-                                                                  const int* counts, const uint8_t* mask) {
-  const int s = blockIdx.y;
-  if (!mask[s]) return;
-  const SlotDev& S = slots[s];
-  const JobDev& J = jobs[S.job];
-  const int n = counts[s], nb = bands_of(J), ncy = J.ncy;
-  int* const cursor = S.cell_count + nb + 1;
-  __shared__ int h[kBands + 1], off[kBands + 1], base[kBands + 1], fill[kBands + 1];
-  extern __shared__ __align__(16) uint32_t band_smem[];
-  uint32_t (*st)[kBandChunk] = reinterpret_cast<uint32_t (*)[kBandChunk]>(band_smem);
-  short* const bandof = reinterpret_cast<short*>(band_smem + 7 * kBandChunk);
-  constexpr int PER = kBandChunk / kBandThreads;
-  const int t = threadIdx.x;
-  for (int c0 = blockIdx.x * kBandChunk; c0 < n; c0 += gridDim.x * kBandChunk) {
-    const int m = min(kBandChunk, n - c0);
-    for (int b = t; b <= nb; b += kBandThreads) { h[b] = 0; fill[b] = 0; }
-    __syncthreads();
-    int bb[PER];
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int k = t + u * kBandThreads;
-      bb[u] = k < m ? band_of(__ldcs(S.cell + c0 + k), ncy, nb) : -1;
-      if (bb[u] >= 0) atomicAdd(&h[bb[u]], 1);
-    }
-    __syncthreads();
-    if (t == 0) {
-      int a = 0;
-      for (int b = 0; b <= nb; ++b) { off[b] = a; a += h[b]; }
-    }
-    __syncthreads();
-    for (int b = t; b <= nb; b += kBandThreads) base[b] = h[b] ? atomicAdd(cursor + b, h[b]) : 0;
-#pragma unroll
-    for (int u = 0; u < PER; ++u) {
-      const int k = t + u * kBandThreads;
-      if (bb[u] < 0) continue;
-      const int r = off[bb[u]] + atomicAdd(&fill[bb[u]], 1);
-      const int p = c0 + k;
-      st[0][r] = __ldcs(S.cell + p);
-      st[1][r] = __float_as_uint(__ldcs(S.fx + p));
-      st[2][r] = __float_as_uint(__ldcs(S.fy + p));
-      st[3][r] = __float_as_uint(__ldcs(S.vx + p));
-      st[4][r] = __float_as_uint(__ldcs(S.vy + p));
-      st[5][r] = __float_as_uint(__ldcs(S.vz + p));
-      st[6][r] = __ldcs(S.pid + p);
-      bandof[r] = (short)bb[u];
-    }
-    __syncthreads();
-    for (int r = t; r < m; r += kBandThreads) {
-      const int b = bandof[r];
-      const int d = base[b] + (r - off[b]);
-      S.cell_b[d] = st[0][r];
-      S.fx_b[d] = __uint_as_float(st[1][r]);
-      S.fy_b[d] = __uint_as_float(st[2][r]);
-      S.vx_b[d] = __uint_as_float(st[3][r]);
-      S.vy_b[d] = __uint_as_float(st[4][r]);
-      S.vz_b[d] = __uint_as_float(st[5][r]);
-      S.pid_b[d] = st[6][r];
-    }
-    __syncthreads();
-  }
-}
-
 template <typename T>
 __device__ __forceinline__ void swp(T*& a, T*& b) { T* t = a; a = b; b = t; }
 
@@ -392,30 +267,8 @@ int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, int offset, cudaStrea
   return 1;
 }
 
-int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, bool banded,
-                cudaStream_t st) {
+int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
   if (L.nslots == 0) return 0;
-  int k = 0;
-  if (banded) {
-    // particles in arbitrary order: group them into bands of rows first (into the second
-    // array set), then the cell sort below runs on the band-ordered arrays
-    const int gb = std::min(std::max((max_particles + kBandChunk - 1) / kBandChunk, 1), 2 * L.num_sms);
-    const int gh = std::min(std::max((max_particles + 255) / 256, 1), 4 * L.num_sms);
-    sort_band_zero<<<L.nslots, 256, 0, st>>>(L.jobs, L.slots, mask);
-    sort_band_hist<<<dim3(gh, L.nslots), kBandThreads, 0, st>>>(L.jobs, L.slots, L.counts, mask);
-    sort_band_scan<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.jobs, L.slots, mask, L.nslots);
-    constexpr size_t smem = 7 * kBandChunk * sizeof(uint32_t) + kBandChunk * sizeof(short);
-    static bool configured[64] = {};   // once per device (function attributes are per context)
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !configured[dev]) {
-      cudaFuncSetAttribute(sort_band_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (dev >= 0 && dev < 64) configured[dev] = true;
-    }
-    sort_band_scatter<<<dim3(gb, L.nslots), kBandThreads, smem, st>>>(L.jobs, L.slots, L.counts, mask);
-    sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
-    k += 5;
-  }
   const int ncells = max_cells + 1;
   const int ntiles = (ncells + kTile - 1) / kTile;
   const int gz = std::min(std::max((ncells + 255) / 256, 1), 4 * L.num_sms);
@@ -427,5 +280,5 @@ int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int m
   sort_apply<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_scatter<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
   sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
-  return k + 7;
+  return 7;
 }
