@@ -231,8 +231,15 @@ int pic_job_diagnostics(pic_engine* e, int job, pic_diagnostics* out);
  * PIC_OPT_MG_CLUSTER_TOP: largest level side solved by a thread-block cluster (65 = none,
  *   default); applies to jobs created after the call.
  * PIC_OPT_MG_COARSE_TOP: largest level side (3..129) solved inside one CTA's shared memory
- *   (65 = default); applies to jobs created after the call. */
-enum { PIC_OPT_MG_LEVELS_KERNEL = 1, PIC_OPT_MG_CLUSTER_TOP = 2, PIC_OPT_MG_COARSE_TOP = 3 };
+ *   (65 = default); applies to jobs created after the call.
+ * PIC_OPT_MOVER_CTAS_PER_SM: CTAs per SM of the persistent particle pass (0 = as many as
+ *   fit, the default; larger values are capped there).  Takes effect at the next step.
+ * PIC_OPT_MG_WIDE_TILES: on multigrid tile levels with at most this many tiles per SM each
+ *   tile runs on a 1024-thread CTA (a shorter latency chain when the level cannot fill the
+ *   GPU), on the others on a 256-thread CTA (default 2; 0 = never).  Takes effect at the next
+ *   field solve. */
+enum { PIC_OPT_MG_LEVELS_KERNEL = 1, PIC_OPT_MG_CLUSTER_TOP = 2, PIC_OPT_MG_COARSE_TOP = 3,
+       PIC_OPT_MOVER_CTAS_PER_SM = 4, PIC_OPT_MG_WIDE_TILES = 5 };
 int pic_engine_set_option(pic_engine* e, int option, int64_t value);
 int pic_engine_get_option(pic_engine* e, int option, int64_t* value);
 /* Counting-sort cadence of one job (0 = never), from its next step on. */

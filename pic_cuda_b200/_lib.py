@@ -22,7 +22,7 @@ PROC_ELASTIC, PROC_EXCITATION, PROC_IONIZATION, PROC_CHARGE_EXCHANGE = 1, 2, 3, 
 PHASE_KICK, PHASE_MCC, PHASE_DRIFT, PHASE_WALLS, PHASE_DEPOSIT = 1, 2, 4, 8, 16
 GRID_RHO, GRID_PHI, GRID_EX, GRID_EY = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
-OPT_MG_LEVELS_KERNEL, OPT_MG_CLUSTER_TOP, OPT_MG_COARSE_TOP = 1, 2, 3
+OPT_MG_LEVELS_KERNEL, OPT_MG_CLUSTER_TOP, OPT_MG_COARSE_TOP, OPT_MOVER_CTAS_PER_SM, OPT_MG_WIDE_TILES = 1, 2, 3, 4, 5
 NODE_FLUID, NODE_DIRICHLET, NODE_SOLID = 0, 1, 2
 EMB_COARSEN_ANY, EMB_PROLONG_BILINEAR = 1, 2
 

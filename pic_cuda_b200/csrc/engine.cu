@@ -237,7 +237,9 @@ struct pic_engine {
   // (admitting and retiring jobs while others run should not cost a device-wide cudaFree).
   cudaMemPool_t pool = nullptr;
   int num_sms = 148;
-  int mover_bps = 4;
+  int mover_bps = 4;        // mover CTAs per SM: the occupancy limit
+  int mover_cps = 0;        // PIC_OPT_MOVER_CTAS_PER_SM (0: mover_bps)
+  int wide_factor = 2;      // PIC_OPT_MG_WIDE_TILES
   int cluster_C = 0;          // thread-block cluster size of the coarse solver (0: none)
   // Largest level side given to the cluster coarse solver.  Measured on B200 (1025^2 job):
   // tile kernels over all SMs for every level above 65^2 and one CTA below beat the
@@ -312,7 +314,7 @@ EngineLaunch make_launch(pic_engine* E, const uint8_t* active) {
   L.nslots = E->njobs_hw * kSlotsPerJob;
   L.njobs = E->njobs_hw;
   L.num_sms = E->num_sms;
-  L.mover_grid = E->num_sms * E->mover_bps;
+  L.mover_grid = E->num_sms * (E->mover_cps > 0 ? std::min(E->mover_cps, E->mover_bps) : E->mover_bps);
   L.running = E->d_running;
   L.gbar = reinterpret_cast<unsigned*>(E->d_running + 2);  // the grid barrier's arrival counter
   L.absorbed = E->d_aux + 4 * kMaxJobs * kSlotsPerJob;
@@ -491,6 +493,7 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   M.nu_pre_max = nu_pre_max;
   M.nu_post_max = nu_post_max;
   M.pdl = E->pdl ? 1 : 0;
+  M.wide_factor = E->wide_factor;
   M.fast_nu_pre = (!ids.empty() && nu_pre_min == nu_pre_max) ? nu_pre_max : -1;
   M.fast_nu_post = (!ids.empty() && nu_post_min == nu_post_max) ? nu_post_max : -1;
   // Levels 1..lc as phases of one cooperative launch (PIC_OPT_MG_LEVELS_KERNEL).  Measured on
@@ -857,6 +860,7 @@ int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out) {
     if (const char* v = std::getenv("PIC_MG_COARSE_TOP")) E->coarse_top = std::atoi(v);
     if (const char* v = std::getenv("PIC_PDL")) E->pdl = std::atoi(v) != 0;
     if (const char* v = std::getenv("PIC_MG_LEVELS_KERNEL")) E->levels_kernel = std::atoi(v) == 1;
+    if (const char* v = std::getenv("PIC_MG_WIDE_TILES")) E->wide_factor = std::min(std::max(std::atoi(v), 0), 64);
   }
   const int nslots = kMaxJobs * kSlotsPerJob;
   cudaError_t e = cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking);
@@ -1668,6 +1672,12 @@ int pic_engine_set_option(pic_engine* E, int option, int64_t value) {
   } else if (option == PIC_OPT_MG_COARSE_TOP) {
     if (value < 3 || value > PIC_COARSE_MAX) return fail(PIC_ERR_ARG, "PIC_OPT_MG_COARSE_TOP out of range (3..129)");
     E->coarse_top = (int)value;
+  } else if (option == PIC_OPT_MOVER_CTAS_PER_SM) {
+    if (value < 0 || value > 32) return fail(PIC_ERR_ARG, "PIC_OPT_MOVER_CTAS_PER_SM out of range (0..32)");
+    E->mover_cps = (int)value;
+  } else if (option == PIC_OPT_MG_WIDE_TILES) {
+    if (value < 0 || value > 64) return fail(PIC_ERR_ARG, "PIC_OPT_MG_WIDE_TILES out of range (0..64)");
+    E->wide_factor = (int)value;
   } else {
     return fail(PIC_ERR_ARG, "unknown option");
   }
@@ -1683,6 +1693,8 @@ int pic_engine_get_option(pic_engine* E, int option, int64_t* value) {
   if (option == PIC_OPT_MG_LEVELS_KERNEL) *value = E->levels_kernel;
   else if (option == PIC_OPT_MG_CLUSTER_TOP) *value = E->cluster_top;
   else if (option == PIC_OPT_MG_COARSE_TOP) *value = E->coarse_top;
+  else if (option == PIC_OPT_MOVER_CTAS_PER_SM) *value = E->mover_cps;
+  else if (option == PIC_OPT_MG_WIDE_TILES) *value = E->wide_factor;
   else return fail(PIC_ERR_ARG, "unknown option");
   return PIC_OK;
 }

@@ -71,6 +71,7 @@ struct MgLaunch {
   int nu_pre_max, nu_post_max;                           // shared-memory sizing of the tile kernels
   int fast_nu_pre, fast_nu_post;                         // smoothing counts shared by every job, else -1
   int pdl;                                               // programmatic dependent launches in the V-cycle
+  int wide_factor;                                       // 1024-thread tile CTAs on levels with <= this x SMs tiles
   int levels_grid;                                       // >0: levels 1..lc in one cooperative launch
   size_t levels_smem, levels_quarter_floats;
 };

@@ -1230,11 +1230,13 @@ int mg_levels_configure(int num_sms, int nu_pre_max, int nu_post_max, size_t coa
 
 // Tile launches of one level: the compile-time-shape kernels when every job of the launch
 // has the same smoothing count (<= kMaxFastNu), else the generic ones.
-// 1024-thread CTAs where a level has at most two tiles per SM.  pdl: the launch follows a
+// 1024-thread CTAs where a level has at most wide_factor (default 2) tiles per SM.  pdl: the
+// launch follows a
 // kernel of the V-cycle that this one's prologue may overlap (programmatic serialisation).
 static bool launch_down(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl, cudaStream_t s) {
   if (M.fast_nu_pre >= 0 && M.fast_nu_pre <= kMaxFastNu) {
-    down_fast(M.fast_nu_pre, M.n_down[l], M.n_down[l] <= 2 * L.num_sms, pdl && M.pdl, M.down_tiles[l], L.jobs, L.st,
+    down_fast(M.fast_nu_pre, M.n_down[l], M.n_down[l] <= M.wide_factor * L.num_sms, pdl && M.pdl, M.down_tiles[l],
+              L.jobs, L.st,
               l, s);
     return true;
   }
@@ -1243,7 +1245,8 @@ static bool launch_down(const MgLaunch& M, int l, const EngineLaunch& L, bool pd
 }
 static bool launch_up(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl, cudaStream_t s) {
   if (M.fast_nu_post >= 0 && M.fast_nu_post <= kMaxFastNu) {
-    up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= 2 * L.num_sms, pdl && M.pdl, M.up_tiles[l], L.jobs, L.st, l,
+    up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= M.wide_factor * L.num_sms, pdl && M.pdl, M.up_tiles[l], L.jobs,
+            L.st, l,
             l == 0 ? 1 : 0, L.running, s);
     return true;
   }

@@ -109,3 +109,30 @@ def test_multi_wave_grid_repeatable_bitwise():
         e.close()
     for phi, cyc in out[1:]:
         assert np.array_equal(phi, out[0][0]) and cyc == out[0][1]
+
+
+@pytest.mark.parametrize("opts", [
+    {L.OPT_MOVER_CTAS_PER_SM: 1},
+    {L.OPT_MOVER_CTAS_PER_SM: 3, L.OPT_MG_WIDE_TILES: 0},
+    {L.OPT_MG_WIDE_TILES: 64, L.OPT_MG_LEVELS_KERNEL: 1},
+])
+def test_tuning_options_bitwise_identical(opts):
+    """The launch shapes the autotuner chooses among (CTAs per SM of the particle pass, CTA
+    size of the multigrid tile levels, one launch per level or the cooperative levels kernel)
+    change no result: with the int64 deposit every step is bit for bit the default's."""
+    specs = _jobs()
+    e = Engine(0)
+    ref = _run(e, specs, 5)
+    e.close()
+    e = Engine(0)
+    for k, v in opts.items():
+        e.set_option(k, v)
+        assert e.get_option(k) == v
+    got = _run(e, specs, 5)
+    e.close()
+    for a, b in zip(ref, got):
+        for s in (0, 1):
+            for key in ("pid", "x", "y", "vx", "vy", "vz"):
+                assert np.array_equal(a[0][s][key], b[0][s][key]), (s, key)
+        assert np.array_equal(a[1], b[1])
+        assert a[2]["vcycles"] == b[2]["vcycles"]
