@@ -424,7 +424,7 @@ void free_job(pic_engine* E, JobHost& J) {
 int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   out.release();
   std::vector<TileRef> init, upd, down[PIC_MAX_LEVELS], up[PIC_MAX_LEVELS];
-  std::vector<int> coarse, cluster;
+  std::vector<int> coarse, cluster, finish;
   size_t cluster_smem = 0;
   int max_depth = 0, max_cycles = 1, nu_pre_max = 1, nu_post_max = 1;
   int nu_pre_min = 1 << 30, nu_post_min = 1 << 30;
@@ -444,6 +444,7 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
     if (D.lc == 0)
       for (int tj = 0; tj < t0; ++tj)
         for (int ti = 0; ti < t0; ++ti) upd.push_back({id, ti, tj, tj * t0 + ti, t0 * t0, 0});
+    if (D.lc >= 1) finish.push_back(id);
     for (int l = 0; l < D.lc; ++l) {
       const int tc = (D.nl[l + 1] + 15) / 16;
       for (int tj = 0; tj < tc; ++tj)
@@ -472,6 +473,8 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   }
   std::vector<int> lists(coarse);
   lists.insert(lists.end(), cluster.begin(), cluster.end());
+  lists.insert(lists.end(), finish.begin(), finish.end());
+  lists.insert(lists.end(), ids.begin(), ids.end());
   if (!lists.empty()) {
     CK(cudaMalloc(&out.d_coarse, lists.size() * sizeof(int)));
     CK(cudaMemcpy(out.d_coarse, lists.data(), lists.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -486,6 +489,8 @@ int build_mg(pic_engine* E, const std::vector<int>& ids, MgBuild& out) {
   }
   M.coarse_jobs = out.d_coarse; M.n_coarse = (int)coarse.size();
   M.cluster_jobs = out.d_coarse + coarse.size(); M.n_cluster = (int)cluster.size();
+  M.finish_jobs = out.d_coarse + coarse.size() + cluster.size(); M.n_finish = (int)finish.size();
+  M.init_jobs = M.finish_jobs + finish.size(); M.n_init_jobs = (int)ids.size();
   M.cluster_C = E->cluster_C;
   M.cluster_smem = cluster_smem;
   M.max_depth = max_depth;

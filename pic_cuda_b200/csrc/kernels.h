@@ -59,11 +59,13 @@ void launch_rho_sum(const JobDev* jd, JobState* st, double* scratch, int nparts,
 // Multigrid (all jobs of a launch at once).
 struct MgLaunch {
   const TileRef* init_tiles; int n_init;                 // level-0 residual, 32x32 owned
+  const int* init_jobs; int n_init_jobs;                 // every job of the solve (mg_init_finish_kernel)
   const TileRef* down_tiles[PIC_MAX_LEVELS]; int n_down[PIC_MAX_LEVELS];   // coarse 16x16 owned
   const TileRef* up_tiles[PIC_MAX_LEVELS]; int n_up[PIC_MAX_LEVELS];       // fine 32x32 owned
   const TileRef* upd_tiles; int n_upd;                   // level-0 update for jobs with lc == 0
   const int* coarse_jobs; int n_coarse;                  // single-CTA coarse solve
   const int* cluster_jobs; int n_cluster;                // thread-block-cluster coarse solve
+  const int* finish_jobs; int n_finish;                  // jobs with level-0 up tiles (lc >= 1)
   int cluster_C;
   size_t cluster_smem;
   int max_depth;                                         // max lc over jobs

@@ -91,7 +91,7 @@ __device__ bool last_of_job(JobState& T, int nlocal) {
 // batch of asynchronous copies; the guess is formed once per node in shared memory.  The
 // same pass sums the deposited charge (deterministic per-tile partials, like the norms).
 __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict__ tiles, const JobDev* __restrict__ jobs,
-                                                      JobState* __restrict__ st, int* running) {
+                                                      const JobState* __restrict__ st) {
   constexpr int PW = kTI + 2, NT = 256;
   constexpr int NP = (PW * PW + NT - 1) / NT;
   constexpr int NO = kTI * kTI / NT;
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   __shared__ __align__(16) double RH[kTI * kTI]; // rho of the owned nodes, raw
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
-  JobState& T = st[tr.job];
+  const JobState& T = st[tr.job];
   const int nx = J.nx, ny = J.ny;
   const int cur = T.phi_cur;
   const double* __restrict__ phi = J.phi64[cur];
@@ -188,27 +188,43 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
     partials[2 * (tr.pbase + tr.local) + 1] = sf;
     partials[2 * tr.nlocal + tr.pbase + tr.local] = sq;   // deposited charge (third block)
   }
-  if (last_of_job(T, tr.nlocal)) {
-    __threadfence();
-    const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
-    const double f2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 1);
-    const double q = ordered_sum(partials + 2 * tr.nlocal + tr.pbase, tr.nlocal, 1, 0);
-    if (t != 0) return;
-    T.rnorm2 = r2;
-    T.fnorm2 = f2;
-    T.total_charge = q * qref;
-    T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
-    T.cycles = 0;
-    T.converged = 0;
-    if (xs) {
-      T.phi_prev1 = cur + 1;
-      T.phi_cur = tgt;
-      T.phi_nxt = hist ? prev : (cur + 2) % 3;
-    } else {
-      T.phi_nxt = cur ^ 1;
-    }
-    atomicAdd(running, 1);
+  // the job's norms and state follow in mg_init_finish_kernel
+}
+
+// After mg_init_kernel, one CTA per job: the tiles' partial norms and charge summed in a fixed
+// order, the relative residual of the initial guess, the potential buffers the defect
+// correction uses (with the warm start, the guess's buffer), and the job joins the running
+// count.
+__global__ void __launch_bounds__(256) mg_init_finish_kernel(const int* __restrict__ job_list,
+                                                             const JobDev* __restrict__ jobs,
+                                                             JobState* __restrict__ st, int* running) {
+  const int job = job_list[blockIdx.x];
+  const JobDev& J = jobs[job];
+  JobState& T = st[job];
+  const int t0 = (J.nx + kTI - 1) / kTI;   // the tile list's t0 x t0 tiles (square grids)
+  const int n = t0 * t0;
+  const double r2 = ordered_sum(J.partials, n, 2, 0);
+  const double f2 = ordered_sum(J.partials, n, 2, 1);
+  const double q = ordered_sum(J.partials + 2 * n, n, 1, 0);
+  if (threadIdx.x != 0) return;
+  const int cur = T.phi_cur;
+  const bool xs = J.warm_start != 0;
+  const int prev = T.phi_prev1 - 1;
+  const bool hist = xs && prev >= 0;
+  T.rnorm2 = r2;
+  T.fnorm2 = f2;
+  T.total_charge = q * J.qref;
+  T.relres = f2 > 0.0 ? sqrt(r2 / f2) : sqrt(r2);
+  T.cycles = 0;
+  T.converged = 0;
+  if (xs) {
+    T.phi_prev1 = cur + 1;
+    T.phi_cur = hist ? 3 - cur - prev : (cur + 1) % 3;
+    T.phi_nxt = hist ? prev : (cur + 2) % 3;
+  } else {
+    T.phi_nxt = cur ^ 1;
   }
+  atomicAdd(running, 1);
 }
 
 // Thread groups a tile is processed by: a whole 256-thread CTA, or one 256-thread quarter of a
@@ -914,14 +930,16 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
 // tensor-map loads; on level 0 phi64 (with a one-node halo) and rho of the owned nodes come
 // in one batch of asynchronous copies beside them.
 template <int NU, int MODE, int NT>
-__global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const TileRef* __restrict__ tiles,
+__global__ void __launch_bounds__(NT, MODE ? 5 : 1) mg_up_fast_kernel(const TileRef* __restrict__ tiles,
                                                                       const JobDev* __restrict__ jobs,
-                                                                      JobState* __restrict__ st, int l, int* running) {
+                                                                      JobState* __restrict__ st, int l) {
   constexpr int H = 2 * NU, X = MODE, W = mgt::up_w(NU, X), OFF = mgt::up_off(NU, X), P = mgt::up_bw(NU, X);
   constexpr int CW = mgt::up_cw(NU, X), COFF = mgt::up_coff(NU, X), CP = mgt::up_cbw(NU, X);
   static_assert(W == kTU + 2 * H + 2 * X, "tile shape");
   constexpr int PW = kTU + 2;
-  constexpr int NL = (W * W + NT - 1) / NT;
+  constexpr int KC = (W + X + 1) / 2;              // coarse cells per tile row
+  constexpr int NKC = (KC * KC + NT - 1) / NT;
+  static_assert(KC + 1 <= CW, "coarse tile holds every cell's right and upper neighbour");
   constexpr int NP = MODE ? (PW * PW + NT - 1) / NT : 0;
   constexpr int NO = kTU * kTU / NT;
   __shared__ __align__(128) float es[W * P];
@@ -934,8 +952,9 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   float* const f = fs + OFF;
   const float* const cs = css + COFF;
   tma::pdl_trigger();
-  // tile, job and job-state fields: within a V-cycle only this kernel's own last CTA (level 0)
-  // writes the state, so they are read before waiting for the previous launch
+  // tile, job and job-state fields: the state changes only in mg_finish_kernel, at the end of
+  // a V-cycle (the next V-cycle's first launch waits for it), so they are read before waiting
+  // for the previous launch
   const TileRef tr = tiles[blockIdx.x];
   const JobDev& J = jobs[tr.job];
   JobState& T = st[tr.job];
@@ -961,8 +980,6 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
   const RhoSrc rho{J.deposit_mode, J.rho_f, J.rho_i, J.rho_d};
   float* const f0 = fsel ? J.f[0] : J.f0b;   // the new defect goes to the other buffer
   double* const partials = J.partials;
-  const double tol = J.tol;
-  const int max_cycles = J.max_cycles;
   const int t = threadIdx.x;
   if (t == 0) {
     tma::mbar_init(&mbar, 1);
@@ -1001,17 +1018,25 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
     tma::cp_async_wait_all();
   }
   if (!tiles_arrived(&mbar, &T)) return;
-  // ---- bilinear prolongation added to the pre-smoothed correction
+  // ---- bilinear prolongation added to the pre-smoothed correction: one coarse cell per
+  // thread and pass, its four fine nodes (2c, 2c + 1 in each direction) with prolong_value's
+  // expressions.  gx0 has the parity X, so cell k of the tile holds tile columns 2k - X and
+  // 2k + 1 - X (the first and last cells hold one column each).
 #pragma unroll
-  for (int u = 0; u < NL; ++u) {
+  for (int u = 0; u < NKC; ++u) {
     const int q = t + u * NT;
-    if (q < W * W) {
-      const int ly = q / W, lx = q - ly * W;
+    if (q < KC * KC) {
+      const int ky = q / KC, kx = q - ky * KC;
+      const float* cp = cs + ky * CP + kx;
+      const int lx = 2 * kx - X, ly = 2 * ky - X;
       const int gx = gx0 + lx, gy = gy0 + ly;
-      if ((unsigned)gx < (unsigned)nf && (unsigned)gy < (unsigned)nf) {
-        const float* cp = cs + ((gy >> 1) - cy0) * CP + ((gx >> 1) - cx0);
-        e[ly * P + lx] += prolong_value(cp, CP, gx & 1, gy & 1);
-      }
+      const bool x0 = lx >= 0 && (unsigned)gx < (unsigned)nf, x1 = lx + 1 < W && (unsigned)(gx + 1) < (unsigned)nf;
+      const bool y0 = ly >= 0 && (unsigned)gy < (unsigned)nf, y1 = ly + 1 < W && (unsigned)(gy + 1) < (unsigned)nf;
+      const int b = ly * P + lx;
+      if (y0 && x0) e[b] += prolong_value(cp, CP, false, false);
+      if (y0 && x1) e[b + 1] += prolong_value(cp, CP, true, false);
+      if (y1 && x0) e[b + P] += prolong_value(cp, CP, false, true);
+      if (y1 && x1) e[b + P + 1] += prolong_value(cp, CP, true, true);
     }
   }
   __syncthreads();
@@ -1058,22 +1083,39 @@ __global__ void __launch_bounds__(NT, MODE ? 4 : 1) mg_up_fast_kernel(const Tile
       f0[gy * pf + gx] = (float)r;
       ar += r * r;
     }
+    // the tile's partial only: the job's norm, convergence test and buffer swap follow in
+    // mg_finish_kernel, so no CTA waits for its stores or a shared ticket before it leaves
     const double sr = block_sum(ar);
     if (t == 0) partials[2 * (tr.pbase + tr.local)] = sr;
-    if (last_of_job(T, tr.nlocal)) {
-      __threadfence();
-      const double r2 = ordered_sum(partials + 2 * tr.pbase, tr.nlocal, 2, 0);
-      if (t != 0) return;
-      T.rnorm2 = r2;
-      T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
-      T.cycles += 1;
-      T.phi_cur = nxt;
-      T.phi_nxt = cur;
-      T.fsel = fsel ^ 1;
-      if (T.relres < tol) { T.converged = 1; atomicSub(running, 1); }
-      else if (T.cycles >= max_cycles) { T.converged = 2; atomicSub(running, 1); }
-    }
   }
+}
+
+// End of a V-cycle for the jobs whose level 0 ran in mg_up_fast_kernel<., 1, .>: one CTA per
+// job sums the tiles' partial norms in a fixed order, counts the cycle, swaps the potential
+// and defect buffers and takes a converged job out of the running count.  Launched after the
+// level-0 up kernel (waits for it in tma::pdl_wait); the next V-cycle's first launch waits for
+// this one.
+__global__ void __launch_bounds__(256) mg_finish_kernel(const int* __restrict__ job_list,
+                                                        const JobDev* __restrict__ jobs,
+                                                        JobState* __restrict__ st, int* running) {
+  tma::pdl_trigger();
+  tma::pdl_wait();
+  const int job = job_list[blockIdx.x];
+  const JobDev& J = jobs[job];
+  JobState& T = st[job];
+  if (T.converged) return;
+  const int tu = (J.nl[0] + kTU - 1) / kTU;
+  const double r2 = ordered_sum(J.partials, tu * tu, 2, 0);
+  if (threadIdx.x != 0) return;
+  T.rnorm2 = r2;
+  T.relres = T.fnorm2 > 0.0 ? sqrt(r2 / T.fnorm2) : sqrt(r2);
+  T.cycles += 1;
+  const int cur = T.phi_cur;
+  T.phi_cur = T.phi_nxt;
+  T.phi_nxt = cur;
+  T.fsel ^= 1;
+  if (T.relres < J.tol) { T.converged = 1; atomicSub(running, 1); }
+  else if (T.cycles >= J.max_cycles) { T.converged = 2; atomicSub(running, 1); }
 }
 
 // Launch with optional programmatic stream serialisation (the kernel may start while the
@@ -1100,10 +1142,10 @@ void launch_down_fast(int grid, bool wide, bool pdl, const TileRef* tiles, const
 }
 template <int NU>
 void launch_up_fast(int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, JobState* st, int l,
-                    int mode, int* running, cudaStream_t s) {
-  if (mode == 1) launch_k(mg_up_fast_kernel<NU, 1, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l, running);
-  else if (wide) launch_k(mg_up_fast_kernel<NU, 0, 1024>, grid, 1024, 0, pdl, s, tiles, jobs, st, l, running);
-  else launch_k(mg_up_fast_kernel<NU, 0, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l, running);
+                    int mode, cudaStream_t s) {
+  if (mode == 1) launch_k(mg_up_fast_kernel<NU, 1, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l);
+  else if (wide) launch_k(mg_up_fast_kernel<NU, 0, 1024>, grid, 1024, 0, pdl, s, tiles, jobs, st, l);
+  else launch_k(mg_up_fast_kernel<NU, 0, 256>, grid, 256, 0, pdl, s, tiles, jobs, st, l);
 }
 void down_fast(int nu, int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, const JobState* st,
                int l, cudaStream_t s) {
@@ -1116,13 +1158,13 @@ void down_fast(int nu, int grid, bool wide, bool pdl, const TileRef* tiles, cons
   }
 }
 void up_fast(int nu, int grid, bool wide, bool pdl, const TileRef* tiles, const JobDev* jobs, JobState* st, int l,
-             int mode, int* running, cudaStream_t s) {
+             int mode, cudaStream_t s) {
   switch (nu) {
-    case 0: launch_up_fast<0>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
-    case 1: launch_up_fast<1>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
-    case 2: launch_up_fast<2>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
-    case 3: launch_up_fast<3>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
-    default: launch_up_fast<4>(grid, wide, pdl, tiles, jobs, st, l, mode, running, s); break;
+    case 0: launch_up_fast<0>(grid, wide, pdl, tiles, jobs, st, l, mode, s); break;
+    case 1: launch_up_fast<1>(grid, wide, pdl, tiles, jobs, st, l, mode, s); break;
+    case 2: launch_up_fast<2>(grid, wide, pdl, tiles, jobs, st, l, mode, s); break;
+    case 3: launch_up_fast<3>(grid, wide, pdl, tiles, jobs, st, l, mode, s); break;
+    default: launch_up_fast<4>(grid, wide, pdl, tiles, jobs, st, l, mode, s); break;
   }
 }
 
@@ -1202,8 +1244,9 @@ void mg_configure_coarse(size_t smem_bytes) {
 int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   cudaMemsetAsync(L.running, 0, sizeof(int), s);
   if (!M.n_init) return 0;
-  mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st, L.running);
-  return 1;
+  mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st);
+  mg_init_finish_kernel<<<M.n_init_jobs, 256, 0, s>>>(M.init_jobs, L.jobs, L.st, L.running);
+  return 2;
 }
 
 
@@ -1246,8 +1289,9 @@ static bool launch_down(const MgLaunch& M, int l, const EngineLaunch& L, bool pd
 static bool launch_up(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl, cudaStream_t s) {
   if (M.fast_nu_post >= 0 && M.fast_nu_post <= kMaxFastNu) {
     up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= M.wide_factor * L.num_sms, pdl && M.pdl, M.up_tiles[l], L.jobs,
-            L.st, l,
-            l == 0 ? 1 : 0, L.running, s);
+            L.st, l, l == 0 ? 1 : 0, s);
+    if (l == 0)
+      launch_k(mg_finish_kernel, M.n_finish, 256, 0, M.pdl != 0, s, M.finish_jobs, L.jobs, L.st, L.running);
     return true;
   }
   mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
@@ -1281,7 +1325,7 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, mg_levels_kernel, a);
     ++k;
-    if (M.n_up[0]) { launch_up(M, 0, L, false, s); ++k; }
+    if (M.n_up[0]) k += launch_up(M, 0, L, false, s) ? 2 : 1;   // + mg_finish_kernel
     if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
     return k;
   }
@@ -1298,7 +1342,7 @@ int launch_mg_vcycle(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   }
   if (M.n_cluster) { k += launch_mg_cluster(M.cluster_jobs, M.n_cluster, M.cluster_C, M.cluster_smem, L.jobs, L.st, s); prev_fast = false; }
   for (int l = M.max_depth - 1; l >= 0; --l)
-    if (M.n_up[l]) { prev_fast = launch_up(M, l, L, prev_fast, s); ++k; }
+    if (M.n_up[l]) { prev_fast = launch_up(M, l, L, prev_fast, s); k += (prev_fast && l == 0) ? 2 : 1; }
   if (M.n_upd) { mg_up_kernel<<<M.n_upd, 256, up_smem(0), s>>>(M.upd_tiles, L.jobs, L.st, 0, 2, L.running); ++k; }
   return k;
 }
