@@ -187,6 +187,12 @@ typedef struct pic_engine pic_engine;
 int pic_engine_create(int device, int64_t pool_bytes, pic_engine** out);
 int pic_engine_destroy(pic_engine* e);
 int pic_engine_bytes_needed(const pic_job_config* cfg, int64_t* bytes);  /* job footprint */
+/* Maps `bytes` of device memory into the engine's job memory pool now (one allocation, freed
+ * back to the pool at once), so that jobs created later take their arrays from memory that is
+ * already mapped instead of growing the pool while they are admitted.  The pool keeps the
+ * memory until the engine is destroyed.  The reservation does not count against pool_bytes
+ * (only job memory does). */
+int pic_engine_reserve(pic_engine* e, int64_t bytes);
 int pic_job_create(pic_engine* e, const pic_job_config* cfg, int* job_id);
 int pic_job_destroy(pic_engine* e, int job_id);
 int pic_engine_num_jobs(pic_engine* e, int* n);

@@ -81,6 +81,7 @@ _SIGS = {
     "pic_engine_destroy": (_I, [_VP]),
     "pic_engine_bytes_needed": (_I, [C.POINTER(JobConfig), C.POINTER(_I64)]),
     "pic_engine_num_jobs": (_I, [_VP, C.POINTER(_I)]),
+    "pic_engine_reserve": (_I, [_VP, _I64]),
     "pic_job_create": (_I, [_VP, C.POINTER(JobConfig), C.POINTER(_I)]),
     "pic_job_destroy": (_I, [_VP, _I]),
     "pic_job_load_species": (_I, [_VP, _I, _I, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _I]),

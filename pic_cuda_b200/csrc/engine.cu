@@ -590,16 +590,29 @@ int phase_mark(pic_engine* E, int ph, bool begin, cudaStream_t s) {
   return PIC_OK;
 }
 
-int flush(pic_engine* E, cudaStream_t s) {
+// Applies the deferred kick and collisions of the given job (of every job with job < 0) now,
+// before its particles are read back or replaced; the other jobs keep theirs for their next step.
+int flush(pic_engine* E, cudaStream_t s, int job = -1) {
   bool any = false;
-  for (int j = 0; j < E->njobs_hw; ++j) any |= E->jobs[j].alive && E->jobs[j].pending;
+  for (int j = 0; j < E->njobs_hw; ++j) any |= (job < 0 || j == job) && E->jobs[j].alive && E->jobs[j].pending;
   if (!any) return PIC_OK;
-  EngineLaunch L = make_launch(E, nullptr);
-  E->launches += launch_ke_reset_pending(E->d_st, E->njobs_hw, s);
+  const uint8_t* active = nullptr;
+  JobState* st = E->d_st;
+  int nst = E->njobs_hw;
+  if (job >= 0) {
+    const int rc = job_mask(E, job, s);
+    if (rc) return rc;
+    active = E->d_mask;
+    st = E->d_st + job;
+    nst = 1;
+  }
+  EngineLaunch L = make_launch(E, active);
+  E->launches += launch_ke_reset_pending(st, nst, s);
   E->launches += launch_mover(L, PIC_PHASE_KICK_I | PIC_PHASE_MCC_I | PIC_PHASE_GATED_I, 0, s);
   E->launches += launch_ionize(L, false, s);
-  E->launches += launch_step_end(E->d_st, E->njobs_hw, nullptr, 0, 0, s);
-  for (int j = 0; j < E->njobs_hw; ++j) E->jobs[j].pending = false;
+  E->launches += launch_step_end(st, nst, nullptr, 0, 0, s);
+  for (int j = 0; j < E->njobs_hw; ++j)
+    if (job < 0 || j == job) E->jobs[j].pending = false;
   CK(cudaGetLastError());
   return PIC_OK;
 }
@@ -948,6 +961,22 @@ int pic_engine_destroy(pic_engine* E) {
   return PIC_OK;
 }
 
+int pic_engine_reserve(pic_engine* E, int64_t bytes) {
+  if (!E) return fail(PIC_ERR_ARG, "null engine");
+  if (bytes < 0) return fail(PIC_ERR_ARG, "negative reservation");
+  if (bytes == 0) return PIC_OK;
+  CK(cudaSetDevice(E->device));
+  void* p = nullptr;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, (size_t)bytes, E->pool, E->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(PIC_ERR_OOM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
+  }
+  CK(cudaFreeAsync(p, E->stream));
+  CK(cudaStreamSynchronize(E->stream));
+  return PIC_OK;
+}
+
 int pic_engine_bytes_needed(const pic_job_config* cfg, int64_t* bytes) {
   std::string why;
   const int rc = validate(cfg, why);
@@ -1241,7 +1270,7 @@ int pic_job_load_species(pic_engine* E, int job, int species, int64_t n, const d
   if (n > 0 && (!x || !y || !vx || !vy)) return fail(PIC_ERR_ARG, "null particle arrays");
   CK(cudaSetDevice(E->device));
   cudaStream_t s = E->stream;
-  rc = flush(E, s);
+  rc = flush(E, s, job);
   if (rc) return rc;
   const double *dx_ = x, *dy_ = y, *dvx = vx, *dvy = vy, *dvz = vz;
   const uint32_t* dpid = pid;
@@ -1303,7 +1332,7 @@ int pic_job_export_species(pic_engine* E, int job, int species, int64_t capacity
   if (species < 0 || species >= J.cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
   CK(cudaSetDevice(E->device));
   cudaStream_t s = E->stream;
-  rc = flush(E, s);
+  rc = flush(E, s, job);
   if (rc) return rc;
   int n = 0;
   rc = read_count(E, job, species, &n);
@@ -1369,7 +1398,7 @@ int pic_job_export_species_raw(pic_engine* E, int job, int species, int64_t capa
   if (rc) return rc;
   if (species < 0 || species >= E->jobs[job].cfg.n_species) return fail(PIC_ERR_ARG, "bad species");
   CK(cudaSetDevice(E->device));
-  rc = flush(E, E->stream);
+  rc = flush(E, E->stream, job);
   if (rc) return rc;
   int n = 0;
   rc = read_count(E, job, species, &n);
@@ -1527,7 +1556,7 @@ int pic_job_run_phases(pic_engine* E, int job, int flags, int64_t step_index, vo
   E->jobs[job].charge_fresh = false;
   CK(cudaSetDevice(E->device));
   cudaStream_t s = pick(E, stream);
-  rc = flush(E, s);
+  rc = flush(E, s, job);
   if (rc) return rc;
   rc = job_mask(E, job, s);
   if (rc) return rc;

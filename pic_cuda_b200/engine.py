@@ -188,6 +188,11 @@ class Engine:
     def step_graph(self, n: int = 1, stream=None) -> None:
         L.check(L.lib().pic_step_graph(self.h, n, stream), "pic_step_graph")
 
+    def reserve(self, nbytes: int) -> None:
+        """Map nbytes of device memory into the job pool now (pic_engine_reserve), so that
+        later job creation does not grow the pool."""
+        L.check(L.lib().pic_engine_reserve(self.h, int(nbytes)), "pic_engine_reserve")
+
     def set_option(self, option: int, value: int) -> None:
         L.check(L.lib().pic_engine_set_option(self.h, option, value), "pic_engine_set_option")
 

@@ -126,9 +126,14 @@ class Server:
     # graphs on every quantum 7.5e9 particle-steps/s, graphs once the set was stable for a
     # quantum 7.6e9, stream-ordered always 11.2e9.  With use_graph the stable quanta use graphs.
     use_graph: bool = False
+    # map the HBM budget into the engine's job pool before the first request (server start-up),
+    # so that admissions take memory that is already mapped
+    reserve: bool = True
     clock: object = time.perf_counter
     sleep: object = time.sleep
     log: list = field(default_factory=list)
+    # one entry per quantum: (start s, steps, active jobs, job set changed, seconds)
+    quanta: list = field(default_factory=list)
 
     def _admit(self, req: Request, now: float):
         cfg = job_config(req.spec)
@@ -142,6 +147,8 @@ class Server:
         return {"phi": job.get_grid(L.GRID_PHI), "species": [job.export_species(s) for s in (0, 1)]}
 
     def run(self, requests: list[Request]) -> dict:
+        if self.reserve:
+            self.engine.reserve(self.budget_bytes)
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         active = []   # [req, job, steps_left, bytes, admitted]
         used = 0
@@ -173,6 +180,7 @@ class Server:
             ts = self.clock()
             (self.engine.step_graph if self.use_graph and not changed else self.engine.step)(k)
             self.engine.sync()
+            self.quanta.append((ts - t0, k, len(active), changed, self.clock() - ts))
             changed = False
             spent["step"] += self.clock() - ts
             particle_steps += k * sum(2.0 * a[0].spec.n_per_species for a in active)

@@ -48,3 +48,29 @@ def test_batched_waves_run_every_job():
     assert all(d["step"] == 40 for _, d in res.per_job)
     assert tuner.chosen and len(tuner.trials) >= 2
     assert res.seconds > 0 and res.rate > 0
+
+
+def test_engine_reserve_maps_pool_memory():
+    """pic_engine_reserve maps memory into the job pool once: the device's free memory drops
+    by at least the reservation, job creation afterwards takes no more from the device, and a
+    negative size is rejected."""
+    import torch
+    from pic_cuda_b200.engine import Engine
+    eng = Engine(0)
+    try:
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info(0)
+        eng.reserve(2 << 30)
+        free1, _ = torch.cuda.mem_get_info(0)
+        assert free0 - free1 >= 2 << 30
+        spec = batch.JobSpec(n=257, ppc=4, Te=2.0, density=1e21, steps=2, seed=5)
+        assert batch.bytes_needed(batch.job_config(spec)) < 1 << 30
+        job = eng.add_job(batch.job_config(spec))
+        torch.cuda.synchronize()
+        free2, _ = torch.cuda.mem_get_info(0)
+        assert free2 >= free1 - (64 << 20)   # the job's arrays came from the reserved pool
+        job.destroy()
+        with pytest.raises(L.PicError):
+            eng.reserve(-1)
+    finally:
+        eng.close()

@@ -63,6 +63,10 @@ class FakeEngine:
     def __init__(self):
         self.jobs = []
         self.calls = []
+        self.reserved = 0
+
+    def reserve(self, nbytes):
+        self.reserved = nbytes
 
     def step_graph(self, k):
         self.calls.append((k, [j.steps for j in self.jobs]))
@@ -105,6 +109,7 @@ def test_server_loop_with_stand_in_engine():
     eng = FakeEngine()
     srv = FakeServer(engine=eng, budget_bytes=budget, quantum=6, clock=clk, sleep=clk.sleep)
     out = srv.run(reqs)
+    assert eng.reserved == budget   # the budget is mapped into the job pool before the first request
     comp = out["completions"]
     assert [c.index for c in comp] == list(range(len(specs)))
     # every job ran exactly its own number of steps
