@@ -28,7 +28,13 @@ __host__ __device__ constexpr int down_bw(int nu) { return round4(down_off(nu) +
 // floor(gx0 / 2) = i0 / 2 - ceil((2 NU + X) / 2).
 __host__ __device__ constexpr int up_w(int nu, int x) { return kTU + 4 * nu + 2 * x; }
 __host__ __device__ constexpr int up_off(int nu, int x) { return align_off(2 * nu + x); }
-__host__ __device__ constexpr int up_bw(int nu, int x) { return round4(up_off(nu, x) + up_w(nu, x)); }
+// Row pitch BW of the up-leg tiles.  At two post-sweeps (tile widths 40 and 42) a pitch of 52
+// floats (20 mod 32 banks) with row groups of up_group = 40 threads puts the accesses of every
+// warp of a half-sweep, including warps that straddle two row groups, in distinct banks
+// (the smallest pitch, 40 or 48, gives 1.5-1.6 wavefronts per access); other smoothing counts
+// keep the smallest pitch and one thread per interior column.
+__host__ __device__ constexpr int up_bw(int nu, int x) { return nu == 2 ? 52 : round4(up_off(nu, x) + up_w(nu, x)); }
+__host__ __device__ constexpr int up_group(int nu, int x) { return nu == 2 ? 40 : up_w(nu, x) - 2; }
 __host__ __device__ constexpr int up_cw(int nu, int x) { return up_w(nu, x) / 2 + 2; }
 __host__ __device__ constexpr int up_coff(int nu, int x) { return align_off((2 * nu + x + 1) / 2); }
 __host__ __device__ constexpr int up_cbw(int nu, int x) { return round4(up_coff(nu, x) + up_cw(nu, x)); }

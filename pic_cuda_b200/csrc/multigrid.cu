@@ -797,18 +797,23 @@ constexpr int kMaxFastNu = 4;
 
 // NU red-black SOR sweeps on a W x W tile.  ZERO: the correction enters as 0 (pre-smoothing
 // from a zero guess), so the first half-sweep reads no neighbours (they are all +0).
-template <int W, int P, int NU, int NT, bool ZERO>
+// MG threads make one row group (MG >= W - 2, the interior columns of a tile; the extra
+// threads of a group idle): with the tile pitch P chosen for it (mg_tiles.h), the lanes of a
+// warp that straddles two groups then fall into distinct banks.  Boundary tiles, with fewer
+// interior columns, leave more threads of each group idle.
+template <int W, int P, int NU, int NT, bool ZERO, int MG = W - 2>
 __device__ __forceinline__ void tile_sweeps_cols(float* e, const float* f, int gx0, int gy0, int n, float h2,
                                                  float omega) {
-  constexpr int kGmin = NT / (W - 2);                           // row groups of an interior tile
-  constexpr int kRows = ((W - 1) / 2 + kGmin - 1) / kGmin;      // rows of one colour per thread, at most
+  static_assert(MG >= W - 2 && MG <= NT, "row group width");
+  constexpr int G = NT / MG;                                    // row groups
+  constexpr int kRows = ((W - 1) / 2 + G - 1) / G;              // rows of one colour per thread, at most
   const int t = threadIdx.x;
   const int lx_lo = max(1, 1 - gx0), lx_hi = min(W - 2, n - 2 - gx0);
   const int ly_lo = max(1, 1 - gy0), ly_hi = min(W - 2, n - 2 - gy0);
   const int m = lx_hi - lx_lo + 1;
-  const int G = m > 0 ? NT / m : 0;
-  const int lx = lx_lo + (m > 0 ? t % m : 0), g = m > 0 ? t / m : NT;
-  const bool on = g < G && ly_hi >= ly_lo;
+  const int c = t % MG, g = t / MG;
+  const int lx = lx_lo + c;
+  const bool on = g < G && c < m && ly_hi >= ly_lo;
   const int par = gx0 + gy0 + lx;  // node (lx, ly) has colour (par + ly) & 1
   const float om1 = 1.f - omega;
 #pragma unroll
@@ -1043,7 +1048,7 @@ __global__ void __launch_bounds__(NT, MODE ? 5 : 1) mg_up_fast_kernel(const Tile
     }
   }
   __syncthreads();
-  tile_sweeps_cols<W, P, NU, NT, false>(e, f, gx0, gy0, nf, h2, omega);
+  tile_sweeps_cols<W, P, NU, NT, false, mgt::up_group(NU, X)>(e, f, gx0, gy0, nf, h2, omega);
   if constexpr (MODE == 0) {
 #pragma unroll
     for (int u = 0; u < NO; ++u) {
