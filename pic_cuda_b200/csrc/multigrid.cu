@@ -898,7 +898,7 @@ __global__ void __launch_bounds__(NT) mg_down_fast_kernel(const TileRef* __restr
     tma::tensor_load_2d(fs, map, gx0 - OFF, gy0, &mbar);
   }
   if (!tiles_arrived(&mbar, const_cast<JobState*>(&T))) return;
-  tile_sweeps_cols<W, P, NU, NT, true>(e, f, gx0, gy0, nf, h2, omega);
+  tile_sweeps_cols<W, P, NU, NT, true, mgt::down_group(NU)>(e, f, gx0, gy0, nf, h2, omega);
   // owned fine nodes [2 ic0, 2 ic0 + 2 kTC)
 #pragma unroll
   for (int u = 0; u < (4 * kTC * kTC) / NT; ++u) {
