@@ -946,7 +946,6 @@ __global__ void __launch_bounds__(NT, MODE ? 5 : 1) mg_up_fast_kernel(const Tile
   static_assert(W == kTU + 2 * H + 2 * X, "tile shape");
   constexpr int PW = kTU + 2;
   constexpr int KC = (W + X + 1) / 2;              // coarse cells per tile row
-  constexpr int NKC = (KC * KC + NT - 1) / NT;
   static_assert(KC + 1 <= CW, "coarse tile holds every cell's right and upper neighbour");
   constexpr int NP = MODE ? (PW * PW + NT - 1) / NT : 0;
   constexpr int NO = kTU * kTU / NT;
@@ -1026,25 +1025,25 @@ __global__ void __launch_bounds__(NT, MODE ? 5 : 1) mg_up_fast_kernel(const Tile
     tma::cp_async_wait_all();
   }
   if (!tiles_arrived(&mbar, &T)) return;
-  // ---- bilinear prolongation added to the pre-smoothed correction: one coarse cell per
-  // thread and pass, its four fine nodes (2c, 2c + 1 in each direction) with prolong_value's
-  // expressions.  gx0 has the parity X, so cell k of the tile holds tile columns 2k - X and
-  // 2k + 1 - X (the first and last cells hold one column each).
+  // ---- bilinear prolongation added to the pre-smoothed correction: per thread and pass one
+  // tile column lx and one row ky of coarse cells, i.e. the column's two fine nodes in tile rows
+  // 2 ky - X and 2 ky + 1 - X (gx0 and gy0 have the parity X), with prolong_value's expressions;
+  // the lanes of a warp sit on consecutive columns, so their updates of e meet no bank conflict
+  // (a 2 x 2 block of fine nodes per thread put the lanes two columns apart).
+  constexpr int NPR = (W * KC + NT - 1) / NT;
 #pragma unroll
-  for (int u = 0; u < NKC; ++u) {
+  for (int u = 0; u < NPR; ++u) {
     const int q = t + u * NT;
-    if (q < KC * KC) {
-      const int ky = q / KC, kx = q - ky * KC;
+    if (q < W * KC) {
+      const int ky = q / W, lx = q - ky * W;
+      const int gx = gx0 + lx, kx = (lx + X) >> 1;
+      const bool io = ((lx + X) & 1) != 0;
+      const int ly = 2 * ky - X, gy = gy0 + ly;
       const float* cp = cs + ky * CP + kx;
-      const int lx = 2 * kx - X, ly = 2 * ky - X;
-      const int gx = gx0 + lx, gy = gy0 + ly;
-      const bool x0 = lx >= 0 && (unsigned)gx < (unsigned)nf, x1 = lx + 1 < W && (unsigned)(gx + 1) < (unsigned)nf;
-      const bool y0 = ly >= 0 && (unsigned)gy < (unsigned)nf, y1 = ly + 1 < W && (unsigned)(gy + 1) < (unsigned)nf;
-      const int b = ly * P + lx;
-      if (y0 && x0) e[b] += prolong_value(cp, CP, false, false);
-      if (y0 && x1) e[b + 1] += prolong_value(cp, CP, true, false);
-      if (y1 && x0) e[b + P] += prolong_value(cp, CP, false, true);
-      if (y1 && x1) e[b + P + 1] += prolong_value(cp, CP, true, true);
+      if ((unsigned)gx < (unsigned)nf) {
+        if (ly >= 0 && (unsigned)gy < (unsigned)nf) e[ly * P + lx] += prolong_value(cp, CP, io, false);
+        if (ly + 1 < W && (unsigned)(gy + 1) < (unsigned)nf) e[(ly + 1) * P + lx] += prolong_value(cp, CP, io, true);
+      }
     }
   }
   __syncthreads();
