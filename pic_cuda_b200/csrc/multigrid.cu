@@ -64,7 +64,7 @@ __device__ double ordered_sum(const double* p, int n, int stride, int off) {
   double s = 0.0;
 #pragma unroll 8
   for (int k = threadIdx.x; k < n; k += blockDim.x) s += p[(size_t)k * stride + off];
-  __shared__ double sh[256];
+  __shared__ double sh[1024];   // blockDim.x <= 1024, a power of two
   sh[threadIdx.x] = s;
   __syncthreads();
   for (int o = blockDim.x / 2; o; o >>= 1) {
@@ -194,11 +194,11 @@ __global__ void __launch_bounds__(256) mg_init_kernel(const TileRef* __restrict_
   // the job's norms and state follow in mg_init_finish_kernel
 }
 
-// After mg_init_kernel, one CTA per job: the tiles' partial norms and charge summed in a fixed
+// After mg_init_kernel, one 1024-thread CTA per job: the tiles' partial norms and charge summed in a fixed
 // order, the relative residual of the initial guess, the potential buffers the defect
 // correction uses (with the warm start, the guess's buffer), and the job joins the running
 // count.
-__global__ void __launch_bounds__(256) mg_init_finish_kernel(const int* __restrict__ job_list,
+__global__ void __launch_bounds__(1024) mg_init_finish_kernel(const int* __restrict__ job_list,
                                                              const JobDev* __restrict__ jobs,
                                                              JobState* __restrict__ st, int* running) {
   const int job = job_list[blockIdx.x];
@@ -1097,12 +1097,12 @@ __global__ void __launch_bounds__(NT, MODE ? 5 : 1) mg_up_fast_kernel(const Tile
   }
 }
 
-// End of a V-cycle for the jobs whose level 0 ran in mg_up_fast_kernel<., 1, .>: one CTA per
-// job sums the tiles' partial norms in a fixed order, counts the cycle, swaps the potential
-// and defect buffers and takes a converged job out of the running count.  Launched after the
+// End of a V-cycle for the jobs whose level 0 ran in mg_up_fast_kernel<., 1, .>: one
+// 1024-thread CTA per job sums the tiles' partial norms in a fixed order, counts the cycle,
+// swaps the potential and defect buffers and takes a converged job out of the running count.  Launched after the
 // level-0 up kernel (waits for it in tma::pdl_wait); the next V-cycle's first launch waits for
 // this one.
-__global__ void __launch_bounds__(256) mg_finish_kernel(const int* __restrict__ job_list,
+__global__ void __launch_bounds__(1024) mg_finish_kernel(const int* __restrict__ job_list,
                                                         const JobDev* __restrict__ jobs,
                                                         JobState* __restrict__ st, int* running) {
   tma::pdl_trigger();
@@ -1252,7 +1252,7 @@ int launch_mg_init(const EngineLaunch& L, const MgLaunch& M, cudaStream_t s) {
   cudaMemsetAsync(L.running, 0, sizeof(int), s);
   if (!M.n_init) return 0;
   mg_init_kernel<<<M.n_init, 256, 0, s>>>(M.init_tiles, L.jobs, L.st);
-  mg_init_finish_kernel<<<M.n_init_jobs, 256, 0, s>>>(M.init_jobs, L.jobs, L.st, L.running);
+  mg_init_finish_kernel<<<M.n_init_jobs, 1024, 0, s>>>(M.init_jobs, L.jobs, L.st, L.running);
   return 2;
 }
 
@@ -1298,7 +1298,7 @@ static bool launch_up(const MgLaunch& M, int l, const EngineLaunch& L, bool pdl,
     up_fast(M.fast_nu_post, M.n_up[l], M.n_up[l] <= M.wide_factor * L.num_sms, pdl && M.pdl, M.up_tiles[l], L.jobs,
             L.st, l, l == 0 ? 1 : 0, s);
     if (l == 0)
-      launch_k(mg_finish_kernel, M.n_finish, 256, 0, M.pdl != 0, s, M.finish_jobs, L.jobs, L.st, L.running);
+      launch_k(mg_finish_kernel, M.n_finish, 1024, 0, M.pdl != 0, s, M.finish_jobs, L.jobs, L.st, L.running);
     return true;
   }
   mg_up_kernel<<<M.n_up[l], 256, up_smem(M.nu_post_max), s>>>(M.up_tiles[l], L.jobs, L.st, l, l == 0 ? 1 : 0,
