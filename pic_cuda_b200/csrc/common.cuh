@@ -19,6 +19,9 @@
 #include "pic_b200.h"
 
 #define PIC_CELL_OUT 0xFFFFFFFFu
+// A counting sort that falls due skips a slot whose particles are nearly in cell order: fewer
+// than 1/32 of them follow a particle of a later cell (ions, which seldom leave their cell).
+constexpr int kSortDisorderShift = 5;
 #define PIC_MAX_LEVELS 14
 #ifndef PIC_COARSE_MAX
 #define PIC_COARSE_MAX 129          // largest level side the one-CTA coarse solver takes (smem)

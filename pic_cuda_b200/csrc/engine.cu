@@ -655,7 +655,7 @@ int sort_jobs(pic_engine* E, const EngineLaunch& L, Due due, cudaStream_t s, boo
   if (!any) return PIC_OK;
   CK(cudaMemcpyAsync(E->d_mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, s));
   phase_mark(E, 0, true, s);
-  E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), s);
+  E->launches += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), true, s);
   phase_mark(E, 0, false, s);
   return PIC_OK;
 }
@@ -751,7 +751,7 @@ int build_step_graph(pic_engine* E, bool with_sort, cudaGraphExec_t* out, int64_
       max_cells = std::max(max_cells, J.dev.ncx * J.dev.ncy);
     }
     n += launch_sort_mask(L, E->d_mask, 1, E->side_stream);
-    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), E->side_stream);
+    n += launch_sort(L, E->d_mask, max_cells, (int)std::min<int64_t>(max_p, 1 << 30), true, E->side_stream);
   }
   if (err == cudaSuccess) err = cudaEventRecord(E->ev_join, E->side_stream);
   n += launch_mg_init(L, E->mg_all.L, s);
@@ -1606,7 +1606,7 @@ int pic_job_sort(pic_engine* E, int job, void* stream) {
   int64_t maxp = 0;
   for (int k = 0; k < J.cfg.n_species; ++k) maxp = std::max<int64_t>(maxp, J.cfg.species[k].capacity);
   EngineLaunch L = make_launch(E, nullptr);
-  launch_sort(L, E->d_mask, J.dev.ncx * J.dev.ncy, (int)std::min<int64_t>(maxp, 1 << 30), s);
+  launch_sort(L, E->d_mask, J.dev.ncx * J.dev.ncy, (int)std::min<int64_t>(maxp, 1 << 30), false, s);
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   return PIC_OK;

@@ -28,7 +28,7 @@ struct EngineLaunch {
   SlotDev* slots_mut;
   int* counts;            // live particles per slot
   int* hit_counts;        // hits of the last WALLS phase per slot
-  int* aux;               // 4 ints per slot (compaction counters)
+  int* aux;               // 4 ints per slot: compaction counters, lost newborns, sort descents
   int* chunk_prefix;      // nslots + 1
   const uint8_t* active;  // per slot
   int nslots;
@@ -45,7 +45,11 @@ int mover_blocks_per_sm();
 int launch_mover(const EngineLaunch& L, int flags, uint32_t explicit_step, cudaStream_t s);
 int launch_compact(const EngineLaunch& L, cudaStream_t s);
 int launch_ionize(const EngineLaunch& L, bool drift_and_deposit, cudaStream_t s);
-int launch_sort(const EngineLaunch& L, const uint8_t* sort_mask, int max_cells, int max_particles, cudaStream_t s);
+// Counting sort of the slots in sort_mask; by_disorder: the histogram pass also counts the
+// particles that follow a particle of a later cell (aux[4 s + 3]), and slots where they are
+// fewer than 1/32 of the particles are left as they are.
+int launch_sort(const EngineLaunch& L, uint8_t* sort_mask, int max_cells, int max_particles, bool by_disorder,
+                cudaStream_t s);
 int launch_step_begin(JobState* st, const JobDev* jobs, int njobs, const uint8_t* job_mask, cudaStream_t s);
 int launch_ke_reset_pending(JobState* st, int njobs, cudaStream_t s);
 int launch_step_end(JobState* st, int njobs, const uint8_t* job_mask, int set_pending, int advance, cudaStream_t s);

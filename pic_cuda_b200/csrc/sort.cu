@@ -21,9 +21,10 @@ __device__ __forceinline__ uint32_t dense_key(uint32_t c, int ncx, uint32_t ncel
   return c == PIC_CELL_OUT ? ncells : (uint32_t)cell_j(c) * (uint32_t)ncx + (uint32_t)cell_i(c);
 }
 
-__global__ void sort_zero(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask) {
+__global__ void sort_zero(const JobDev* jobs, const SlotDev* slots, const uint8_t* mask, int* aux) {
   const int s = blockIdx.y;
   if (!mask[s]) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) aux[4 * s + 3] = 0;   // descents, counted by sort_hist
   const SlotDev& S = slots[s];
   const JobDev& J = jobs[S.job];
   const int ncells = J.ncx * J.ncy + 1;
@@ -52,8 +53,11 @@ __device__ __forceinline__ void run_segment(uint32_t key, int& first, int& last)
 constexpr int kSortRounds = 4;
 constexpr int kSortItem = 32 * kSortRounds;
 
-// Histogram of cell keys, one atomic per warp segment of equal keys.
-__global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* counts, const uint8_t* mask) {
+// Histogram of cell keys, one atomic per warp segment of equal keys.  With count_descents, also
+// the particles whose key is below their predecessor's (within a warp iteration's 4 x 32), one
+// atomic per CTA into aux[4 s + 3].
+__global__ void __launch_bounds__(256) sort_hist(const JobDev* jobs, const SlotDev* slots, const int* counts,
+                                                 const uint8_t* mask, int* aux, int count_descents) {
   const int s = blockIdx.y;
   if (!mask[s]) return;
   const SlotDev& S = slots[s];
@@ -65,6 +69,7 @@ __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* c
   const int ncx = J.ncx;
   const int lane = lane_id();
   const int nitems = (n + kSortItem - 1) / kSortItem;
+  int descents = 0;
   for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < nitems; it += (gridDim.x * blockDim.x) >> 5) {
     uint32_t key[kSortRounds];
 #pragma unroll
@@ -77,7 +82,22 @@ __global__ void sort_hist(const JobDev* jobs, const SlotDev* slots, const int* c
       int first, last;
       run_segment(key[r], first, last);
       if (lane == last && key[r] != kNoKey) atomicAdd(cnt + key[r], last - first + 1);
+      if (count_descents) {
+        uint32_t prev = __shfl_up_sync(0xffffffffu, key[r], 1);
+        const uint32_t wrap = r > 0 ? __shfl_sync(0xffffffffu, key[r > 0 ? r - 1 : 0], 31) : kNoKey;
+        if (lane == 0) prev = wrap;
+        descents += (key[r] != kNoKey && prev != kNoKey && key[r] < prev) ? 1 : 0;
+      }
     }
+  }
+  if (count_descents) {
+    __shared__ int block_desc;
+    if (threadIdx.x == 0) block_desc = 0;
+    __syncthreads();
+    const int w = __reduce_add_sync(0xffffffffu, descents);
+    if (lane == 0 && w) atomicAdd(&block_desc, w);
+    __syncthreads();
+    if (threadIdx.x == 0 && block_desc) atomicAdd(aux + 4 * s + 3, block_desc);
   }
 }
 
@@ -247,6 +267,14 @@ __global__ void sort_swap(SlotDev* slots, const uint8_t* mask, int nslots) {
   swp(S.vx, S.vx_b); swp(S.vy, S.vy_b); swp(S.vz, S.vz_b); swp(S.pid, S.pid_b);
 }
 
+// Slots of the mask whose particles are nearly in cell order (descents below 1/32 of the
+// particles) leave the mask: their histogram is not scanned and they are not moved.
+__global__ void sort_filter_kernel(uint8_t* mask, const int* counts, const int* aux, int nslots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots || !mask[s]) return;
+  if (aux[4 * s + 3] < (counts[s] >> kSortDisorderShift)) mask[s] = 0;
+}
+
 // Slots whose job is due for a counting sort: sort_every > 0 and (step + offset) % sort_every
 // == 0 (offset 1: the sort at the end of a step, before the step counter advances).
 __global__ void sort_mask_kernel(const JobDev* jobs, const JobState* st, const uint8_t* active, uint8_t* mask, int nslots,
@@ -267,18 +295,20 @@ int launch_sort_mask(const EngineLaunch& L, uint8_t* mask, int offset, cudaStrea
   return 1;
 }
 
-int launch_sort(const EngineLaunch& L, const uint8_t* mask, int max_cells, int max_particles, cudaStream_t st) {
+int launch_sort(const EngineLaunch& L, uint8_t* mask, int max_cells, int max_particles, bool by_disorder,
+                cudaStream_t st) {
   if (L.nslots == 0) return 0;
   const int ncells = max_cells + 1;
   const int ntiles = (ncells + kTile - 1) / kTile;
   const int gz = std::min(std::max((ncells + 255) / 256, 1), 4 * L.num_sms);
   const int gp = std::min(std::max((max_particles + 255) / 256, 1), 8 * L.num_sms);
-  sort_zero<<<dim3(gz, L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
-  sort_hist<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
+  sort_zero<<<dim3(gz, L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask, L.aux);
+  sort_hist<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask, L.aux, by_disorder ? 1 : 0);
+  if (by_disorder) sort_filter_kernel<<<(L.nslots + 255) / 256, 256, 0, st>>>(mask, L.counts, L.aux, L.nslots);
   sort_tile_sums<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_scan_parts<<<L.nslots, 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_apply<<<dim3(std::min(ntiles, 4 * L.num_sms), L.nslots), 256, 0, st>>>(L.jobs, L.slots, mask);
   sort_scatter<<<dim3(gp, L.nslots), 256, 0, st>>>(L.jobs, L.slots, L.counts, mask);
   sort_swap<<<(L.nslots + 255) / 256, 256, 0, st>>>(L.slots_mut, mask, L.nslots);
-  return 7;
+  return by_disorder ? 8 : 7;
 }
