@@ -361,10 +361,11 @@ __device__ __forceinline__ float prolong_value(const float* cp, int pitch, bool 
 // ---------------------------------------------------------------- mg_coarse
 // Levels lc .. L-1 of one job in the shared memory of one 1024-thread CTA.  Level l occupies
 // E then F, n_l rows of pitch n_l + 1 (even).  Every red-black half-sweep, restriction and
-// prolongation maps thread t to column i = 1 + t % (n-2) and walks the rows 1 + t / (n-2)
-// + k G (G = threads / (n-2) row groups), so the lanes of a warp touch consecutive columns:
-// with an even pitch the two colours of a column pair fall into distinct banks, and no lane
-// idles on the other colour.  Every level uses the whole CTA: the small levels are a chain of
+// prolongation maps thread t to a column and a row group (col_map: groups of the power of two
+// at or above the n-2 interior columns) and walks the group's rows k G apart, so the lanes of
+// a warp touch consecutive columns: with an even pitch the two colours of a column pair fall
+// into distinct banks, and no lane idles on the other colour.  Every level uses the whole CTA
+// (levels up to 17^2 the first 128 threads): the small levels are a chain of
 // barrier-separated phases whose length is one node's latency when each thread has at most
 // one node (measured on B200: one warp walking 17^2 .. 3^2 alone took 12 of the solve's 29 us).
 constexpr int kCoarseThreads = 1024;
@@ -376,21 +377,25 @@ struct CoarseLevel {
   int n;         // side
   float h2;      // h_l^2
   float ih2;     // 1 / h_l^2
-  float rm;      // 1 / (n - 2) in FP32 (column map), 0 if the level has no interior
 };
 
-// Thread t of T on m interior columns: column 1 + t % m, row group t / m of G = T / m.  The
-// quotient comes from (t + 0.5) * (1/m) in FP32, exact for t, T < 2^12 and m < 2^12 (the
-// fraction stays >= 0.5 / m from an integer, far above the rounding error).
+// Thread t of T on m interior columns: row groups of 2^s >= m threads (the smallest such
+// power of two), column 1 + t % 2^s, group t / 2^s of G = T / 2^s; lanes past the m columns
+// idle (group G).  With a power-of-two group width a warp holds whole groups or a part of one,
+// so the lanes of a half-sweep fall in distinct banks; groups of exactly m threads put lanes of
+// neighbouring groups, two rows apart, in the same banks (65^2: 940 shared-memory wavefronts
+// per half-sweep set against 640; 33^2: 310 against 160).
 struct ColMap {
   int col, g, G;
 };
-__device__ __forceinline__ ColMap col_map(int t, int T, int m, float rm) {
+__device__ __forceinline__ ColMap col_map(int t, int T, int m) {
   ColMap c;
   if (m <= 0) { c.col = 1; c.g = 1; c.G = 0; return c; }
-  c.G = (int)(((float)T + 0.5f) * rm);
-  c.g = (int)(((float)t + 0.5f) * rm);
-  c.col = 1 + t - c.g * m;
+  const int sh = m > 1 ? 32 - __clz(m - 1) : 0;
+  c.G = T >> sh;
+  c.g = t >> sh;
+  c.col = 1 + (t & ((1 << sh) - 1));
+  if (c.col > m) c.g = c.G;
   return c;
 }
 
@@ -413,7 +418,7 @@ __device__ void level_sweeps(float* sm, const CoarseLevel& L, float omega, int n
   float* const e = sm + L.off;
   const float* const f = e + n * P;
   const float h2 = L.h2;
-  const ColMap cm = col_map(t, T, n - 2, L.rm);
+  const ColMap cm = col_map(t, T, n - 2);
   const int i = cm.col, g = cm.g, G = cm.G;
   const bool on = g < G;
   const float om1 = 1.f - omega;
@@ -448,7 +453,7 @@ __device__ void level_restrict(float* sm, const CoarseLevel& A, const CoarseLeve
   const float* const f = e + n * P;
   float* const fn = sm + B.off + nc * Pc;
   const float inv_h2 = A.ih2;
-  const ColMap cm = col_map(t, T, nc - 2, B.rm);
+  const ColMap cm = col_map(t, T, nc - 2);
   const int ic = cm.col, g = cm.g, G = cm.G;
   if (g < G)
     for (int jc = 1 + g; jc <= nc - 2; jc += G) {
@@ -474,7 +479,7 @@ __device__ void level_prolong(float* sm, const CoarseLevel& A, const CoarseLevel
   const int n = A.n, P = n + 1, Pc = B.n + 1;
   float* const e = sm + A.off;
   const float* const c = sm + B.off;
-  const ColMap cm = col_map(t, T, n - 2, A.rm);
+  const ColMap cm = col_map(t, T, n - 2);
   const int i = cm.col, g = cm.g, G = cm.G;
   if (g < G)
     for (int j = 1 + g; j <= n - 2; j += G)
@@ -547,7 +552,6 @@ __device__ void coarse_solve(const int job, const JobDev* __restrict__ jobs, con
     lv[l].n = n;
     lv[l].h2 = (float)(hl * hl);
     lv[l].ih2 = (float)(1.0 / (hl * hl));
-    lv[l].rm = n > 2 ? 1.f / (float)(n - 2) : 0.f;
   }
   __syncthreads();
   if (t == 0) {
