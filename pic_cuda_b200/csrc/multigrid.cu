@@ -9,16 +9,19 @@
 // the update phi += e and the norms are FP64 (defect correction), so the FP64 relative
 // residual can be driven to 1e-9 and below.
 // Kernels (one launch covers all jobs through tile lists):
-//   mg_init    level 0: r = F - A phi (FP64), ||r||^2, ||F||^2; r -> f0 (FP32)
+//   mg_init    level 0: r = F - A phi (FP64), ||r||^2, ||F||^2; r -> f0 (FP32); per-tile
+//              partials, summed in a fixed order by mg_init_finish (one CTA per job)
 //   mg_down    per level above the coarse one: nu_pre sweeps from e = 0 on a 16x16 tile of
 //              coarse nodes (fine tile + halo 2*nu+2 in shared memory, every sweep done
 //              locally: a node at distance d from the tile edge is exact for d half-sweeps),
 //              then residual + full weighting straight from shared memory
 //   mg_coarse  one CTA per job runs the whole V-cycle from <= 65x65 down in shared memory
-//   (levels 129^2-513^2 and below run in one thread-block cluster, mg_cluster.cu)
+//   (opt-in: levels up to 257^2 or 513^2 in one thread-block cluster, mg_cluster.cu)
 //   mg_up      prolongation + nu_post sweeps on 32x32 tiles; on level 0 also the FP64
-//              update phi += e, the new FP64 residual and the norm (last CTA of each
-//              job reduces the per-tile partials in a fixed order: deterministic).
+//              update phi += e, the new FP64 residual and the tile's partial norm;
+//              mg_finish (one CTA per job) sums the partials in a fixed order
+//              (deterministic), counts the cycle and decides convergence.  The generic
+//              kernels (mixed smoothing counts) still let the last tile CTA of a job do it.
 #include <algorithm>
 #include "common.cuh"
 #include "kernels.h"
