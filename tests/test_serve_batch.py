@@ -2,6 +2,7 @@
 budget, the FIFO replay, and the request loop driven by a stand-in engine."""
 import numpy as np
 
+from pic_cuda_b200 import _lib as L
 from pic_cuda_b200 import batch, serve
 
 
@@ -122,3 +123,49 @@ def test_server_loop_with_stand_in_engine():
     assert max(len(c[1]) for c in eng.calls) > 1
     assert all(c.finished >= c.admitted >= c.arrival for c in comp)
     assert out["p99"] >= out["p50"] > 0
+
+
+class _OptEngine:
+    """Stand-in engine that keeps the options the tuner sets."""
+    def __init__(self):
+        self.opts = {}
+
+    def set_option(self, k, v):
+        self.opts[k] = v
+
+
+class _SortJob:
+    def __init__(self):
+        self.sort_every = None
+
+    def set_sort_every(self, v):
+        self.sort_every = v
+
+
+def test_autotuner_coordinate_search_on_host():
+    """The tuner times each knob's candidates with the others at their best so far, keeps the
+    fastest, leaves it applied, and stays within half of the steps it may use."""
+    from pic_cuda_b200 import autotune
+    eng, jobs = _OptEngine(), [_SortJob(), _SortJob()]
+    cost = {("lk", 1): 0.5, ("mc", 3): 0.25, ("wt", 4): 0.125}
+
+    class T(autotune.Tuner):
+        def _time(self, engine, stream, steps):
+            o = engine.opts
+            c = 10.0 - cost.get(("lk", o[L.OPT_MG_LEVELS_KERNEL]), 0.0)
+            c -= cost.get(("mc", o[L.OPT_MOVER_CTAS_PER_SM]), 0.0)
+            c -= cost.get(("wt", o[L.OPT_MG_WIDE_TILES]), 0.0)
+            c -= 0.0625 if jobs[0].sort_every == 20 else 0.0
+            return c
+
+    t = T(steps_per_trial=3)
+    used = t.tune(eng, jobs, None, max_steps=300)
+    assert t.chosen == {"levels_kernel": 1, "sort_every": 20, "mover_ctas_per_sm": 3, "mg_wide_tiles": 4}
+    assert eng.opts == {L.OPT_MG_LEVELS_KERNEL: 1, L.OPT_MOVER_CTAS_PER_SM: 3, L.OPT_MG_WIDE_TILES: 4}
+    assert all(j.sort_every == 20 for j in jobs)
+    # one trial for the start point and one per further candidate: 1 + 1 + 1 + 1 + 2
+    assert len(t.trials) == 6 and used == 6 * 4
+    # a small step budget cuts the search short and stays within half of it
+    t2 = T(steps_per_trial=3)
+    used2 = t2.tune(_OptEngine(), [_SortJob()], None, max_steps=20)
+    assert used2 <= 10 and len(t2.trials) == used2 // 4
